@@ -1,0 +1,70 @@
+/*
+ * shoc_grid.h -- builds a SHOC-style sparse window for a closed rectangular
+ * (or curvilinear) basin: the layout model/hd/master/preprocess.c:108
+ * (build_sparse_map) produces, restricted to what the tracer step reads.
+ *
+ * Numbering: wet cells layer by layer from the surface layer (k = nz-1)
+ * down, i fastest then j (preprocess.c:355-370); each layer's lateral ghost
+ * cells follow its wet cells (preprocess.c:532-563); one sediment cell per
+ * column comes last with a self-mapping zm1.  Slot 0 is unused.
+ */
+#ifndef SHOC_GRID_H
+#define SHOC_GRID_H
+
+#include "shoc_tr.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct shoc_grid_spec {
+  int nx, ny, nz;              /* nce1, nce2, layers */
+  const double *layers;        /* [nz+1] layer faces, layers[0] deepest */
+  const double *bathy;         /* [ny*nx] bottom z (negative down) */
+  const unsigned char *land;   /* [ny*nx] nonzero = land column */
+  /* metrics at cell centres and faces, all [(ny+1)*(nx+1)] with row
+   * stride nx+1 so faces on the i = nx / j = ny edges have values */
+  const double *h1acell, *h2acell, *h1au1, *h2au1, *h1au2, *h2au2;
+} shoc_grid_spec;
+
+/* A built window.  Owns every array; geom points into them. */
+typedef struct shoc_grid {
+  shoc_tr_geom geom;
+  int nx, ny, nz;
+  int nwet;                    /* wet 3D cells (== a3_t) */
+  int ncol;                    /* wet columns (== b2_t) */
+  int nghost;                  /* lateral ghost cells */
+  int *kbot;                   /* [ny*nx] bottom layer, -1 for land */
+  int *map_top;                /* [ny*nx] surface-layer cell, 0 for land */
+  int *is_wet;                 /* [sgsiz] 1 for wet cells */
+  /* owned storage */
+  int *w3_t, *w2_t, *bot_t, *w3_e1, *w3_e2;
+  int *xp1, *xm1, *yp1, *ym1, *zp1, *zm1, *m2d, *s2i, *s2j, *s2k;
+  int *bpt, *bin;
+  double *h1au1, *h2au2, *h1au2, *h2au1, *h1acell, *h2acell, *cellarea, *botz;
+  double *gridz;
+} shoc_grid;
+
+/* Returns 0 on success, SHOC_TR_EGEOM on an inconsistent spec,
+ * SHOC_TR_ENOMEM on allocation failure. */
+int shoc_grid_build(const shoc_grid_spec *spec, shoc_grid *out);
+void shoc_grid_free(shoc_grid *g);
+
+/* Surface vectors for a free surface at eta: nsur_t[cc] is the cell holding
+ * the surface (the walk of tracers.c:5756-5769); sur_t is set equal. */
+void shoc_grid_init_surface(const shoc_grid *g, const double *eta,
+                            int *sur_t, int *nsur_t);
+
+/* Vertical velocity from continuity, bottom up (the z-model branch of
+ * model/hd/momentum/vel3d.c:4609 vel_w_update, no sources): w at the bottom
+ * face of each column's bottom cell is 0 and w[zp1] = (flux into cell c
+ * from below and the sides) / cellarea, up to the cell below the surface
+ * cell sur_t.  w is zeroed first. */
+void shoc_grid_w_from_continuity(const shoc_grid *g, const int *sur_t,
+                                 const double *u1flux3d,
+                                 const double *u2flux3d, double *w);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,81 @@
+"""CPU checkers for the tracer step (TEST INFRASTRUCTURE ONLY).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may import this package, and only as the thing results are checked
+against or timed beside -- never as part of the product path.
+
+  run_oracle(case, nsteps, ...)  the C restatement (oracle/shoc_oracle.c)
+  run_ref(case, nsteps, ...)     the reference's own tracers.c, compiled
+                                 unmodified (oracle/_ref, built by
+                                 oracle/build.py where the reference exists)
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from ems_b200 import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_libs = {}
+
+
+def _load(name):
+    if name in _libs:
+        return _libs[name]
+    from . import build
+    if name == "oracle":
+        path = build.oracle_lib()
+        L = C.CDLL(path)
+        L.oracle_run.argtypes = [C.POINTER(_abi.Geom), C.POINTER(_abi.State),
+                                 C.POINTER(_abi.Opts), C.c_int, C.POINTER(_abi.Diag)]
+        L.oracle_run.restype = C.c_int
+    else:
+        fname = "libshoc_ref_omp.so" if name == "ref_omp" else "libshoc_ref.so"
+        path = os.path.join(HERE, "_ref", fname)
+        if not os.path.exists(path):
+            build.ref_libs()
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_run.argtypes = [C.POINTER(_abi.Geom), C.POINTER(_abi.State),
+                              C.POINTER(_abi.Opts), C.c_int, C.c_int, C.POINTER(_abi.Diag)]
+        L.ref_run.restype = C.c_int
+        L.ref_last_message.restype = C.c_char_p
+    _libs[name] = L
+    return L
+
+
+def ref_available(omp=False):
+    return _load("ref_omp" if omp else "ref") is not None
+
+
+def _call(fn, case, nsteps, tr, sur, nsur, *extra):
+    keep = []
+    if tr is None:
+        tr, sur, nsur = case.copy_state()
+    st = case.make_state(tr, sur, nsur, keep)
+    op = case.make_opts(keep)
+    d = _abi.Diag()
+    rc = fn(C.byref(case.win.geom), C.byref(st), C.byref(op), int(nsteps), *extra, C.byref(d))
+    return rc, tr, sur, nsur, d
+
+
+def run_oracle(case, nsteps, tr=None, sur=None, nsur=None):
+    """nsteps of the restatement; returns (status, tr, sur_t, nsur_t, diag)."""
+    return _call(_load("oracle").oracle_run, case, nsteps, tr, sur, nsur)
+
+
+def run_ref(case, nsteps, tr=None, sur=None, nsur=None, nthreads=1):
+    """nsteps of the reference build; nthreads > 1 uses its OpenMP loop."""
+    L = _load("ref_omp" if nthreads > 1 else "ref")
+    if L is None:
+        raise FileNotFoundError("reference build oracle/_ref not available")
+    return _call(L.ref_run, case, nsteps, tr, sur, nsur, C.c_int(int(nthreads)))
+
+
+def max_rel_err(a, b, cells, floor=1e-300):
+    """max over cells of |a-b| / max(|b|, floor), per tracer row."""
+    a = np.asarray(a)[..., cells]
+    b = np.asarray(b)[..., cells]
+    return (np.abs(a - b) / np.maximum(np.abs(b), floor)).max(axis=-1)

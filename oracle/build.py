@@ -1,0 +1,87 @@
+"""Builds the CPU checkers (TEST INFRASTRUCTURE ONLY).
+
+  oracle/_lib/liboracle.so          the C restatement in oracle/shoc_oracle.c
+  oracle/_ref/libshoc_ref.so        the reference's own model/hd/tracers/tracers.c,
+                                    compiled unmodified, single thread
+  oracle/_ref/libshoc_ref_omp.so    the same with -fopenmp -DHAVE_OMP (the
+                                    reference's OpenMP tracer loop)
+
+The reference libraries are built only where the reference source tree is
+present (REF_ROOT, default /root/reference); elsewhere the prebuilt files
+are used as they are.  The reference build uses three stub headers
+(oracle/ref/stub) for netcdf.h / ems_conf.h / svn_rev.h and the no-op link
+stubs in oracle/ref/ref_harness.c.  Flags: -O3 -march=x86-64-v3
+-ffp-contract=off, so no product or sum is fused and results are bitwise
+comparable with the restatement.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+LIB = os.path.join(HERE, "_lib")
+REF_OUT = os.path.join(HERE, "_ref")
+
+CFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared"]
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout)
+        raise RuntimeError("oracle build failed: " + " ".join(cmd))
+
+
+def oracle_lib(force=False):
+    os.makedirs(LIB, exist_ok=True)
+    out = os.path.join(LIB, "liboracle.so")
+    src = os.path.join(HERE, "shoc_oracle.c")
+    deps = [src, os.path.join(HERE, "shoc_oracle.h"), os.path.join(ROOT, "include", "shoc_tr.h")]
+    if force or _stale(out, deps):
+        _run(["gcc", "-std=c99"] + CFLAGS + ["-I", os.path.join(ROOT, "include"), "-o", out,
+                                             src, "-lm"])
+    return out
+
+
+def ref_available():
+    return os.path.exists(os.path.join(REF_ROOT, "model", "hd", "tracers", "tracers.c"))
+
+
+def ref_libs(force=False):
+    """Compile the reference tracer step (only where its sources exist)."""
+    outs = [os.path.join(REF_OUT, "libshoc_ref.so"), os.path.join(REF_OUT, "libshoc_ref_omp.so")]
+    if not ref_available():
+        return [o for o in outs if os.path.exists(o)]
+    os.makedirs(REF_OUT, exist_ok=True)
+    R = REF_ROOT
+    inc = ["-I", os.path.join(HERE, "ref", "stub"), "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(R, "lib", "include"), "-I", os.path.join(R, "model", "hd", "include")]
+    for sub in ("sediments", "tracerstats", "waves", "ecology", "da"):
+        inc += ["-I", os.path.join(R, "model", "lib", sub, "include")]
+    srcs = [os.path.join(R, "model", "hd", "tracers", "tracers.c"),
+            os.path.join(HERE, "ref", "ref_harness.c")]
+    deps = srcs + [os.path.join(ROOT, "include", "shoc_tr.h")]
+    for out, extra in ((outs[0], []), (outs[1], ["-fopenmp", "-DHAVE_OMP"])):
+        if force or _stale(out, deps):
+            _run(["gcc", "-w"] + CFLAGS + extra + inc + ["-o", out] + srcs + ["-lm"])
+    return outs
+
+
+def build_all(force=False):
+    out = [oracle_lib(force)]
+    out += ref_libs(force)
+    return out
+
+
+if __name__ == "__main__":
+    for p in build_all(force="--force" in sys.argv):
+        print(p)
