@@ -50,7 +50,7 @@ def grid_lib(force=False):
     srcs = [os.path.join(CSRC, s) for s in GRID_SRC]
     deps = srcs + [os.path.join(CSRC, "shoc_grid.h"), os.path.join(INCLUDE, "shoc_tr.h")]
     if force or _stale(out, deps):
-        _run(["gcc", "-O2", "-fPIC", "-shared", "-std=c99", "-I", INCLUDE, "-I", CSRC,
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-fopenmp", "-I", INCLUDE, "-I", CSRC,
               "-o", out] + srcs)
     return out
 

@@ -290,3 +290,148 @@ void shoc_grid_w_from_continuity(const shoc_grid *g, const int *sur_t,
     }
   }
 }
+
+/* ---------------------------------------------------------------------- */
+/* seeded synthetic fields                                                 */
+
+#include <math.h>
+
+static unsigned long long mix64(unsigned long long x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+static double u01(unsigned long long seed, unsigned long long a, unsigned long long b) {
+  unsigned long long h = mix64(seed ^ mix64(a * 0x100000001b3ull + mix64(b)));
+  return ((h >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+/* z of the top / bottom face of wet cell c */
+static double cell_top(const shoc_grid *g, const double *eta, int c) {
+  const shoc_tr_geom *G = &g->geom;
+  double e = eta[G->m2d[c]];
+  double t = (G->zp1[c] == c) ? e : G->gridz[G->zp1[c]];
+  return t < e ? t : e;
+}
+static double cell_bot(const shoc_grid *g, int c) {
+  const shoc_tr_geom *G = &g->geom;
+  int zm = G->zm1[c];
+  return g->is_wet[zm] ? G->gridz[c] : G->botz[G->m2d[c]];
+}
+
+int shoc_synth_flow(const shoc_grid *g, const double *psi, const double *amp, const double *eta,
+                    double umax, double *u1, double *u2, double *u1flux3d, double *u2flux3d,
+                    double *dzu1, double *dzu2) {
+  const shoc_tr_geom *G = &g->geom;
+  const int nx = g->nx, ny = g->ny, S = G->sgsiz;
+  const size_t nf = (size_t)(nx + 1) * (ny + 1);
+  double *D = (double *)calloc(nf, sizeof(double));
+  double *Q = (double *)calloc(nf, sizeof(double));
+  if (!D || !Q) { free(D); free(Q); return SHOC_TR_ENOMEM; }
+  memset(u1, 0, S * sizeof(double)); memset(u2, 0, S * sizeof(double));
+  memset(u1flux3d, 0, S * sizeof(double)); memset(u2flux3d, 0, S * sizeof(double));
+  memset(dzu1, 0, S * sizeof(double)); memset(dzu2, 0, S * sizeof(double));
+  double vmax = 0.0;
+  for (int axis = 0; axis < 2; axis++) {
+    const int *nbm = axis == 0 ? G->xm1 : G->ym1;
+    double *flux = axis == 0 ? u1flux3d : u2flux3d;
+    double *vel = axis == 0 ? u1 : u2;
+    double *dzf = axis == 0 ? dzu1 : dzu2;
+    memset(D, 0, nf * sizeof(double));
+    memset(Q, 0, nf * sizeof(double));
+    for (int pass = 0; pass < 3; pass++) {
+      for (int cc = 1; cc <= G->a3_t; cc++) {
+        int c = G->w3_t[cc], nb = nbm[c];
+        if (!g->is_wet[nb]) continue;
+        int i = G->s2i[c], j = G->s2j[c];
+        size_t f = (size_t)j * (nx + 1) + i;
+        double tp = fmin(cell_top(g, eta, c), cell_top(g, eta, nb));
+        double bt = fmax(cell_bot(g, c), cell_bot(g, nb));
+        double dz = tp - bt > 0.0 ? tp - bt : 0.0;
+        double zmid = 0.5 * (tp + bt);
+        if (pass == 0) {
+          D[f] += dz;
+        } else {
+          double q = cos(3.141592653589793 * zmid / fmax(D[f], 1e-9));
+          if (pass == 1) {
+            Q[f] += dz * q;
+          } else {
+            double U = axis == 0 ? psi[(size_t)(j + 1) * (nx + 1) + i] - psi[f]
+                                 : -(psi[(size_t)j * (nx + 1) + i + 1] - psi[f]);
+            double qbar = Q[f] / D[f];
+            int jj = j < ny ? j : ny - 1, ii = i < nx ? i : nx - 1;
+            double a = amp[(size_t)jj * nx + ii];
+            double fl = U * dz / D[f] + a * fabs(U) / D[f] * dz * (q - qbar);
+            int c2 = G->m2d[c];
+            double h2 = axis == 0 ? G->h2au1[c2] : G->h1au2[c2];
+            double v = dz > 0.0 ? fl / (dz * h2) : 0.0;
+            flux[c] = fl;
+            vel[c] = v;
+            dzf[c] = dz;
+            if (fabs(v) > vmax) vmax = fabs(v);
+          }
+        }
+      }
+    }
+  }
+  double s = vmax > 0.0 ? umax / vmax : 0.0;
+  for (int c = 0; c < S; c++) {
+    u1[c] *= s; u2[c] *= s; u1flux3d[c] *= s; u2flux3d[c] *= s;
+  }
+  free(D);
+  free(Q);
+  return SHOC_TR_OK;
+}
+
+void shoc_synth_kz_exp(const shoc_grid *g, double k0, double k1, double *Kz) {
+  const shoc_tr_geom *G = &g->geom;
+  memset(Kz, 0, (size_t)G->sgsiz * sizeof(double));
+  double r = log(k1 / k0);
+  for (int cc = 1; cc <= G->a3_t; cc++) {
+    int c = G->w3_t[cc];
+    double H = -G->botz[G->m2d[c]];
+    double fr = -G->gridz[c] / H;
+    fr = fr < 0.0 ? 0.0 : (fr > 1.0 ? 1.0 : fr);
+    Kz[c] = k0 * exp(r * fr);
+  }
+}
+
+void shoc_synth_kz_logu(const shoc_grid *g, unsigned long long seed, double lo, double hi,
+                        double *Kz) {
+  const shoc_tr_geom *G = &g->geom;
+  memset(Kz, 0, (size_t)G->sgsiz * sizeof(double));
+  double a = log(lo), b = log(hi);
+#pragma omp parallel for schedule(static)
+  for (int cc = 1; cc <= G->a3_t; cc++) {
+    int c = G->w3_t[cc];
+    Kz[c] = exp(a + (b - a) * u01(seed, 0x4b7a, (unsigned long long)c));
+  }
+}
+
+void shoc_synth_tracers_logn(const shoc_grid *g, unsigned long long seed, int ntr, double lo_mag,
+                             double hi_mag, const double *sm, double *tr) {
+  const shoc_tr_geom *G = &g->geom;
+  const size_t S = (size_t)G->sgsiz, n2 = (size_t)g->nx * g->ny;
+  memset(tr, 0, S * ntr * sizeof(double));
+  for (int n = 0; n < ntr; n++) {
+    double mag = lo_mag * pow(hi_mag / lo_mag, ntr > 1 ? (double)n / (ntr - 1) : 0.0);
+    double *t = tr + (size_t)n * S;
+    const double *f = sm + (size_t)n * n2;
+    double cosk[4096];
+    for (int k = 0; k < G->nz && k < 4096; k++)
+      cosk[k] = 0.3 * cos(3.141592653589793 * k / G->nz + n);
+#pragma omp parallel for schedule(static)
+    for (int cc = 1; cc <= G->a3_t; cc++) {
+      int c = G->w3_t[cc];
+      int i = G->s2i[c], j = G->s2j[c], k = G->s2k[c];
+      /* approximately normal noise: Irwin-Hall sum of four uniforms */
+      unsigned long long hh = mix64(seed ^ mix64(((unsigned long long)n << 40) ^ (unsigned long long)c));
+      double nz4 = ((double)(hh & 0xffff) + (double)((hh >> 16) & 0xffff) +
+                    (double)((hh >> 32) & 0xffff) + (double)(hh >> 48)) / 65536.0 - 2.0;
+      double lg = 1.5 * (f[(size_t)j * g->nx + i] - 0.5) + 0.25 * 1.7320508075688772 * nz4 +
+                  cosk[k];
+      t[c] = mag * exp(lg);
+    }
+  }
+}

@@ -68,3 +68,31 @@ void shoc_grid_w_from_continuity(const shoc_grid *g, const int *sur_t,
 }
 #endif
 #endif
+
+/* ---- seeded synthetic fields (loops over every wet cell / face) ---- */
+#ifdef __cplusplus
+extern "C" {
+#endif
+/* Face volume fluxes of a closed basin from a corner transport
+ * streamfunction psi [(ny+1)*(nx+1)] (barotropic, spread over each face's
+ * wet layers by thickness) plus a baroclinic part amp [ny*nx] * |U| / D *
+ * dz * (q - qbar) whose depth integral is zero on every face; scaled so the
+ * largest face velocity is umax.  Fills u1, u2, u1flux3d, u2flux3d, dzu1,
+ * dzu2 [sgsiz] (zero elsewhere).  eta: free surface [sgsizS]. */
+int shoc_synth_flow(const shoc_grid *g, const double *psi, const double *amp,
+                    const double *eta, double umax, double *u1, double *u2,
+                    double *u1flux3d, double *u2flux3d, double *dzu1, double *dzu2);
+/* Kz at bottom faces: k0 * (k1/k0)^(depth of the face / column depth). */
+void shoc_synth_kz_exp(const shoc_grid *g, double k0, double k1, double *Kz);
+/* Kz log-uniform in [lo, hi], independent per cell (counter-based RNG). */
+void shoc_synth_kz_logu(const shoc_grid *g, unsigned long long seed, double lo,
+                        double hi, double *Kz);
+/* Tracer n: mag_n * exp(1.5 (sm_n - 0.5) + 0.25 N + 0.3 cos(pi k / nz + n)), N a
+ * unit-variance Irwin-Hall (four-uniform) deviate from a counter-based hash,
+ * mag_n log-spaced in [lo_mag, hi_mag]; sm [ntr*ny*nx] smooth fields. */
+void shoc_synth_tracers_logn(const shoc_grid *g, unsigned long long seed, int ntr,
+                             double lo_mag, double hi_mag, const double *sm,
+                             double *tr);
+#ifdef __cplusplus
+}
+#endif

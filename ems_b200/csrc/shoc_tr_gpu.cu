@@ -1,0 +1,1116 @@
+// shoc_tr_gpu.cu -- host side and per-step kernels of the B200 SHOC tracer
+// step (C-ABI in include/shoc_tr_gpu.h).
+//
+// Per step, on the handle's stream:
+//   k_reset     clears the per-step reductions
+//   k_lateral   set_lateral_BC_tr (tracers.c:5574) into both tracer buffers
+//   k_set_dz    one thread per column: set_dz (tracers.c:5731-5848), the
+//               scheme work arrays w5/w9 (:561-567) and their 2/(w9+w9)
+//               factors, the sub-step search (:591-668) as a min-reduction,
+//               and the tracer-independent tridiagonal LU factors of
+//               vert_diffuse_3d / implicit_vdiff_tr (:3841-3889, :4185-4195)
+//   per sub-step:
+//     k_courant   w6/w7/w8 (:726-737)
+//     k_transport all (column, tracer) pairs: see column_pass
+//     k_serial    the rare columns whose tr_bounds thin-surface fix couples
+//                 tracers, one thread per column looping over tracers
+// Tracers ping-pong between two buffers; a step is captured in a CUDA graph
+// once its sub-step schedule is known.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "shoc_tr_gpu.h"
+#include "shoc_tr_kernels.cuh"
+
+using namespace shoc;
+
+namespace {
+
+constexpr int kItermax = 20;  // tracers.c:430
+
+struct Sched {
+  double dtm = 0.0;
+  std::vector<SubStep> sub;
+};
+
+}  // namespace
+
+struct shoc_tr_gpu {
+  int device = 0;
+  int precision = SHOC_TR_FP64;
+  cudaStream_t stream = nullptr;
+  int ntr = 0, S = 0, S2 = 0, nz = 0, ncol = 0, nbpt = 0;
+  Geo G{};
+  Flow F{};
+  Work W{};
+  Opt O{};
+  TrSet T{};
+  int nslot = 0;
+  bool any_vdiff = false, any_hdiff = false;
+  double dt = 0.0;
+  // device allocations
+  std::vector<void *> allocs;
+  double *tr[2] = {nullptr, nullptr};
+  int cur = 0;
+  int *bpt = nullptr, *bin = nullptr;
+  // host mirror of the per-tracer flags
+  std::vector<uint8_t> trf;
+  // schedule / graph
+  int probe_left = 2;
+  bool have_sched = false;
+  Sched sched;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  int graph_nsub = -1;
+  // tiling
+  int tw = 8;
+  // profiling
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  double prof_ms = 0.0;
+  int prof_n = 0;
+  long long launches = 0;
+  // pinned readback
+  unsigned long long *h_dtm = nullptr;
+  int *h_status = nullptr;
+  unsigned long long *h_nwarn = nullptr;
+  int *h_counts = nullptr;
+  int *d_counts = nullptr;  // [0] vcs, [1] vc
+  int last_status = 0;
+  long long warn_total = 0;
+};
+
+namespace {
+
+#define CK(x)                                       \
+  do {                                              \
+    cudaError_t e_ = (x);                           \
+    if (e_ != cudaSuccess) {                        \
+      fprintf(stderr, "shoc_tr_gpu: %s:%d %s\n", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+      return SHOC_TR_ECUDA;                         \
+    }                                               \
+  } while (0)
+
+template <class T>
+int dalloc(shoc_tr_gpu *h, T **p, size_t n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, (n ? n : 1) * sizeof(T));
+  if (e != cudaSuccess) return SHOC_TR_ENOMEM;
+  h->allocs.push_back(q);
+  *p = (T *)q;
+  return 0;
+}
+
+template <class T>
+int dupload(shoc_tr_gpu *h, T **p, const T *src, size_t n) {
+  int rc = dalloc(h, p, n);
+  if (rc) return rc;
+  if (src && n) CK(cudaMemcpy(*p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  else CK(cudaMemset(*p, 0, (n ? n : 1) * sizeof(T)));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// kernels
+
+__global__ void k_reset(Work W, int *counts) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    *W.dtm_bits = 0x7ff0000000000000ull;  // +inf
+    *W.serial_count = 0;
+    counts[0] = 0;
+    counts[1] = 0;
+  }
+}
+
+// Lateral ghosts take their interior value (set_lateral_BC_tr): written into
+// both tracer buffers so the value read during every sub-step, and the value
+// left in the returned array, is the start-of-step one.
+__global__ void k_lateral(int nbpt, const int *bpt, const int *bin, int ntr, int S,
+                          double *tra, double *trb) {
+  long long tot = (long long)nbpt * ntr;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    int n = (int)(i / nbpt), b = (int)(i % nbpt);
+    size_t off = (size_t)n * S;
+    double v = tra[off + bin[b]];
+    tra[off + bpt[b]] = v;
+    trb[off + bpt[b]] = v;
+  }
+}
+
+__device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) {
+  atomicMin(p, (unsigned long long)__double_as_longlong(v));
+}
+
+// One thread per column.
+__global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *counts) {
+  int col = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+  if (col < G.ncol) {
+    const int *zm1 = G.zm1, *zp1 = G.zp1;
+    const int top = G.col_top[col], bot = G.col_bot[col];
+    // new and old surface cells (tracers.c:5739-5755)
+    const int lim = G.nz + 2;  // every column walk is bounded by the layer count
+    int sur = W.nsur_t[col];
+    int c = top, m = zm1[c];
+    for (int it = 0; c != m && G.gridz[c] >= F.eta[top] && it < lim; ++it) {
+      c = m;
+      m = zm1[c];
+    }
+    int nsur = c;
+    W.sur_t[col] = sur;
+    W.nsur_t[col] = nsur;
+    // cells-to-process membership (:5778-5800)
+    int s = sur > nsur ? sur : nsur;
+    int c2 = G.m2d[s];
+    double tz = F.eta[c2] < F.oldeta[c2] ? F.eta[c2] : F.oldeta[c2];
+    double bz = SHOC_TR_DRY_FRAC * O.hmin + G.botz[c2];
+    bool wet = (tz > bz && s != zm1[s]);
+    // thicknesses (:5824-5846)
+    {
+      int cc = sur, c3 = cc;
+      int t2 = G.m2d[c3];
+      double tp = F.oldeta[t2];
+      int it = 0;
+      for (; c3 < bot && it < lim; ++it) {
+        double b = G.gridz[c3];
+        W.dz[c3] = tp - b;
+        tp = b;
+        c3 = zm1[c3];
+      }
+      W.dz[bot] = tp - G.botz[t2];
+      c3 = cc;
+      for (int j = 0; cc > t2 && j < lim; ++j) {
+        cc = zp1[cc];
+        W.dz[cc] = W.dz[c3];
+      }
+      if (it >= lim) atomicOr(W.status, ST_GEOM);
+    }
+    // scheme work arrays over every cell of the column (:530-567)
+    {
+      int cc = top;
+      for (int it = 0; it < lim; ++it) {
+        int zm = zm1[cc];
+        double dzm = W.dz[zm], dzc = W.dz[cc];
+        if (O.trasc == SHOC_TR_QUICKEST) W.w5[cc] = dzm / (dzm + dzc);
+        W.w9[cc] = 0.5 * (dzc + dzm);
+        if (cc == bot) break;
+        cc = zm;
+      }
+      cc = top;
+      for (int it = 0; it < lim; ++it) {
+        int zm = zm1[cc], zp = zp1[cc];
+        double w9c = W.w9[cc];
+        double w9m = (cc == bot) ? 0.0 : W.w9[zm];
+        W.dbz[cc] = 2.0 / (w9m + w9c);
+        W.dfz[cc] = 2.0 / (w9c + W.w9[zp]);
+        if (cc == bot) break;
+        cc = zm;
+      }
+    }
+    int flags = 0;
+    int cbs = 0;
+    if (wet) {
+      flags |= COL_WET;
+      atomicAdd(&counts[0], 1);
+      // sub-step search over this column's cells to process (:591-661)
+      int nc = 0;
+      int cc = s;
+      bool first = true;
+      for (int it = 0; it < lim; ++it) {
+        nc++;
+        if (O.substep) {
+          int xp = G.xp1[cc], yp = G.yp1[cc], zp = zp1[cc];
+          double d4 = 0.5 * (F.u1[cc] + F.u1[xp]);
+          if (fabs(d4) < kMinVal) d4 = kMinVal;
+          double d1 = kSF * fabs(G.h1acell[c2] / d4);
+          if (d1 < dtmin) dtmin = d1;
+          d4 = 0.5 * (F.u2[cc] + F.u2[yp]);
+          if (fabs(d4) < kMinVal) d4 = kMinVal;
+          double d2 = kSF * fabs(G.h2acell[c2] / d4);
+          if (d2 < dtmin) dtmin = d2;
+          if (!first) {
+            d4 = 0.5 * (F.w[cc] + F.w[zp]);
+            if (fabs(d4) < kMinVal) d4 = kMinVal;
+            double d3 = kSF * fabs(W.dz[cc] * 1.0 / d4);
+            if (d3 > 0.0 && d3 < dtmin) dtmin = d3;
+          }
+        }
+        first = false;
+        int nx = zm1[cc];
+        if (nx == zm1[nx]) break;  // next is the sediment cell
+        cc = nx;
+      }
+      atomicAdd(&counts[1], nc);
+      // tr_bounds thin-surface test (:3250-3252)
+      if (s < bot && W.dz[sur] < O.hmin) {
+        flags |= COL_THIN;
+        if (s != top) flags |= COL_SERIAL;
+      }
+      // implicit vertical diffusion set-up (:3841-3889) and LU (:4185-4195)
+      int cs = nsur;
+      int zm = zm1[cs];
+      if (zm == zm1[zm] || !W.dz[zm]) {
+        flags |= COL_SINGLE;
+      } else if (any_vdiff && !W.dz[cs]) {
+        // zero-thickness surface cell: the reference solves over an empty
+        // range and reads stale work memory; report instead of guessing
+        flags |= COL_NOSOLVE;
+        atomicOr(W.status, ST_GEOM);
+      } else if (any_vdiff) {
+        int ca = cs, za = zm;
+        for (int it = 0; ca != za && W.dz[ca] && it < lim; ++it) {
+          ca = za;
+          za = zm1[ca];
+        }
+        cbs = zp1[ca];
+        // dzface(c) = 0.5 (dz[zm1] + dz[c]) for c in [cbs, cs]
+        double dt = F.dt;
+        int cb = cbs;
+        int zpb = zp1[cb];
+        double dzf_p = 0.5 * (W.dz[cb] + W.dz[zpb]);
+        double dzdt = W.dz[cb] / dt;
+        double cp1 = -F.Kz[zpb] / dzf_p;
+        double C = dzdt - cp1;
+        double div = C;
+        W.vd_cm1[cb] = 0.0;
+        W.vd_div[cb] = div;
+        W.vd_ud[cb] = 0.0;
+        W.vd_dzdt[cb] = dzdt;
+        double bp1 = cp1;
+        int cc2 = zpb;
+        for (int it = 0; cc2 != cs && it < lim; ++it) {
+          int zp = zp1[cc2];
+          double dzf_c = dzf_p;
+          dzf_p = 0.5 * (W.dz[cc2] + W.dz[zp]);
+          dzdt = W.dz[cc2] / dt;
+          double cm1 = -F.Kz[cc2] / dzf_c;
+          cp1 = -F.Kz[zp] / dzf_p;
+          C = dzdt - cm1 - cp1;
+          double ud = bp1 / div;
+          div = C - cm1 * ud;
+          if (div == 0.0) atomicOr(W.status, ST_PIVOT);
+          W.vd_cm1[cc2] = cm1;
+          W.vd_div[cc2] = div;
+          W.vd_ud[cc2] = ud;
+          W.vd_dzdt[cc2] = dzdt;
+          bp1 = cp1;
+          cc2 = zp;
+        }
+        {
+          double dzf_c = dzf_p;
+          dzdt = W.dz[cs] / dt;
+          double cm1 = -F.Kz[cs] / dzf_c;
+          C = dzdt - cm1;
+          double ud = bp1 / div;
+          div = C - cm1 * ud;
+          if (div == 0.0) atomicOr(W.status, ST_PIVOT);
+          W.vd_cm1[cs] = cm1;
+          W.vd_div[cs] = div;
+          W.vd_ud[cs] = ud;
+          W.vd_dzdt[cs] = dzdt;
+        }
+      }
+      if (flags & COL_SERIAL) {
+        int i = atomicAdd(W.serial_count, 1);
+        W.serial_list[i] = col;
+      }
+    } else if (col == G.v2col) {
+      atomicOr(W.status, ST_LASTDRY);
+    }
+    ColInfo ci;
+    ci.s = wet ? s : 0;
+    ci.co = sur;
+    ci.cs = nsur;
+    ci.cbs = cbs;
+    ci.flags = flags;
+    W.col[col] = ci;
+  }
+  // block-reduce the sub-step minimum
+  double v = dtmin;
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v < __longlong_as_double(0x7ff0000000000000ll))
+    atomic_min_pos(W.dtm_bits, v);
+}
+
+// Courant numbers of one sub-step over every wet cell (tracers.c:730-736).
+__global__ void k_courant(Geo G, Flow F, Work W, double dtu) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.S; c += gridDim.x * blockDim.x) {
+    if (!(G.cflag[c] & CF_WET)) continue;
+    int c2 = G.m2d[c];
+    W.w6[c] = F.u1[c] * dtu / G.h1au1[c2];
+    W.w7[c] = F.u2[c] * dtu / G.h2au2[c2];
+    W.w8[c] = F.w[c] * dtu / (W.w9[c] * 1.0);
+  }
+}
+
+// Main transport kernel: block = 32 adjacent columns x tw tracers; the tw
+// tracer warps of one block share the columns' per-cell data through L1.
+template <bool LAST>
+__global__ void __launch_bounds__(256) k_transport(Geo G, Flow F, Work W, Opt O, TrSet T,
+                                                   SubStep ss, const double *__restrict__ tr_in,
+                                                   double *__restrict__ tr_out, int tw,
+                                                   int nchunk) {
+  extern __shared__ double sol_s[];
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int tile = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int col = tile * 32 + lane;
+  const int slot = chunk * tw + wy;
+  if (slot >= T.nslot) return;  // warp-uniform
+  bool act = col < G.ncol;
+  if (act && (W.col[col].flags & COL_SERIAL)) act = false;
+  int kb = act ? G.col_kb[col] : G.nz;
+  int kstart = __reduce_min_sync(0xffffffffu, kb);
+  const int n = T.slot_tr[slot];
+  SmemSol sol{sol_s + wy * 32 + lane, tw * 32};
+  bool c3 = false;
+  unsigned long long warn = 0;
+  int stat = 0;
+  column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S, col,
+                    n, kstart, act, sol, c3, warn, stat);
+  unsigned long long wsum = warn;
+  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+  int sor = (int)__reduce_or_sync(0xffffffffu, (unsigned)stat);
+  if (lane == 0) {
+    if (wsum) atomicAdd(W.nwarn, wsum);
+    if (sor) atomicOr(W.status, sor);
+  }
+}
+
+// Columns where tr_bounds' thin-surface cursor can move between tracers:
+// one thread per column, tracers in tbdy order, as the reference loops.
+template <bool LAST>
+__global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
+                         const double *__restrict__ tr_in, double *__restrict__ tr_out) {
+  int cnt = *W.serial_count;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    int col = W.serial_list[i];
+    LocalSol sol;
+    bool c3 = false;
+    unsigned long long warn = 0;
+    int stat = 0;
+    for (int sl = 0; sl < T.nslot; ++sl) {
+      int n = T.slot_tr[sl];
+      column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S,
+                        col, n, G.col_kb[col], true, sol, c3, warn, stat);
+    }
+    if (warn) atomicAdd(W.nwarn, warn);
+    if (stat) atomicOr(W.status, stat);
+  }
+}
+
+// Compensated (Neumaier) FP64 mass sum per tracer over wet cells.
+__global__ void k_mass(Geo G, const double *tr, const double *dz, int ntr, double *out) {
+  int n = blockIdx.y;
+  const double *t = tr + (size_t)n * G.S;
+  double s = 0.0, comp = 0.0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.S; c += gridDim.x * blockDim.x) {
+    if (!(G.cflag[c] & CF_WET)) continue;
+    double v = t[c] * dz[c] * G.cellarea[G.m2d[c]];
+    double u = s + v;
+    comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+    s = u;
+  }
+  s += comp;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) b += part[i];
+    out[(size_t)n * gridDim.x + blockIdx.x] = b;
+  }
+}
+
+int map_status(int st) {
+  if (st & ST_GEOM) return SHOC_TR_EGEOM;
+  if (st & ST_PIVOT) return SHOC_TR_EPIVOT;
+  if (st & ST_NAN) return SHOC_TR_ENAN;
+  if (st & ST_LASTDRY) return SHOC_TR_EUNSUPPORTED;
+  if (st & ST_SCRATCH) return SHOC_TR_ESCRATCH;
+  return SHOC_TR_OK;
+}
+
+int check_geom(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr) {
+  if (!g || !o || ntr < 0) return SHOC_TR_EARG;
+  if (o->trasc != SHOC_TR_QUICKEST && o->trasc != SHOC_TR_VANLEER) return SHOC_TR_EUNSUPPORTED;
+  if (g->v3_t != g->b3_t || g->b3_t != g->a3_t) return SHOC_TR_EUNSUPPORTED;  // OBC / aux cells
+  if (g->v2_t != g->b2_t || g->b2_t != g->a2_t) return SHOC_TR_EUNSUPPORTED;
+  if (g->nz < 1 || g->nz > kSerialMaxLayers) return SHOC_TR_EUNSUPPORTED;
+  if (g->sgsiz < 2 || g->sgsizS < 2 || g->b2_t < 1) return SHOC_TR_EGEOM;
+  const int S = g->sgsiz;
+  std::vector<uint8_t> wet(S, 0);
+  for (int i = 1; i <= g->a3_t; i++) {
+    int c = g->w3_t[i];
+    if (c < 1 || c >= S) return SHOC_TR_EGEOM;
+    wet[c] = 1;
+  }
+  for (int c = 1; c < S; c++) {
+    const int *mp[6] = {g->xp1, g->xm1, g->yp1, g->ym1, g->zp1, g->zm1};
+    for (int q = 0; q < 6; q++)
+      if (mp[q][c] < 0 || mp[q][c] >= S) return SHOC_TR_EGEOM;
+    if (!wet[c]) continue;
+    if (g->m2d[c] < 1 || g->m2d[c] >= g->sgsizS) return SHOC_TR_EGEOM;
+    // the stencil of the neighbouring face reuses this cell's values
+    if (wet[g->xp1[c]] && g->xm1[g->xp1[c]] != c) return SHOC_TR_EGEOM;
+    if (wet[g->yp1[c]] && g->ym1[g->yp1[c]] != c) return SHOC_TR_EGEOM;
+    if (g->zp1[c] != c && g->zm1[g->zp1[c]] != c) return SHOC_TR_EGEOM;
+  }
+  for (int cc = 1; cc <= g->b2_t; cc++) {
+    int top = g->w2_t[cc], bot = g->bot_t[cc];
+    if (top < 1 || top >= g->sgsizS || !wet[top] || bot < 1 || bot >= S || !wet[bot])
+      return SHOC_TR_EGEOM;
+    if (g->zp1[top] != top || g->s2k[top] != g->nz - 1) return SHOC_TR_EGEOM;
+    // bottom reaches the top through zp1 and sits on a self-mapping sediment
+    int sed = g->zm1[bot];
+    if (sed == bot || wet[sed] || g->zm1[sed] != sed || g->zp1[sed] != bot) return SHOC_TR_EGEOM;
+    int c = bot, steps = 0;
+    while (c != top && steps <= g->nz) {
+      c = g->zp1[c];
+      steps++;
+    }
+    if (c != top) return SHOC_TR_EGEOM;
+  }
+  for (int i = 1; i <= g->nbpt; i++)
+    if (g->bpt[i] < 1 || g->bpt[i] >= S || g->bin[i] < 1 || g->bin[i] >= S) return SHOC_TR_EGEOM;
+  return SHOC_TR_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C-ABI
+
+extern "C" {
+
+const char *shoc_tr_gpu_strerror(int st) {
+  switch (st) {
+    case SHOC_TR_OK: return "ok";
+    case SHOC_TR_ESUBSTEP: return "maximum number of tracer sub-steps exceeded";
+    case SHOC_TR_EPIVOT: return "zero pivot in the implicit vertical diffusion solve";
+    case SHOC_TR_ENAN: return "NaN in a tracer after the step";
+    case SHOC_TR_EGEOM: return "geometry fails the layout checks";
+    case SHOC_TR_EUNSUPPORTED: return "unsupported option";
+    case SHOC_TR_ECUDA: return "CUDA runtime error";
+    case SHOC_TR_EARG: return "bad argument";
+    case SHOC_TR_ENOMEM: return "allocation failed";
+    case SHOC_TR_ESCRATCH: return "problem larger than the fixed scratch area";
+  }
+  return "unknown status";
+}
+
+void shoc_tr_gpu_destroy(shoc_tr_gpu *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int i = 0; i < 2; i++)
+    if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
+  for (auto &e : h->ev) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  for (void *p : h->allocs) cudaFree(p);
+  if (h->h_dtm) cudaFreeHost(h->h_dtm);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, int precision,
+                       int device, shoc_tr_gpu **out) {
+  if (!out) return SHOC_TR_EARG;
+  *out = nullptr;
+  int rc = check_geom(g, o, ntr);
+  if (rc) return rc;
+  if (precision != SHOC_TR_FP64) return SHOC_TR_EUNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || device < 0 || device >= ndev)
+    return SHOC_TR_ECUDA;
+  shoc_tr_gpu *h = new shoc_tr_gpu();
+  h->device = device;
+  h->precision = precision;
+  h->ntr = ntr;
+  h->S = g->sgsiz;
+  h->S2 = g->sgsizS;
+  h->nz = g->nz;
+  h->ncol = g->b2_t;
+  h->nbpt = g->nbpt;
+#define TRY(x)                \
+  do {                        \
+    int r_ = (x);             \
+    if (r_) {                 \
+      shoc_tr_gpu_destroy(h); \
+      return r_;              \
+    }                         \
+  } while (0)
+  if (cudaSetDevice(device) != cudaSuccess) TRY(SHOC_TR_ECUDA);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    TRY(SHOC_TR_ECUDA);
+  const int S = h->S, S2 = h->S2, ncol = h->ncol;
+
+  // ---- host precomputation ----
+  std::vector<uint8_t> cflag(S, 0);
+  for (int i = 1; i <= g->a3_t; i++) cflag[g->w3_t[i]] |= CF_WET;
+  for (int i = 1; i <= g->v3_e1; i++) cflag[g->w3_e1[i]] |= CF_E1;
+  for (int i = 1; i <= g->v3_e2; i++) cflag[g->w3_e2[i]] |= CF_E2;
+  std::vector<Face2D> fx(S2), fy(S2);
+  for (int c2 = 1; c2 < S2; c2++) {
+    int xm = g->xm1[c2], xp = g->xp1[c2], ym = g->ym1[c2], yp = g->yp1[c2];
+    if (xm >= S2 || xp >= S2 || ym >= S2 || yp >= S2) continue;  // not a 2D cell
+    Face2D a, b;
+    // d3 / d4 (tracers.c:568-577) and the QUICKEST metric factors (:1862-1864)
+    a.d = g->h1acell[xm] / (g->h1acell[xm] + g->h1acell[c2]);
+    a.db = 2.0 / (g->h1au1[xm] + g->h1au1[c2]);
+    a.df = 2.0 / (g->h1au1[c2] + g->h1au1[xp]);
+    a.hm = g->h1au1[xm];
+    a.h0 = g->h1au1[c2];
+    a.hp = g->h1au1[xp];
+    b.d = g->h2acell[ym] / (g->h2acell[ym] + g->h2acell[c2]);
+    b.db = 2.0 / (g->h2au2[ym] + g->h2au2[c2]);
+    b.df = 2.0 / (g->h2au2[c2] + g->h2au2[yp]);
+    b.hm = g->h2au2[ym];
+    b.h0 = g->h2au2[c2];
+    b.hp = g->h2au2[yp];
+    fx[c2] = a;
+    fy[c2] = b;
+  }
+  std::vector<int> col_top(ncol), col_bot(ncol), col_kb(ncol), sur0(ncol, 0);
+  for (int cc = 1; cc <= ncol; cc++) {
+    col_top[cc - 1] = g->w2_t[cc];
+    col_bot[cc - 1] = g->bot_t[cc];
+    col_kb[cc - 1] = g->s2k[g->bot_t[cc]];
+  }
+
+  // ---- device geometry ----
+  Geo &G = h->G;
+  G.S = S;
+  G.S2 = S2;
+  G.nz = g->nz;
+  G.ncol = ncol;
+  G.v2col = g->v2_t - 1;
+  int *ip;
+  TRY(dupload(h, &ip, g->xp1, S)); G.xp1 = ip;
+  TRY(dupload(h, &ip, g->xm1, S)); G.xm1 = ip;
+  TRY(dupload(h, &ip, g->yp1, S)); G.yp1 = ip;
+  TRY(dupload(h, &ip, g->ym1, S)); G.ym1 = ip;
+  TRY(dupload(h, &ip, g->zp1, S)); G.zp1 = ip;
+  TRY(dupload(h, &ip, g->zm1, S)); G.zm1 = ip;
+  TRY(dupload(h, &ip, g->m2d, S)); G.m2d = ip;
+  uint8_t *u8;
+  TRY(dupload(h, &u8, cflag.data(), S)); G.cflag = u8;
+  TRY(dupload(h, &ip, col_top.data(), ncol)); G.col_top = ip;
+  TRY(dupload(h, &ip, col_bot.data(), ncol)); G.col_bot = ip;
+  TRY(dupload(h, &ip, col_kb.data(), ncol)); G.col_kb = ip;
+  double *dp;
+  TRY(dupload(h, &dp, g->h1au1, S2)); G.h1au1 = dp;
+  TRY(dupload(h, &dp, g->h2au2, S2)); G.h2au2 = dp;
+  TRY(dupload(h, &dp, g->h1au2, S2)); G.h1au2 = dp;
+  TRY(dupload(h, &dp, g->h2au1, S2)); G.h2au1 = dp;
+  TRY(dupload(h, &dp, g->h1acell, S2)); G.h1acell = dp;
+  TRY(dupload(h, &dp, g->h2acell, S2)); G.h2acell = dp;
+  TRY(dupload(h, &dp, g->cellarea, S2)); G.cellarea = dp;
+  TRY(dupload(h, &dp, g->botz, S2)); G.botz = dp;
+  TRY(dupload(h, &dp, g->gridz, S)); G.gridz = dp;
+  Face2D *fp;
+  TRY(dupload(h, &fp, fx.data(), S2)); G.fx = fp;
+  TRY(dupload(h, &fp, fy.data(), S2)); G.fy = fp;
+  if (g->nbpt > 0) {
+    TRY(dupload(h, &h->bpt, g->bpt + 1, g->nbpt));
+    TRY(dupload(h, &h->bin, g->bin + 1, g->nbpt));
+  }
+
+  // ---- options and tracers ----
+  h->O.trasc = o->trasc;
+  h->O.ultimate = o->ultimate;
+  h->O.substep =
+      (o->stab & (SHOC_TR_SUB_STEP | SHOC_TR_SUB_STEP_NOSURF | SHOC_TR_SUB_STEP_TRACER)) ? 1 : 0;
+  h->O.hmin = o->hmin;
+  h->trf.assign(ntr, 0);
+  std::vector<int> slot;
+  for (int i = 0; i < o->ntbdy; i++) {
+    int n = o->tbdy[i];
+    if (n < 0 || n >= ntr) TRY(SHOC_TR_EARG);
+    h->trf[n] |= TR_TBDY;
+    if (o->advect[n]) h->trf[n] |= TR_ADV;
+    if (o->diffuse[n]) {
+      h->trf[n] |= TR_HDIFF;
+      h->any_hdiff = true;
+    }
+    slot.push_back(n);
+  }
+  for (int i = 0; i < o->ntdif_v; i++) {
+    int n = o->tdif_v[i];
+    if (n < 0 || n >= ntr) TRY(SHOC_TR_EARG);
+    h->trf[n] |= TR_VDIFF;
+    h->any_vdiff = true;
+  }
+  for (int n = 0; n < ntr; n++)
+    if (!(h->trf[n] & TR_TBDY)) slot.push_back(n);
+  h->nslot = (int)slot.size();
+  TrSet &T = h->T;
+  T.ntr = ntr;
+  T.nslot = h->nslot;
+  TRY(dupload(h, &ip, slot.data(), slot.size())); T.slot_tr = ip;
+  TRY(dupload(h, &u8, h->trf.data(), ntr)); T.trf = u8;
+  TRY(dupload(h, &dp, o->mintr, ntr)); T.mintr = dp;
+  TRY(dupload(h, &dp, o->maxtr, ntr)); T.maxtr = dp;
+
+  // ---- work arrays ----
+  Work &W = h->W;
+  TRY(dupload<double>(h, &W.dz, nullptr, S));
+  TRY(dupload<double>(h, &W.w5, nullptr, S));
+  TRY(dupload<double>(h, &W.w9, nullptr, S));
+  TRY(dupload<double>(h, &W.dbz, nullptr, S));
+  TRY(dupload<double>(h, &W.dfz, nullptr, S));
+  TRY(dupload<double>(h, &W.w6, nullptr, S));
+  TRY(dupload<double>(h, &W.w7, nullptr, S));
+  TRY(dupload<double>(h, &W.w8, nullptr, S));
+  TRY(dupload<double>(h, &W.vd_cm1, nullptr, S));
+  TRY(dupload<double>(h, &W.vd_div, nullptr, S));
+  TRY(dupload<double>(h, &W.vd_ud, nullptr, S));
+  TRY(dupload<double>(h, &W.vd_dzdt, nullptr, S));
+  TRY(dupload<int>(h, &W.sur_t, nullptr, ncol));
+  TRY(dupload<int>(h, &W.nsur_t, nullptr, ncol));
+  TRY(dupload<ColInfo>(h, &W.col, nullptr, ncol));
+  TRY(dupload<int>(h, &W.status, nullptr, 1));
+  TRY(dupload<unsigned long long>(h, &W.dtm_bits, nullptr, 1));
+  TRY(dupload<unsigned long long>(h, &W.nwarn, nullptr, 1));
+  TRY(dupload<int>(h, &W.serial_list, nullptr, ncol));
+  TRY(dupload<int>(h, &W.serial_count, nullptr, 1));
+  TRY(dupload<int>(h, &h->d_counts, nullptr, 2));
+  for (int b = 0; b < 2; b++) TRY(dupload<double>(h, &h->tr[b], nullptr, (size_t)ntr * S));
+  // flow fields
+  Flow &F = h->F;
+  TRY(dupload<double>(h, (double **)&F.u1, nullptr, S));
+  TRY(dupload<double>(h, (double **)&F.u2, nullptr, S));
+  TRY(dupload<double>(h, (double **)&F.w, nullptr, S));
+  TRY(dupload<double>(h, (double **)&F.u1flux3d, nullptr, S));
+  TRY(dupload<double>(h, (double **)&F.u2flux3d, nullptr, S));
+  TRY(dupload<double>(h, (double **)&F.Kz, nullptr, S));
+  if (h->any_hdiff) {
+    TRY(dupload<double>(h, (double **)&F.dzu1, nullptr, S));
+    TRY(dupload<double>(h, (double **)&F.dzu2, nullptr, S));
+    TRY(dupload<double>(h, (double **)&F.u1kh, nullptr, S));
+    TRY(dupload<double>(h, (double **)&F.u2kh, nullptr, S));
+  }
+  TRY(dupload<double>(h, (double **)&F.eta, nullptr, S2));
+  TRY(dupload<double>(h, (double **)&F.oldeta, nullptr, S2));
+  // pinned readback words
+  void *pin = nullptr;
+  if (cudaHostAlloc(&pin, 64, cudaHostAllocDefault) != cudaSuccess) TRY(SHOC_TR_ENOMEM);
+  h->h_dtm = (unsigned long long *)pin;
+  h->h_status = (int *)((char *)pin + 8);
+  h->h_nwarn = (unsigned long long *)((char *)pin + 16);
+  h->h_counts = (int *)((char *)pin + 24);
+  // tiling: shared memory per block = nz * tw * 32 doubles
+  int tw = 8;
+  while (tw > 1 && (size_t)g->nz * tw * 32 * sizeof(double) > 200 * 1024) tw /= 2;
+  h->tw = tw;
+  if (cudaFuncSetAttribute(k_transport<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           227 * 1024) != cudaSuccess ||
+      cudaFuncSetAttribute(k_transport<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           227 * 1024) != cudaSuccess)
+    TRY(SHOC_TR_ECUDA);
+#undef TRY
+  *out = h;
+  return SHOC_TR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Sub-step schedule from the device minimum (tracers.c:591-668, :715-720).
+int make_schedule(shoc_tr_gpu *h, double dmin, Sched &s) {
+  double dt = h->dt, dtm = dt;
+  if (h->O.substep) {
+    if (dmin < dtm) dtm = dmin;
+    if (dtm != dt) dtm = floor(dtm);
+  }
+  s.dtm = dtm;
+  s.sub.clear();
+  if (dtm == 0.0 || (int)(dt / dtm) > kItermax) return SHOC_TR_ESUBSTEP;
+  double trem = dt, prev_f = 0.0;
+  bool first = true;
+  while (trem > 0) {
+    double dtu = dtm;
+    if (trem < dtu) dtu = trem;
+    if (dtu > 0.0) {
+      SubStep ss;
+      ss.dtu = dtu;
+      ss.trem = trem;
+      ss.subeta_f = 1.0 + (dtu - trem) / dt;
+      ss.osub_f = prev_f;
+      ss.first = first ? 1 : 0;
+      prev_f = ss.subeta_f;
+      first = false;
+      s.sub.push_back(ss);
+    }
+    trem -= dtu;
+  }
+  return SHOC_TR_OK;
+}
+
+int launch_part_a(shoc_tr_gpu *h) {
+  cudaStream_t st = h->stream;
+  k_reset<<<1, 32, 0, st>>>(h->W, h->d_counts);
+  h->launches++;
+  if (h->nbpt > 0) {
+    long long tot = (long long)h->nbpt * h->ntr;
+    int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
+    k_lateral<<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S, h->tr[h->cur],
+                                      h->tr[h->cur ^ 1]);
+    h->launches++;
+  }
+  int nb = (h->ncol + 127) / 128;
+  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->any_vdiff ? 1 : 0, h->d_counts);
+  h->launches++;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
+  cudaStream_t st = h->stream;
+  int cur = cur0;
+  const int nsub = (int)s.sub.size();
+  const int tw = h->tw;
+  const int nchunk = (h->nslot + tw - 1) / tw;
+  const int ntile = (h->ncol + 31) / 32;
+  dim3 blk(32, tw);
+  size_t smem = (size_t)h->nz * tw * 32 * sizeof(double);
+  int cblocks = std::min((h->S + 255) / 256, 148 * 32);
+  for (int i = 0; i < nsub; i++) {
+    const SubStep &ss = s.sub[i];
+    bool last = (i == nsub - 1);
+    k_courant<<<cblocks, 256, 0, st>>>(h->G, h->F, h->W, ss.dtu);
+    h->launches++;
+    const double *tin = h->tr[cur];
+    double *tout = h->tr[cur ^ 1];
+    if (h->nslot > 0) {
+      bool prof = h->profile && last;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (prof) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+      }
+      if (last)
+        k_transport<true><<<ntile * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                            tin, tout, tw, nchunk);
+      else
+        k_transport<false><<<ntile * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                             tin, tout, tw, nchunk);
+      if (prof) {
+        cudaEventRecord(e1, st);
+        h->ev.push_back({e0, e1});
+      }
+      h->launches++;
+      if (last)
+        k_serial<true><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+      else
+        k_serial<false><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+      h->launches++;
+    }
+    cur ^= 1;
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+int read_status(shoc_tr_gpu *h) {
+  CK(cudaMemcpyAsync(h->h_dtm, h->W.dtm_bits, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->h_status, h->W.status, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->h_counts, h->d_counts, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+// One step.  When the schedule is not yet known the step synchronises after
+// k_set_dz to read the sub-step minimum; afterwards steps replay a graph.
+int step_async(shoc_tr_gpu *h) {
+  if (h->probe_left > 0 || !h->have_sched) {
+    int rc = launch_part_a(h);
+    if (rc) return rc;
+    rc = read_status(h);
+    if (rc) return rc;
+    int st = *h->h_status;
+    if (st & (ST_LASTDRY | ST_GEOM)) {
+      h->last_status = map_status(st);
+      return h->last_status;
+    }
+    double dmin;
+    unsigned long long b = *h->h_dtm;
+    memcpy(&dmin, &b, 8);
+    Sched s;
+    rc = make_schedule(h, dmin, s);
+    if (rc) {
+      h->last_status = rc;
+      return rc;
+    }
+    rc = launch_part_b(h, s, h->cur);
+    if (rc) return rc;
+    if (s.sub.size() & 1) h->cur ^= 1;
+    bool same = h->have_sched && s.sub.size() == h->sched.sub.size();
+    if (same)
+      for (size_t i = 0; i < s.sub.size(); i++)
+        if (memcmp(&s.sub[i], &h->sched.sub[i], sizeof(SubStep)) != 0) same = false;
+    if (!same) {
+      for (int i = 0; i < 2; i++)
+        if (h->graph[i]) {
+          cudaGraphExecDestroy(h->graph[i]);
+          h->graph[i] = nullptr;
+        }
+    }
+    h->sched = s;
+    h->have_sched = true;
+    if (h->probe_left > 0) h->probe_left--;
+    return 0;
+  }
+  if (h->profile) {
+    // profiling launches directly so each transport launch is timed
+    int rc = launch_part_a(h);
+    if (rc) return rc;
+    rc = launch_part_b(h, h->sched, h->cur);
+    if (rc) return rc;
+    if (h->sched.sub.size() & 1) h->cur ^= 1;
+    return 0;
+  }
+  int gi = h->cur;
+  if (!h->graph[gi]) {
+    cudaGraph_t graph;
+    long long l0 = h->launches;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_part_a(h);
+    if (!rc) rc = launch_part_b(h, h->sched, h->cur);
+    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+    if (rc) return rc;
+    CK(e);
+    CK(cudaGraphInstantiate(&h->graph[gi], graph, 0));
+    cudaGraphDestroy(graph);
+    h->launches = l0;
+  }
+  CK(cudaGraphLaunch(h->graph[gi], h->stream));
+  h->launches += 2 + (h->nbpt > 0 ? 1 : 0) +
+                 (1 + (h->nslot > 0 ? 2 : 0)) * (long long)h->sched.sub.size();
+  if (h->sched.sub.size() & 1) h->cur ^= 1;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
+  if (!h || !tr_wc) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  for (int n = 0; n < h->ntr; n++) {
+    CK(cudaMemcpyAsync(h->tr[h->cur] + (size_t)n * h->S, tr_wc[n], (size_t)h->S * sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->tr[h->cur ^ 1] + (size_t)n * h->S, tr_wc[n],
+                       (size_t)h->S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  }
+  return 0;
+}
+
+int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc) {
+  if (!h || !tr_wc) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  for (int n = 0; n < h->ntr; n++)
+    CK(cudaMemcpyAsync(tr_wc[n], h->tr[h->cur] + (size_t)n * h->S, (size_t)h->S * sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
+  if (!h || !st) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  const size_t S = (size_t)h->S * sizeof(double), S2 = (size_t)h->S2 * sizeof(double);
+  cudaStream_t s = h->stream;
+  const struct {
+    const double *dst;
+    const double *src;
+    size_t n;
+  } cp[] = {{h->F.u1, st->u1, S},         {h->F.u2, st->u2, S},
+            {h->F.w, st->w, S},           {h->F.u1flux3d, st->u1flux3d, S},
+            {h->F.u2flux3d, st->u2flux3d, S}, {h->F.Kz, st->Kz, S},
+            {h->F.eta, st->eta, S2},      {h->F.oldeta, st->oldeta, S2}};
+  for (auto &x : cp) {
+    if (!x.src) return SHOC_TR_EARG;
+    CK(cudaMemcpyAsync((void *)x.dst, x.src, x.n, cudaMemcpyHostToDevice, s));
+  }
+  if (h->any_hdiff) {
+    if (!st->dzu1 || !st->dzu2 || !st->u1kh || !st->u2kh) return SHOC_TR_EARG;
+    CK(cudaMemcpyAsync((void *)h->F.dzu1, st->dzu1, S, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync((void *)h->F.dzu2, st->dzu2, S, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync((void *)h->F.u1kh, st->u1kh, S, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync((void *)h->F.u2kh, st->u2kh, S, cudaMemcpyHostToDevice, s));
+  }
+  if (st->sur_t && st->nsur_t) {
+    CK(cudaMemcpyAsync(h->W.sur_t, st->sur_t + 1, (size_t)h->ncol * sizeof(int),
+                       cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(h->W.nsur_t, st->nsur_t + 1, (size_t)h->ncol * sizeof(int),
+                       cudaMemcpyHostToDevice, s));
+  }
+  if (st->dt != h->dt) {
+    h->dt = st->dt;
+    h->F.dt = st->dt;
+    for (int i = 0; i < 2; i++)
+      if (h->graph[i]) {
+        cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+      }
+    h->have_sched = false;
+  }
+  h->probe_left = 2;
+  return 0;
+}
+
+int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
+  if (!h) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  if (sur_t)
+    CK(cudaMemcpyAsync(sur_t + 1, h->W.sur_t, (size_t)h->ncol * sizeof(int),
+                       cudaMemcpyDeviceToHost, h->stream));
+  if (nsur_t)
+    CK(cudaMemcpyAsync(nsur_t + 1, h->W.nsur_t, (size_t)h->ncol * sizeof(int),
+                       cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return 0;
+}
+
+int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps) {
+  if (!h || nsteps < 0) return SHOC_TR_EARG;
+  if (h->dt <= 0.0) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  for (int i = 0; i < nsteps; i++) {
+    int rc = step_async(h);
+    if (rc) return rc;
+  }
+  return 0;
+}
+
+int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag) {
+  if (!h) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  CK(cudaMemcpyAsync(h->h_status, h->W.status, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->h_nwarn, h->W.nwarn, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(h->h_counts, h->d_counts, 8, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->W.status, 0, 4, h->stream));
+  CK(cudaMemsetAsync(h->W.nwarn, 0, 8, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  int rc = map_status(*h->h_status);
+  if (!rc) rc = h->last_status;
+  h->last_status = 0;
+  if (diag) {
+    diag->nsub = (int)h->sched.sub.size();
+    diag->dtm = h->sched.dtm;
+    diag->nwarn = (long long)*h->h_nwarn;
+    diag->vcs = h->h_counts[0];
+    diag->vc = h->h_counts[1];
+  }
+  if (h->profile) {
+    for (auto &e : h->ev) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e.first, e.second);
+      h->prof_ms += ms;
+      h->prof_n++;
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+    h->ev.clear();
+  }
+  return rc;
+}
+
+int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag) {
+  if (!h || !st || !st->tr_wc || st->ntr != h->ntr) return SHOC_TR_EARG;
+  int rc = shoc_tr_gpu_set_flow(h, st);
+  if (rc) return rc;
+  rc = shoc_tr_gpu_upload_tracers(h, st->tr_wc);
+  if (rc) return rc;
+  rc = shoc_tr_gpu_run(h, 1);
+  if (rc) {
+    shoc_tr_gpu_sync(h, nullptr);
+    return rc;
+  }
+  rc = shoc_tr_gpu_sync(h, diag);
+  int rc2 = shoc_tr_gpu_download_tracers(h, st->tr_wc);
+  if (!rc) rc = rc2;
+  rc2 = shoc_tr_gpu_get_surface(h, st->sur_t, st->nsur_t);
+  if (!rc) rc = rc2;
+  return rc;
+}
+
+int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
+  if (!h || !mass) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  const int nb = 148 * 2;
+  double *part = nullptr;
+  CK(cudaMallocAsync(&part, (size_t)nb * std::max(h->ntr, 1) * sizeof(double), h->stream));
+  if (h->ntr > 0) {
+    k_mass<<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->tr[h->cur], h->W.dz, h->ntr, part);
+    h->launches++;
+  }
+  std::vector<double> hp((size_t)nb * h->ntr);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaFreeAsync(part, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int n = 0; n < h->ntr; n++) {
+    double s = 0.0, comp = 0.0;
+    for (int b = 0; b < nb; b++) {
+      double v = hp[(size_t)n * nb + b], u = s + v;
+      comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+      s = u;
+    }
+    mass[n] = s + comp;
+  }
+  return 0;
+}
+
+void *shoc_tr_gpu_stream(shoc_tr_gpu *h) { return h ? (void *)h->stream : nullptr; }
+
+int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block) {
+  if (!h) return SHOC_TR_EARG;
+  if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
+  if (tracers_per_block > 0) {
+    if (tracers_per_block > 8 || (size_t)h->nz * tracers_per_block * 32 * sizeof(double) >
+                                     227 * 1024)
+      return SHOC_TR_EUNSUPPORTED;
+    h->tw = tracers_per_block;
+    for (int i = 0; i < 2; i++)
+      if (h->graph[i]) {
+        cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+      }
+  }
+  return 0;
+}
+
+int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable) {
+  if (!h) return SHOC_TR_EARG;
+  h->profile = enable != 0;
+  h->prof_ms = 0.0;
+  h->prof_n = 0;
+  return 0;
+}
+
+int shoc_tr_gpu_kernel_time(shoc_tr_gpu *h, double *ms, int *n) {
+  if (!h) return SHOC_TR_EARG;
+  if (ms) *ms = h->prof_n ? h->prof_ms / h->prof_n : 0.0;
+  if (n) *n = h->prof_n;
+  h->prof_ms = 0.0;
+  h->prof_n = 0;
+  return 0;
+}
+
+long long shoc_tr_gpu_launch_count(shoc_tr_gpu *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+"""Python binding of the C-ABI in include/shoc_tr_gpu.h (libshoc_tr_gpu.so).
+
+This is a thin ctypes layer: every call goes straight to the sm_100a library.
+There is no CPU path -- if the library or a CUDA device is missing, the
+constructor raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libshoc_tr_gpu.so")
+
+FP64 = 0
+FP32_MIXED = 1
+
+# every entry point include/shoc_tr_gpu.h declares
+EXPORTS = (
+    "shoc_tr_gpu_create", "shoc_tr_gpu_destroy", "shoc_tr_gpu_step",
+    "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
+    "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
+    "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_profile",
+    "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_launch_count", "shoc_tr_gpu_strerror",
+)
+
+_lib = None
+
+
+def lib(path=None):
+    """Load the library (built in-tree by __graft_entry__.build())."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise FileNotFoundError(
+            "libshoc_tr_gpu.so not built (%s); run __graft_entry__.build()" % p)
+    L = C.CDLL(p)
+    H = C.c_void_p
+    L.shoc_tr_gpu_create.argtypes = [C.POINTER(_abi.Geom), C.POINTER(_abi.Opts), C.c_int,
+                                     C.c_int, C.c_int, C.POINTER(H)]
+    L.shoc_tr_gpu_destroy.argtypes = [H]
+    L.shoc_tr_gpu_destroy.restype = None
+    L.shoc_tr_gpu_step.argtypes = [H, C.POINTER(_abi.State), C.POINTER(_abi.Diag)]
+    L.shoc_tr_gpu_upload_tracers.argtypes = [H, C.POINTER(_abi.DP)]
+    L.shoc_tr_gpu_download_tracers.argtypes = [H, C.POINTER(_abi.DP)]
+    L.shoc_tr_gpu_set_flow.argtypes = [H, C.POINTER(_abi.State)]
+    L.shoc_tr_gpu_get_surface.argtypes = [H, _abi.IP, _abi.IP]
+    L.shoc_tr_gpu_run.argtypes = [H, C.c_int]
+    L.shoc_tr_gpu_sync.argtypes = [H, C.POINTER(_abi.Diag)]
+    L.shoc_tr_gpu_mass.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_stream.argtypes = [H]
+    L.shoc_tr_gpu_stream.restype = C.c_void_p
+    L.shoc_tr_gpu_set_tiling.argtypes = [H, C.c_int, C.c_int]
+    L.shoc_tr_gpu_profile.argtypes = [H, C.c_int]
+    L.shoc_tr_gpu_kernel_time.argtypes = [H, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.shoc_tr_gpu_launch_count.argtypes = [H]
+    L.shoc_tr_gpu_launch_count.restype = C.c_longlong
+    L.shoc_tr_gpu_strerror.argtypes = [C.c_int]
+    L.shoc_tr_gpu_strerror.restype = C.c_char_p
+    for name in EXPORTS:
+        if name not in ("shoc_tr_gpu_destroy", "shoc_tr_gpu_stream", "shoc_tr_gpu_launch_count",
+                        "shoc_tr_gpu_strerror"):
+            getattr(L, name).restype = C.c_int
+    if path is None:
+        _lib = L
+    return L
+
+
+def _check(where, rc):
+    if rc != 0:
+        raise _abi.StatusError(where, rc)
+
+
+class TracerStep:
+    """One SHOC window's tracer step on a B200 (device-resident tracers).
+
+    Mirrors the reference calls it replaces: ``step()`` is one
+    set_lateral_BC_tr + set_dz + advect_diffuse + vert_diffuse_3d on host
+    arrays (the drop-in), ``run()`` the same on tracers kept in HBM.
+    Failures raise _abi.StatusError with the reference's error meaning
+    (status 1: sub-step limit, tracers.c:664; status 2: zero pivot,
+    tracers.c:4190).
+    """
+
+    def __init__(self, case, precision=FP64, device=0):
+        self.case = case
+        self._keep = []
+        self.L = lib()
+        opts = case.make_opts(self._keep)
+        h = C.c_void_p()
+        _check("shoc_tr_gpu_create",
+               self.L.shoc_tr_gpu_create(C.byref(case.win.geom), C.byref(opts), case.ntr,
+                                         precision, device, C.byref(h)))
+        self.h = h
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.shoc_tr_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- drop-in (host arrays) ------------------------------------------
+    def step(self, tr, sur_t, nsur_t):
+        """One step on host arrays, updated in place; returns the diag."""
+        keep = []
+        st = self.case.make_state(tr, sur_t, nsur_t, keep)
+        d = _abi.Diag()
+        _check("shoc_tr_gpu_step", self.L.shoc_tr_gpu_step(self.h, C.byref(st), C.byref(d)))
+        return d
+
+    # -- device-resident -------------------------------------------------
+    def _rows(self, tr):
+        rows = (_abi.DP * self.case.ntr)(*[tr[n].ctypes.data_as(_abi.DP)
+                                           for n in range(self.case.ntr)])
+        return rows
+
+    def upload(self, tr):
+        assert tr.dtype == np.float64 and tr.flags.c_contiguous
+        _check("upload", self.L.shoc_tr_gpu_upload_tracers(self.h, self._rows(tr)))
+
+    def download(self, out=None):
+        if out is None:
+            out = np.empty((self.case.ntr, self.case.win.sgsiz))
+        _check("download", self.L.shoc_tr_gpu_download_tracers(self.h, self._rows(out)))
+        return out
+
+    def set_flow(self, sur_t=None, nsur_t=None):
+        keep = []
+        c = self.case
+        tr_dummy = np.zeros((c.ntr, 1))
+        st = _abi.State(c.ntr, C.POINTER(_abi.DP)(), _abi.iptr(sur_t), _abi.iptr(nsur_t),
+                        _abi.dptr(c.u1), _abi.dptr(c.u2), _abi.dptr(c.w), _abi.dptr(c.u1flux3d),
+                        _abi.dptr(c.u2flux3d), _abi.dptr(c.Kz), _abi.dptr(c.dzu1),
+                        _abi.dptr(c.dzu2), _abi.dptr(c.u1kh), _abi.dptr(c.u2kh),
+                        _abi.dptr(c.eta), _abi.dptr(c.oldeta), c.dt)
+        keep.append(tr_dummy)
+        _check("set_flow", self.L.shoc_tr_gpu_set_flow(self.h, C.byref(st)))
+
+    def run(self, nsteps):
+        _check("run", self.L.shoc_tr_gpu_run(self.h, int(nsteps)))
+
+    def sync(self):
+        d = _abi.Diag()
+        _check("sync", self.L.shoc_tr_gpu_sync(self.h, C.byref(d)))
+        return d
+
+    def surface(self):
+        g = self.case.win.geom
+        sur = np.zeros(g.b2_t + 1, np.int32)
+        nsur = np.zeros(g.a2_t + 1, np.int32)
+        _check("get_surface", self.L.shoc_tr_gpu_get_surface(self.h, _abi.iptr(sur),
+                                                             _abi.iptr(nsur)))
+        return sur, nsur
+
+    def mass(self):
+        m = np.zeros(self.case.ntr)
+        _check("mass", self.L.shoc_tr_gpu_mass(self.h, _abi.dptr(m)))
+        return m
+
+    def stream(self):
+        return self.L.shoc_tr_gpu_stream(self.h)
+
+    def set_tiling(self, cols=0, tracers=0):
+        _check("set_tiling", self.L.shoc_tr_gpu_set_tiling(self.h, cols, tracers))
+
+    def profile(self, on=True):
+        _check("profile", self.L.shoc_tr_gpu_profile(self.h, 1 if on else 0))
+
+    def kernel_time(self):
+        ms = C.c_double()
+        n = C.c_int()
+        _check("kernel_time", self.L.shoc_tr_gpu_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def launches(self):
+        return int(self.L.shoc_tr_gpu_launch_count(self.h))
+
+    # convenience: the resident path from a case's initial state
+    def start(self, tr=None, sur_t=None, nsur_t=None):
+        c = self.case
+        if tr is None:
+            tr, sur_t, nsur_t = c.copy_state()
+        self.upload(tr)
+        self.set_flow(sur_t, nsur_t)

@@ -74,6 +74,14 @@ def lib():
         L.shoc_grid_init_surface.argtypes = [C.POINTER(_Grid), _abi.DP, _abi.IP, _abi.IP]
         L.shoc_grid_w_from_continuity.argtypes = [
             C.POINTER(_Grid), _abi.IP, _abi.DP, _abi.DP, _abi.DP]
+        L.shoc_synth_flow.argtypes = [C.POINTER(_Grid), _abi.DP, _abi.DP, _abi.DP, C.c_double] + \
+            [_abi.DP] * 6
+        L.shoc_synth_flow.restype = C.c_int
+        L.shoc_synth_kz_exp.argtypes = [C.POINTER(_Grid), C.c_double, C.c_double, _abi.DP]
+        L.shoc_synth_kz_logu.argtypes = [C.POINTER(_Grid), C.c_ulonglong, C.c_double,
+                                         C.c_double, _abi.DP]
+        L.shoc_synth_tracers_logn.argtypes = [C.POINTER(_Grid), C.c_ulonglong, C.c_int,
+                                              C.c_double, C.c_double, _abi.DP, _abi.DP]
         _lib = L
     return _lib
 
@@ -286,61 +294,6 @@ class Case:
         return self.nwet * self.ntr * 2 * s + self.nwet * 5 * s
 
 
-def _flow(win, rng, psi_corner, umax, baroclinic, eta, dt):
-    """Face fluxes / velocities from a corner streamfunction (transport)."""
-    S = win.sgsiz
-    c = win.wet_cells()
-    top = win.cell_top(eta)
-    bot = win.cell_bot()
-    u1flux3d = np.zeros(S)
-    u2flux3d = np.zeros(S)
-    u1 = np.zeros(S)
-    u2 = np.zeros(S)
-    dzu1 = np.zeros(S)
-    dzu2 = np.zeros(S)
-    i, j = win.s2i[c], win.s2j[c]
-    ny, nx = win.ny, win.nx
-    out = []
-    for axis in (0, 1):
-        nb = win.xm1[c] if axis == 0 else win.ym1[c]
-        face = win.is_wet[nb].astype(bool)
-        cf, nbf = c[face], nb[face]
-        fi, fj = i[face], j[face]
-        dz = np.minimum(top[cf], top[nbf]) - np.maximum(bot[cf], bot[nbf])
-        dz = np.maximum(dz, 0.0)
-        fid = fj * (nx + 1) + fi                       # 2D face id
-        D = np.bincount(fid, weights=dz, minlength=(ny + 1) * (nx + 1))
-        if axis == 0:   # west face of (i,j): corners (i,j) and (i,j+1)
-            U = psi_corner[fj + 1, fi] - psi_corner[fj, fi]
-            h2 = win.h2au1[win.m2d[cf]]
-            h1 = win.h1au1[win.m2d[cf]]
-        else:           # south face: corners (i,j) and (i+1,j)
-            U = -(psi_corner[fj, fi + 1] - psi_corner[fj, fi])
-            h2 = win.h1au2[win.m2d[cf]]
-            h1 = win.h2au2[win.m2d[cf]]
-        Df = D[fid]
-        flux = U * dz / Df
-        # baroclinic part with zero depth integral on every face
-        zmid = 0.5 * (np.minimum(top[cf], top[nbf]) + np.maximum(bot[cf], bot[nbf]))
-        q = np.cos(np.pi * zmid / np.maximum(Df, 1e-9))
-        qbar = np.bincount(fid, weights=dz * q, minlength=D.size)[fid] / Df
-        amp = baroclinic[np.minimum(fj, ny - 1), np.minimum(fi, nx - 1)]
-        flux = flux + amp * np.abs(U) / Df * dz * (q - qbar)
-        vel = flux / (dz * h2)
-        out.append((cf, flux, vel, dz, h1))
-    # scale to the requested peak velocity
-    vmax = max(np.abs(o[2]).max() if o[2].size else 0.0 for o in out)
-    s = umax / vmax if vmax > 0 else 0.0
-    (c1, f1, v1, d1, _), (c2, f2, v2, d2, _) = out
-    u1flux3d[c1] = f1 * s
-    u1[c1] = v1 * s
-    dzu1[c1] = d1
-    u2flux3d[c2] = f2 * s
-    u2[c2] = v2 * s
-    dzu2[c2] = d2
-    return u1, u2, u1flux3d, u2flux3d, dzu1, dzu2
-
-
 def _coast_taper(land, width):
     """0 on land and at corners touching land/edge, rising to 1 inland."""
     ny, nx = land.shape
@@ -401,21 +354,30 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
     psi = psi * (0.6 + 0.4 * _smooth(rng, ny + 1, nx + 1, nmodes=5, kmax=3.0))
     psi = psi * _coast_taper(land, width=3)
     bc = baroclinic * (2 * _smooth(rng, ny, nx, nmodes=5, kmax=3.0) - 1)
-    u1, u2, u1flux3d, u2flux3d, dzu1, dzu2 = _flow(win, rng, psi, umax, bc, oldeta, dt)
+    u1, u2, u1flux3d, u2flux3d, dzu1, dzu2 = (np.zeros(S) for _ in range(6))
+    psi = np.ascontiguousarray(psi)
+    bc = np.ascontiguousarray(bc)
+    rc = lib().shoc_synth_flow(C.byref(win._g), dptr(psi), dptr(bc), dptr(oldeta), umax,
+                               dptr(u1), dptr(u2), dptr(u1flux3d), dptr(u2flux3d), dptr(dzu1),
+                               dptr(dzu2))
+    if rc:
+        raise _abi.StatusError("shoc_synth_flow", rc)
     sur_t, _ = win.init_surface(oldeta)
     w = win.w_from_continuity(sur_t, u1flux3d, u2flux3d)
     # vertical diffusivity at bottom faces
     c = win.wet_cells()
     Kz = np.zeros(S)
     if kz[0] == "exp":
-        H = -win.botz[win.m2d[c]]
-        zf = -win.gridz[c]
-        frac = np.clip(zf / H, 0.0, 1.0)
-        Kz[c] = kz[1] * np.exp(np.log(kz[2] / kz[1]) * frac)
+        lib().shoc_synth_kz_exp(C.byref(win._g), kz[1], kz[2], dptr(Kz))
     else:
-        lo, hi = np.log(kz[1]), np.log(kz[2])
-        Kz[c] = np.exp(rng.uniform(lo, hi, c.size))
+        lib().shoc_synth_kz_logu(C.byref(win._g), seed, kz[1], kz[2], dptr(Kz))
     tr = np.zeros((ntr, S))
+    if tracers not in ("gauss", "step"):
+        sm = np.ascontiguousarray(np.stack([_smooth(rng, ny, nx, nmodes=6, kmax=5.0)
+                                            for _ in range(ntr)]))
+        lib().shoc_synth_tracers_logn(C.byref(win._g), seed, ntr, tracers[1], tracers[2],
+                                      dptr(sm), dptr(tr))
+        tracers = "done"
     ii, jj, kk = win.s2i[c], win.s2j[c], win.s2k[c]
     if tracers == "gauss":
         sig = 5.0
@@ -425,14 +387,7 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
     elif tracers == "step":
         for n in range(ntr):
             tr[n, c] = np.where((ii + jj + n) % 7 < 3, 1.0 + n, 0.0)
-    else:
-        lo_mag, hi_mag = tracers[1], tracers[2]
-        for n in range(ntr):
-            mag = lo_mag * (hi_mag / lo_mag) ** (n / max(ntr - 1, 1))
-            sm = _smooth(rng, ny, nx, nmodes=6, kmax=5.0)
-            lg = 1.5 * (sm[jj, ii] - 0.5) + 0.25 * rng.standard_normal(c.size) \
-                + 0.3 * np.cos(np.pi * kk / nz + n)
-            tr[n, c] = mag * np.exp(lg)
+
     # ghost / above-surface values are filled by the step itself
     return Case(name, win, ntr, dt, u1, u2, w, u1flux3d, u2flux3d, Kz, eta, oldeta, tr,
                 trasc=trasc, ultimate=ultimate, stab=stab, hmin=hmin, seed=seed,

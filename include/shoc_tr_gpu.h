@@ -1,0 +1,107 @@
+/*
+ * shoc_tr_gpu.h -- C-ABI of the B200 tracer-transport step for SHOC.
+ *
+ * Replaces, for one window, the calls tracer_step_3d makes between
+ * set_lateral_BC_tr and the auxiliary routines:
+ *
+ *   set_lateral_BC_tr  model/hd/tracers/tracers.c:5574 (called from :159)
+ *   set_dz             model/hd/tracers/tracers.c:5682 (called from
+ *                      model/hd/tracers/transport.c:457 / the 3D mode)
+ *   advect_diffuse     model/hd/tracers/tracers.c:401  (called from :265)
+ *   vert_diffuse_3d    model/hd/tracers/tracers.c:3782 (called from :279)
+ *
+ * with the same inputs (shoc_tr.h mirrors the window structs), the same
+ * results, and the same failures reported as status codes instead of
+ * hd_quit_and_dump: SHOC_TR_ESUBSTEP where tracers.c:664-668 quits,
+ * SHOC_TR_EPIVOT where tracers.c:4190-4193 quits.  There is no CPU path:
+ * without a usable CUDA device every entry point returns SHOC_TR_ECUDA.
+ *
+ * Typical use from the driver (one handle per window, created once):
+ *
+ *   shoc_tr_gpu_create(&geom, &opts, ntr, SHOC_TR_FP64, device, &h);
+ *   each step:  shoc_tr_gpu_step(h, &state, &diag);      // host arrays in/out
+ *
+ * or, keeping tracers resident on the GPU between steps:
+ *
+ *   shoc_tr_gpu_upload_tracers(h, tr_wc);
+ *   shoc_tr_gpu_set_flow(h, &state);       // whenever u/w/Kz/eta change
+ *   shoc_tr_gpu_run(h, nsteps);            // asynchronous on the stream
+ *   shoc_tr_gpu_sync(h, &diag);
+ *   shoc_tr_gpu_download_tracers(h, tr_wc);
+ *
+ * A handle is not thread-safe; each window uses its own handle and stream,
+ * as each dp worker thread owns its window in the reference
+ * (model/hd/control/dp.c:351-359).
+ */
+#ifndef SHOC_TR_GPU_H
+#define SHOC_TR_GPU_H
+
+#include "shoc_tr.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic of the step. */
+#define SHOC_TR_FP64 0        /* plain: FP64 everywhere, matches tracers.c */
+#define SHOC_TR_FP32_MIXED 1  /* FP32 tracers/fluxes/Thomas, FP64 mass sums
+                                 and one FP64-residual refinement per solve */
+
+typedef struct shoc_tr_gpu shoc_tr_gpu;
+
+/* Builds the device copy of the window (maps, lists, metrics) and the
+ * tracer / work buffers.  The geometry arrays are copied; the caller may free
+ * them afterwards.  Replaces the per-window set-up the reference does in
+ * win_consts_init / dp_init (model/hd/master/hd_init.c:244-256). */
+int shoc_tr_gpu_create(const shoc_tr_geom *geom, const shoc_tr_opts *opts,
+                       int ntr, int precision, int device, shoc_tr_gpu **out);
+void shoc_tr_gpu_destroy(shoc_tr_gpu *h);
+
+/* One step on host arrays: copies st's tracers, surface vectors and flow
+ * fields to the device, runs the step, copies tracers and surface vectors
+ * back into st, and waits.  Drop-in for set_lateral_BC_tr + set_dz +
+ * advect_diffuse + vert_diffuse_3d on one window. */
+int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag);
+
+/* Device-resident use. */
+int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc);
+int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc);
+/* Copies flow fields (u1, u2, w, fluxes, Kz, dzu1/dzu2/u1kh/u2kh when any
+ * tracer diffuses horizontally, eta, oldeta, dt) and the surface vectors
+ * sur_t / nsur_t. */
+int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st);
+int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t);
+/* Enqueues nsteps steps on the handle's stream (CUDA-graph replays once the
+ * sub-step schedule is known).  May synchronise once after set_flow to learn
+ * the sub-step count. */
+int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps);
+/* Waits for the stream and returns the first error status raised on the
+ * device since the last sync (and clears it). */
+int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag);
+
+/* Total tracer mass sum(tr * dz * cellarea) over the wet cells of every
+ * tracer, computed in FP64 with compensated (Neumaier) summation. */
+int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
+
+/* cudaStream_t of the handle, for event timing by the caller. */
+void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
+
+/* Launch tuning: columns per block (multiple of 32) and tracers per block.
+ * 0 keeps the current value.  Takes effect at the next step. */
+int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block);
+
+/* Time of the transport kernel per launch, averaged over the launches since
+ * the last call (CUDA events on the handle's stream; enabled by
+ * shoc_tr_gpu_profile(h, 1)). */
+int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable);
+int shoc_tr_gpu_kernel_time(shoc_tr_gpu *h, double *ms_per_launch, int *launches);
+
+/* Counts of kernels this library launched since creation. */
+long long shoc_tr_gpu_launch_count(shoc_tr_gpu *h);
+
+const char *shoc_tr_gpu_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,46 @@
+"""Golden-fixture cases: small seeded windows run through the reference build.
+
+Each entry: name -> (workload, overrides, nsteps).  The same definitions are
+used by make_golden.py (writes the fixtures with the reference's own
+tracers.c, oracle/_ref) and by the tests (check the oracle and the CUDA path
+against them).
+"""
+import hashlib
+
+import numpy as np
+
+from ems_b200 import _abi
+
+MOVING = dict(layers=np.linspace(-30, 2.0, 8))
+
+CASES = {
+    "small_quickest_ultimate": ("small", {}, 10),
+    "small_vanleer": ("small", dict(trasc=_abi.VANLEER, ultimate=0), 10),
+    "small_vanleer_ultimate": ("small", dict(trasc=_abi.VANLEER, ultimate=1), 10),
+    "small_substeps": ("small", dict(dt=2000.0), 2),
+    "small_moving_surface": ("small", dict(eta_offset=(1.9, -1.7), **MOVING), 6),
+    "small_moving_substeps": ("small", dict(eta_offset=(1.9, -1.7), dt=1500.0, **MOVING), 3),
+    "small_clip": ("small", dict(ultimate=0, tracers="step", mintr=[0.0, 0.0, 0.0],
+                                 maxtr=[1.0, 2.0, 2.5]), 20),
+    "small_thin_surface": ("small", dict(eta_offset=(1.9, -1.7), hmin=1.5,
+                                         maxtr=[0.5, 0.5, 0.5], **MOVING), 4),
+    "basin64": ("basin64", {}, 100),
+}
+
+
+def build(name):
+    from ems_b200 import synth
+    wl, kw, nsteps = CASES[name]
+    return synth.make(wl, **kw), nsteps
+
+
+def input_digest(case):
+    """sha256 over every array the step reads, to tell whether a fixture's
+    inputs were regenerated bit for bit on this machine."""
+    h = hashlib.sha256()
+    w = case.win
+    for a in (w.xp1, w.xm1, w.yp1, w.ym1, w.zp1, w.zm1, w.m2d, w.gridz, w.h1au1, w.h2au2,
+              w.h1acell, w.h2acell, w.cellarea, w.botz, case.u1, case.u2, case.w,
+              case.u1flux3d, case.u2flux3d, case.Kz, case.eta, case.oldeta, case.tr):
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
