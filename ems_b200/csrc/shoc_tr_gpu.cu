@@ -405,17 +405,35 @@ __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
   }
 }
 
-// Compensated (Neumaier) FP64 mass sum per tracer over wet cells.
-__global__ void k_mass(Geo G, const double *tr, const double *dz, int ntr, double *out) {
-  int n = blockIdx.y;
+// Compensated (Neumaier) FP64 mass sum per tracer: sum of tr * dz * area
+// over each column from its current surface cell (nsur_t, top at eta) down
+// to the bottom (botz), the water the column holds now.  One thread per
+// (column, tracer); block partials are summed on the host.
+__device__ __forceinline__ void neumaier(double &s, double &comp, double v) {
+  double u = s + v;
+  comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+  s = u;
+}
+
+__global__ void k_mass(Geo G, Flow F, Work W, const double *tr, double *out) {
+  const int n = blockIdx.y;
   const double *t = tr + (size_t)n * G.S;
   double s = 0.0, comp = 0.0;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.S; c += gridDim.x * blockDim.x) {
-    if (!(G.cflag[c] & CF_WET)) continue;
-    double v = t[c] * dz[c] * G.cellarea[G.m2d[c]];
-    double u = s + v;
-    comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
-    s = u;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
+       col += gridDim.x * blockDim.x) {
+    const int top = G.col_top[col], bot = G.col_bot[col];
+    int c = W.nsur_t[col];
+    if (c == G.zm1[c]) continue;  // surface below the bottom: dry
+    const double area = G.cellarea[top];
+    double tz = F.eta[top];
+    for (int it = 0; it <= G.nz; ++it) {
+      double bz = (c == bot) ? G.botz[top] : G.gridz[c];
+      double h = tz - bz;
+      if (h > 0.0) neumaier(s, comp, t[c] * h * area);
+      if (c == bot) break;
+      tz = bz;
+      c = G.zm1[c];
+    }
   }
   s += comp;
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -423,9 +441,9 @@ __global__ void k_mass(Geo G, const double *tr, const double *dz, int ntr, doubl
   if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double b = 0.0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); i++) b += part[i];
-    out[(size_t)n * gridDim.x + blockIdx.x] = b;
+    double b = 0.0, bc = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) neumaier(b, bc, part[i]);
+    out[(size_t)n * gridDim.x + blockIdx.x] = b + bc;
   }
 }
 
@@ -1055,7 +1073,7 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
   double *part = nullptr;
   CK(cudaMallocAsync(&part, (size_t)nb * std::max(h->ntr, 1) * sizeof(double), h->stream));
   if (h->ntr > 0) {
-    k_mass<<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->tr[h->cur], h->W.dz, h->ntr, part);
+    k_mass<<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W, h->tr[h->cur], part);
     h->launches++;
   }
   std::vector<double> hp((size_t)nb * h->ntr);

@@ -79,8 +79,9 @@ int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps);
  * device since the last sync (and clears it). */
 int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag);
 
-/* Total tracer mass sum(tr * dz * cellarea) over the wet cells of every
- * tracer, computed in FP64 with compensated (Neumaier) summation. */
+/* Total tracer mass of every tracer: sum of tr * dz * cellarea over each
+ * column from its current surface cell (top at eta) to the bottom (botz),
+ * accumulated in FP64 with compensated (Neumaier) summation.  mass[ntr]. */
 int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
 
 /* cudaStream_t of the handle, for event timing by the caller. */
