@@ -28,6 +28,7 @@
 
 #include "shoc_tr_gpu.h"
 #include "shoc_tr_kernels.cuh"
+#include "shoc_tr_stage.cuh"
 
 using namespace shoc;
 
@@ -57,7 +58,12 @@ struct shoc_tr_gpu {
   double dt = 0.0;
   // device allocations
   std::vector<void *> allocs;
-  double *tr[2] = {nullptr, nullptr};
+  void *tr[2] = {nullptr, nullptr};   // double (FP64) or float (FP32-mixed)
+  size_t esize = sizeof(double);
+  double *xfer = nullptr;             // one tracer of FP64, for FP32 upload / download
+  Flow32 F3{};
+  f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
+  bool staged = false;                // layer-synchronous fast path
   int cur = 0;
   int *bpt = nullptr, *bin = nullptr;
   // host mirror of the per-tracer flags
@@ -131,14 +137,15 @@ __global__ void k_reset(Work W, int *counts) {
 // Lateral ghosts take their interior value (set_lateral_BC_tr): written into
 // both tracer buffers so the value read during every sub-step, and the value
 // left in the returned array, is the start-of-step one.
-__global__ void k_lateral(int nbpt, const int *bpt, const int *bin, int ntr, int S,
-                          double *tra, double *trb) {
+template <class TR>
+__global__ void k_lateral(int nbpt, const int *bpt, const int *bin, int ntr, int S, TR *tra,
+                          TR *trb) {
   long long tot = (long long)nbpt * ntr;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
        i += (long long)gridDim.x * blockDim.x) {
     int n = (int)(i / nbpt), b = (int)(i % nbpt);
     size_t off = (size_t)n * S;
-    double v = tra[off + bin[b]];
+    TR v = tra[off + bin[b]];
     tra[off + bpt[b]] = v;
     trb[off + bpt[b]] = v;
   }
@@ -149,7 +156,11 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
 }
 
 // One thread per column.
-__global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *counts) {
+// list_all: put every column the staged kernels do not handle on the
+// general-path list (else only the tracer-coupled thin-surface columns).
+// fp32: also write the FP32 thickness and LU factors.
+__global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *counts, int list_all,
+                         int fp32) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   double dtmin = __longlong_as_double(0x7ff0000000000000ll);
   if (col < G.ncol) {
@@ -191,6 +202,14 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
         W.dz[cc] = W.dz[c3];
       }
       if (it >= lim) atomicOr(W.status, ST_GEOM);
+      if (fp32) {
+        int q = top;
+        for (int j = 0; j < lim; ++j) {
+          W.dz32[q] = (float)W.dz[q];
+          if (q == bot) break;
+          q = zm1[q];
+        }
+      }
     }
     // scheme work arrays over every cell of the column (:530-567)
     {
@@ -283,6 +302,7 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
         W.vd_div[cb] = div;
         W.vd_ud[cb] = 0.0;
         W.vd_dzdt[cb] = dzdt;
+        if (fp32) W.lu32[cb] = make_float4((float)dzdt, 0.f, (float)(1.0 / div), 0.f);
         double bp1 = cp1;
         int cc2 = zpb;
         for (int it = 0; cc2 != cs && it < lim; ++it) {
@@ -300,6 +320,8 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
           W.vd_div[cc2] = div;
           W.vd_ud[cc2] = ud;
           W.vd_dzdt[cc2] = dzdt;
+          if (fp32)
+            W.lu32[cc2] = make_float4((float)dzdt, (float)cm1, (float)(1.0 / div), (float)ud);
           bp1 = cp1;
           cc2 = zp;
         }
@@ -315,11 +337,9 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
           W.vd_div[cs] = div;
           W.vd_ud[cs] = ud;
           W.vd_dzdt[cs] = dzdt;
+          if (fp32)
+            W.lu32[cs] = make_float4((float)dzdt, (float)cm1, (float)(1.0 / div), (float)ud);
         }
-      }
-      if (flags & COL_SERIAL) {
-        int i = atomicAdd(W.serial_count, 1);
-        W.serial_list[i] = col;
       }
     } else if (col == G.v2col) {
       atomicOr(W.status, ST_LASTDRY);
@@ -331,6 +351,10 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
     ci.cbs = cbs;
     ci.flags = flags;
     W.col[col] = ci;
+    if ((flags & COL_SERIAL) || (list_all && !staged_column(ci, bot))) {
+      int i = atomicAdd(W.serial_count, 1);
+      W.serial_list[i] = col;
+    }
   }
   // block-reduce the sub-step minimum
   double v = dtmin;
@@ -340,7 +364,10 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
 }
 
 // Courant numbers of one sub-step over every wet cell (tracers.c:730-736).
-__global__ void k_courant(Geo G, Flow F, Work W, double dtu) {
+// only_listed: skip when the general-path list is empty (the staged kernels
+// compute their own Courant numbers).
+__global__ void k_courant(Geo G, Flow F, Work W, double dtu, int only_listed) {
+  if (only_listed && *W.serial_count == 0) return;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.S; c += gridDim.x * blockDim.x) {
     if (!(G.cflag[c] & CF_WET)) continue;
     int c2 = G.m2d[c];
@@ -385,9 +412,9 @@ __global__ void __launch_bounds__(256) k_transport(Geo G, Flow F, Work W, Opt O,
 
 // Columns where tr_bounds' thin-surface cursor can move between tracers:
 // one thread per column, tracers in tbdy order, as the reference loops.
-template <bool LAST>
+template <bool LAST, class TR>
 __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
-                         const double *__restrict__ tr_in, double *__restrict__ tr_out) {
+                         const TR *__restrict__ tr_in, TR *__restrict__ tr_out) {
   int cnt = *W.serial_count;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     int col = W.serial_list[i];
@@ -415,9 +442,31 @@ __device__ __forceinline__ void neumaier(double &s, double &comp, double v) {
   s = u;
 }
 
-__global__ void k_mass(Geo G, Flow F, Work W, const double *tr, double *out) {
+__global__ void k_to_f32(const double *a, float *b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+__global__ void k_to_f64(const float *a, double *b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+// K = dzu h2au1 u1kh / h1au1 (e1) or dzu2 h1au2 u2kh / h2au2 (e2): the
+// tracer-independent factor of hor_diffuse (tracers.c:3660-3666)
+__global__ void k_khfac(Geo G, Flow F, float *khx, float *khy) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < G.S; c += gridDim.x * blockDim.x) {
+    if (!(G.cflag[c] & CF_WET)) continue;
+    int c2 = G.m2d[c];
+    khx[c] = (float)(F.dzu1[c] * G.h2au1[c2] * F.u1kh[c] / G.h1au1[c2]);
+    khy[c] = (float)(F.dzu2[c] * G.h1au2[c2] * F.u2kh[c] / G.h2au2[c2]);
+  }
+}
+
+template <class TR>
+__global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
   const int n = blockIdx.y;
-  const double *t = tr + (size_t)n * G.S;
+  const TR *t = tr + (size_t)n * G.S;
   double s = 0.0, comp = 0.0;
   for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
        col += gridDim.x * blockDim.x) {
@@ -429,7 +478,7 @@ __global__ void k_mass(Geo G, Flow F, Work W, const double *tr, double *out) {
     for (int it = 0; it <= G.nz; ++it) {
       double bz = (c == bot) ? G.botz[top] : G.gridz[c];
       double h = tz - bz;
-      if (h > 0.0) neumaier(s, comp, t[c] * h * area);
+      if (h > 0.0) neumaier(s, comp, (double)t[c] * h * area);
       if (c == bot) break;
       tz = bz;
       c = G.zm1[c];
@@ -445,6 +494,11 @@ __global__ void k_mass(Geo G, Flow F, Work W, const double *tr, double *out) {
     for (int i = 0; i < (int)(blockDim.x >> 5); i++) neumaier(b, bc, part[i]);
     out[(size_t)n * gridDim.x + blockIdx.x] = b + bc;
   }
+}
+
+size_t stage32_smem(int nz, int nw) {
+  return 64 * sizeof(f32::Stage) + (size_t)nz * 32 * sizeof(int) +
+         (size_t)nz * 32 * sizeof(float4) + (size_t)nz * nw * 32 * sizeof(float);
 }
 
 int map_status(int st) {
@@ -546,7 +600,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   *out = nullptr;
   int rc = check_geom(g, o, ntr);
   if (rc) return rc;
-  if (precision != SHOC_TR_FP64) return SHOC_TR_EUNSUPPORTED;
+  if (precision != SHOC_TR_FP64 && precision != SHOC_TR_FP32_MIXED) return SHOC_TR_EUNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || device < 0 || device >= ndev)
     return SHOC_TR_ECUDA;
@@ -702,7 +756,46 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<int>(h, &W.serial_list, nullptr, ncol));
   TRY(dupload<int>(h, &W.serial_count, nullptr, 1));
   TRY(dupload<int>(h, &h->d_counts, nullptr, 2));
-  for (int b = 0; b < 2; b++) TRY(dupload<double>(h, &h->tr[b], nullptr, (size_t)ntr * S));
+  const bool f32p = precision == SHOC_TR_FP32_MIXED;
+  h->esize = f32p ? sizeof(float) : sizeof(double);
+  h->staged = f32p;
+  for (int b = 0; b < 2; b++) {
+    if (f32p) {
+      float *fp = nullptr;
+      TRY(dupload<float>(h, &fp, nullptr, (size_t)ntr * S));
+      h->tr[b] = fp;
+    } else {
+      double *dp2 = nullptr;
+      TRY(dupload<double>(h, &dp2, nullptr, (size_t)ntr * S));
+      h->tr[b] = dp2;
+    }
+  }
+  if (f32p) {
+    TRY(dupload<double>(h, &h->xfer, nullptr, S));
+    TRY(dupload<float>(h, &W.dz32, nullptr, S));
+    TRY(dupload<float4>(h, &W.lu32, nullptr, S));
+    float *fp;
+    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u1 = fp;
+    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u2 = fp;
+    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.w = fp;
+    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u1flux3d = fp;
+    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u2flux3d = fp;
+    if (h->any_hdiff) {
+      TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.khx = fp;
+      TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.khy = fp;
+    }
+    // per-column metric factors of the FP32 face values
+    std::vector<f32::Face2> ax(S2), ay(S2);
+    for (int c2 = 1; c2 < S2; c2++) {
+      const Face2D &a = fx[c2], &b = fy[c2];
+      ax[c2] = {(float)a.d, (float)(a.db * a.hm), (float)(a.db * a.h0), (float)(a.df * a.h0),
+                (float)(a.df * a.hp), a.h0 != 0.0 ? (float)(1.0 / a.h0) : 0.f};
+      ay[c2] = {(float)b.d, (float)(b.db * b.hm), (float)(b.db * b.h0), (float)(b.df * b.h0),
+                (float)(b.df * b.hp), b.h0 != 0.0 ? (float)(1.0 / b.h0) : 0.f};
+    }
+    TRY(dupload(h, &h->fx2, ax.data(), S2));
+    TRY(dupload(h, &h->fy2, ay.data(), S2));
+  }
   // flow fields
   Flow &F = h->F;
   TRY(dupload<double>(h, (double **)&F.u1, nullptr, S));
@@ -726,13 +819,21 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   h->h_status = (int *)((char *)pin + 8);
   h->h_nwarn = (unsigned long long *)((char *)pin + 16);
   h->h_counts = (int *)((char *)pin + 24);
-  // tiling: shared memory per block = nz * tw * 32 doubles
+  // tiling: tracers per block
   int tw = 8;
-  while (tw > 1 && (size_t)g->nz * tw * 32 * sizeof(double) > 200 * 1024) tw /= 2;
+  if (h->staged) {
+    while (tw > 1 && stage32_smem(g->nz, tw) > 112 * 1024) tw--;
+  } else {
+    while (tw > 1 && (size_t)g->nz * tw * 32 * sizeof(double) > 200 * 1024) tw /= 2;
+  }
   h->tw = tw;
   if (cudaFuncSetAttribute(k_transport<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
       cudaFuncSetAttribute(k_transport<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           227 * 1024) != cudaSuccess ||
+      cudaFuncSetAttribute(k_stage32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           227 * 1024) != cudaSuccess ||
+      cudaFuncSetAttribute(k_stage32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess)
     TRY(SHOC_TR_ECUDA);
 #undef TRY
@@ -782,12 +883,18 @@ int launch_part_a(shoc_tr_gpu *h) {
   if (h->nbpt > 0) {
     long long tot = (long long)h->nbpt * h->ntr;
     int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
-    k_lateral<<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S, h->tr[h->cur],
-                                      h->tr[h->cur ^ 1]);
+    if (h->esize == sizeof(float))
+      k_lateral<float><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
+                                               (float *)h->tr[h->cur], (float *)h->tr[h->cur ^ 1]);
+    else
+      k_lateral<double><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
+                                                (double *)h->tr[h->cur],
+                                                (double *)h->tr[h->cur ^ 1]);
     h->launches++;
   }
   int nb = (h->ncol + 127) / 128;
-  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->any_vdiff ? 1 : 0, h->d_counts);
+  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->any_vdiff ? 1 : 0, h->d_counts,
+                               h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0);
   h->launches++;
   CK(cudaGetLastError());
   return 0;
@@ -806,10 +913,44 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
   for (int i = 0; i < nsub; i++) {
     const SubStep &ss = s.sub[i];
     bool last = (i == nsub - 1);
-    k_courant<<<cblocks, 256, 0, st>>>(h->G, h->F, h->W, ss.dtu);
+    k_courant<<<cblocks, 256, 0, st>>>(h->G, h->F, h->W, ss.dtu, h->staged ? 1 : 0);
     h->launches++;
-    const double *tin = h->tr[cur];
-    double *tout = h->tr[cur ^ 1];
+    if (h->staged && h->nslot > 0) {
+      const float *tin = (const float *)h->tr[cur];
+      float *tout = (float *)h->tr[cur ^ 1];
+      const int nw = tw;
+      size_t smem32 = stage32_smem(h->nz, nw);
+      dim3 blk32(32, nw);
+      bool prof = h->profile && last;
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (prof) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, st);
+      }
+      if (last)
+        k_stage32<true><<<ntile * nchunk, blk32, smem32, st>>>(
+            h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2, tin, tout, nw, nchunk,
+            h->any_hdiff ? 1 : 0);
+      else
+        k_stage32<false><<<ntile * nchunk, blk32, smem32, st>>>(
+            h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2, tin, tout, nw, nchunk,
+            h->any_hdiff ? 1 : 0);
+      if (prof) {
+        cudaEventRecord(e1, st);
+        h->ev.push_back({e0, e1});
+      }
+      h->launches++;
+      if (last)
+        k_serial<true, float><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+      else
+        k_serial<false, float><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+      h->launches++;
+      cur ^= 1;
+      continue;
+    }
+    const double *tin = (const double *)h->tr[cur];
+    double *tout = (double *)h->tr[cur ^ 1];
     if (h->nslot > 0) {
       bool prof = h->profile && last;
       cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -830,9 +971,9 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
       }
       h->launches++;
       if (last)
-        k_serial<true><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<true, double><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
       else
-        k_serial<false><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<false, double><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
       h->launches++;
     }
     cur ^= 1;
@@ -927,11 +1068,20 @@ extern "C" {
 int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
   if (!h || !tr_wc) return SHOC_TR_EARG;
   cudaSetDevice(h->device);
+  const size_t S = (size_t)h->S;
   for (int n = 0; n < h->ntr; n++) {
-    CK(cudaMemcpyAsync(h->tr[h->cur] + (size_t)n * h->S, tr_wc[n], (size_t)h->S * sizeof(double),
-                       cudaMemcpyHostToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->tr[h->cur ^ 1] + (size_t)n * h->S, tr_wc[n],
-                       (size_t)h->S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (h->esize == sizeof(double)) {
+      double *a = (double *)h->tr[h->cur] + n * S, *b = (double *)h->tr[h->cur ^ 1] + n * S;
+      CK(cudaMemcpyAsync(a, tr_wc[n], S * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+      CK(cudaMemcpyAsync(b, a, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+      float *a = (float *)h->tr[h->cur] + n * S, *b = (float *)h->tr[h->cur ^ 1] + n * S;
+      CK(cudaMemcpyAsync(h->xfer, tr_wc[n], S * sizeof(double), cudaMemcpyHostToDevice,
+                         h->stream));
+      k_to_f32<<<592, 256, 0, h->stream>>>(h->xfer, a, S);
+      h->launches++;
+      CK(cudaMemcpyAsync(b, a, S * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    }
   }
   return 0;
 }
@@ -939,9 +1089,18 @@ int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
 int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc) {
   if (!h || !tr_wc) return SHOC_TR_EARG;
   cudaSetDevice(h->device);
-  for (int n = 0; n < h->ntr; n++)
-    CK(cudaMemcpyAsync(tr_wc[n], h->tr[h->cur] + (size_t)n * h->S, (size_t)h->S * sizeof(double),
-                       cudaMemcpyDeviceToHost, h->stream));
+  const size_t S = (size_t)h->S;
+  for (int n = 0; n < h->ntr; n++) {
+    if (h->esize == sizeof(double)) {
+      CK(cudaMemcpyAsync(tr_wc[n], (double *)h->tr[h->cur] + n * S, S * sizeof(double),
+                         cudaMemcpyDeviceToHost, h->stream));
+    } else {
+      k_to_f64<<<592, 256, 0, h->stream>>>((float *)h->tr[h->cur] + n * S, h->xfer, S);
+      h->launches++;
+      CK(cudaMemcpyAsync(tr_wc[n], h->xfer, S * sizeof(double), cudaMemcpyDeviceToHost,
+                         h->stream));
+    }
+  }
   CK(cudaStreamSynchronize(h->stream));
   return 0;
 }
@@ -969,6 +1128,20 @@ int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
     CK(cudaMemcpyAsync((void *)h->F.dzu2, st->dzu2, S, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync((void *)h->F.u1kh, st->u1kh, S, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync((void *)h->F.u2kh, st->u2kh, S, cudaMemcpyHostToDevice, s));
+  }
+  if (h->esize == sizeof(float)) {
+    const size_t n = (size_t)h->S;
+    k_to_f32<<<592, 256, 0, s>>>(h->F.u1, (float *)h->F3.u1, n);
+    k_to_f32<<<592, 256, 0, s>>>(h->F.u2, (float *)h->F3.u2, n);
+    k_to_f32<<<592, 256, 0, s>>>(h->F.w, (float *)h->F3.w, n);
+    k_to_f32<<<592, 256, 0, s>>>(h->F.u1flux3d, (float *)h->F3.u1flux3d, n);
+    k_to_f32<<<592, 256, 0, s>>>(h->F.u2flux3d, (float *)h->F3.u2flux3d, n);
+    h->launches += 5;
+    if (h->any_hdiff) {
+      k_khfac<<<592, 256, 0, s>>>(h->G, h->F, (float *)h->F3.khx, (float *)h->F3.khy);
+      h->launches++;
+    }
+    CK(cudaGetLastError());
   }
   if (st->sur_t && st->nsur_t) {
     CK(cudaMemcpyAsync(h->W.sur_t, st->sur_t + 1, (size_t)h->ncol * sizeof(int),
@@ -1073,7 +1246,12 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
   double *part = nullptr;
   CK(cudaMallocAsync(&part, (size_t)nb * std::max(h->ntr, 1) * sizeof(double), h->stream));
   if (h->ntr > 0) {
-    k_mass<<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W, h->tr[h->cur], part);
+    if (h->esize == sizeof(float))
+      k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W,
+                                                             (const float *)h->tr[h->cur], part);
+    else
+      k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W,
+                                                              (const double *)h->tr[h->cur], part);
     h->launches++;
   }
   std::vector<double> hp((size_t)nb * h->ntr);
@@ -1099,8 +1277,10 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
   if (!h) return SHOC_TR_EARG;
   if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
   if (tracers_per_block > 0) {
-    if (tracers_per_block > 8 || (size_t)h->nz * tracers_per_block * 32 * sizeof(double) >
-                                     227 * 1024)
+    if (tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
+    if (h->staged && stage32_smem(h->nz, tracers_per_block) > 227 * 1024)
+      return SHOC_TR_EUNSUPPORTED;
+    if (!h->staged && (size_t)h->nz * tracers_per_block * 32 * sizeof(double) > 227 * 1024)
       return SHOC_TR_EUNSUPPORTED;
     h->tw = tracers_per_block;
     for (int i = 0; i < 2; i++)

@@ -86,6 +86,15 @@ struct Work {
   unsigned long long *dtm_bits;
   unsigned long long *nwarn;
   int *serial_list, *serial_count;
+  // FP32-mixed path: layer thickness and LU factors {dzdt, cm1, 1/div, ud}
+  float *dz32;
+  float4 *lu32;
+};
+
+// FP32 copies of the flow fields (FP32-mixed path), made by set_flow.
+struct Flow32 {
+  const float *u1, *u2, *w, *u1flux3d, *u2flux3d;
+  const float *khx, *khy;  // dzu1 h2au1 u1kh / h1au1 and the e2 analogue
 };
 
 struct Opt {
@@ -284,12 +293,13 @@ struct LocalSol {
 // their loads coalesce; a lane acts once k reaches its own bottom layer.
 // c3_moved carries tr_bounds' thin-surface cursor between tracers of one
 // column (tracers.c:3250-3270 does not reset it); the main kernel only runs
-// columns where the cursor cannot move.
-template <bool LAST, class Sol>
+// columns where the cursor cannot move.  TR is the tracer storage type
+// (double, or float for the FP32-mixed path); arithmetic is FP64 either way.
+template <bool LAST, class Sol, class TR>
 __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const Work &W,
                                             const Opt &O, const TrSet &T, const SubStep &ss,
-                                            const double *__restrict__ tri,
-                                            double *__restrict__ tro, int col, int n, int kstart,
+                                            const TR *__restrict__ tri,
+                                            TR *__restrict__ tro, int col, int n, int kstart,
                                             bool act, Sol &sol, bool &c3_moved,
                                             unsigned long long &warn, int &stat) {
   ColInfo ci = {0, 0, 0, 0, 0};
@@ -344,7 +354,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       w9p = W.w9[czp1];
       w9pp = W.w9[czp2];
       int sed = G.zm1[c];
-      tro[sed] = tbdy ? t0 : tri[sed];
+      tro[sed] = (TR)(tbdy ? t0 : tri[sed]);
     } else {
       c = czp1;
       czp1 = czp2;
@@ -361,7 +371,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
     }
     if (c == cs) k_cs = k;
     if (!upd) {
-      tro[c] = t0;
+      tro[c] = (TR)(t0);
       if (vd && c <= cbs && c >= cs) {
         double dzdt = W.vd_dzdt[c];
         double rhs = dzdt * t0;
@@ -406,7 +416,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       // tr_bounds clip and range check (:3278-3293)
       if (mn <= kClipEps && a < mn) a = mn;
       if (a < mn || a > mx) warn++;
-      tro[c] = a;
+      tro[c] = (TR)(a);
       if (vd && c <= cbs && c >= cs) {
         double dzdt = W.vd_dzdt[c];
         double rhs = dzdt * a;
@@ -453,12 +463,12 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       // one-layer column (tracers.c:4125-4132): max(dzcell, hmin)
       double h = W.dz[cs] > O.hmin ? W.dz[cs] : O.hmin;
       double v = tro[cs];
-      tro[cs] = v + F.dt * (0.0 - 0.0) / h;
+      tro[cs] = (TR)(v + F.dt * (0.0 - 0.0) / h);
     } else if (act && vd) {
       double x = sol.at(k_cs);
       double a = tro[cs];
       double fin = a + (x - a) * 1.0;
-      tro[cs] = fin;
+      tro[cs] = (TR)(fin);
       if (isnan(fin)) stat |= ST_NAN;
       double udp = W.vd_ud[cs];
       int cc = cs, k = k_cs;
@@ -468,7 +478,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
         x = sol.at(k) - udp * x;
         a = tro[cc];
         fin = a + (x - a) * 1.0;
-        tro[cc] = fin;
+        tro[cc] = (TR)(fin);
         if (isnan(fin)) stat |= ST_NAN;
         udp = W.vd_ud[cc];
       }
@@ -495,16 +505,16 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
   // surface and the cells above it (:3309-3323)
   {
     int cc = s;
-    tro[cc] = vs;
+    tro[cc] = (TR)(vs);
     for (int it = 0; cc != ctop && it < G.nz; ++it) {
       cc = G.zp1[cc];
-      tro[cc] = vs;
+      tro[cc] = (TR)(vs);
     }
   }
   if (!vdf) return;
   if (ci.flags & COL_SINGLE) {
     double h = W.dz[cs] > O.hmin ? W.dz[cs] : O.hmin;
-    tro[cs] = vs + F.dt * (0.0 - 0.0) / h;
+    tro[cs] = (TR)(vs + F.dt * (0.0 - 0.0) / h);
     return;
   }
   // Thomas forward over the surface cell and the cells above it up to cs
@@ -535,7 +545,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
     double x = sol.at(k_cs);
     double a = (cs > s) ? tro[cs] : vs;
     double fin = a + (x - a) * 1.0;
-    tro[cs] = fin;
+    tro[cs] = (TR)(fin);
     if (isnan(fin)) stat |= ST_NAN;
     double udp = W.vd_ud[cs];
     int cc = cs, k = k_cs;
@@ -545,7 +555,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       x = sol.at(k) - udp * x;
       a = (cc > s) ? tro[cc] : vs;
       fin = a + (x - a) * 1.0;
-      tro[cc] = fin;
+      tro[cc] = (TR)(fin);
       if (isnan(fin)) stat |= ST_NAN;
       udp = W.vd_ud[cc];
     }

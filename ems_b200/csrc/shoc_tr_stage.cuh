@@ -1,0 +1,579 @@
+// shoc_tr_stage.cuh -- layer-synchronous transport kernels (the fast path).
+//
+// A block owns 32 adjacent wet columns (one per lane) and NW tracers (one
+// per warp).  All warps walk the columns' layers together, bottom to top.
+// Everything that does not depend on the tracer -- the cell and its
+// neighbours' sparse indices, Courant numbers, face coefficients, layer
+// thickness, the implicit solve's LU factors -- is staged for the 32 cells of
+// the next layer into shared memory while the tracer warps work on the
+// current one (double buffer, one __syncthreads per layer).  Tracer warps
+// then only issue the loads of their own tracer's stencil values; the values
+// of x-neighbours that are lanes of the same warp come through shuffles, and
+// so does the flux through the east face (the west face of the next lane).
+// The flux divergence of cell k is finished one layer late, once the flux
+// through its top face (the bottom face of cell k+1) is known.
+//
+// Columns whose free surface crosses a layer face during the step, whose
+// tr_bounds thin-surface cursor couples tracers, or whose implicit solve is
+// degenerate go through the general column path (column_pass) instead.
+#pragma once
+#include "shoc_tr_kernels.cuh"
+
+namespace shoc {
+
+// Columns the staged kernels handle: wet, surface cell unchanged this step
+// (s == co == cs), implicit solve spanning the whole column (or one layer).
+__device__ __forceinline__ bool staged_column(const ColInfo &ci, int cbot) {
+  if (!(ci.flags & COL_WET)) return false;
+  if (ci.flags & (COL_SERIAL | COL_NOSOLVE)) return false;
+  if (ci.s != ci.co || ci.s != ci.cs) return false;
+  if (!(ci.flags & COL_SINGLE) && ci.cbs != cbot) return false;
+  return true;
+}
+
+constexpr int SH_XM1 = 1, SH_XM2 = 2, SH_XP1 = 4, SH_XP2 = 8;
+
+// ===========================================================================
+// FP32-mixed policy: FP32 tracers, face values and Thomas sweeps; FP64 flux
+// divergence, surface column-mass sum (Neumaier), implicit-solve residual and
+// one refinement step.
+
+namespace f32 {
+
+// F = tm1 + a (t0 - tm1) - b curv,   curv = A tX + B tY - 2 tZ
+// (the QUICKEST face value of quickest(), tracers.c:1870-1884, with the
+// tracer-independent factors folded: a = d - cr/2, b = (1 - cr^2)/6, A/B the
+// metric-weighted curvature factors of the upwind side), then ULTIMATE with
+// ircr = 1/|cr|, times the volume flux U, minus K (t0 - tm1) for horizontal
+// diffusion.  Van Leer uses a = 0.5 (1 -+ cr) and the flux-limiter form.
+struct Face {
+  float a, b, A, B, ircr, U, K;
+  int mode;
+};
+constexpr int FM_POS = 1, FM_NEG = 2, FM_ULT = 4, FM_ON = 8, FM_HD = 16;
+
+struct Stage {
+  int c, zp1;
+  int xm1, xm2, xp1, xp2, ym1, ym2, yp1, yp2;
+  int share;
+  int pad;
+  Face fxw, fxe, fys, fyn, fzb;
+  double idz;
+};
+
+// per-column metric factors of one horizontal direction (precomputed once)
+struct Face2 {
+  float d, Ap, Bp, Am, Bm;  // A+/B+ = db*hm, db*h0; A-/B- = df*h0, df*hp
+  float ih;                 // 1 / h1au1 (x) or 1 / h2au2 (y) of the face's column
+};
+
+__device__ __forceinline__ void set_face_h(Face &f, bool on, float cr, const Face2 &m, float U,
+                                           bool ult, int trasc, float K, bool hd) {
+  f.mode = 0;
+  if (!on) return;
+  f.mode = FM_ON | (cr > 0.f ? FM_POS : 0) | (cr < 0.f ? FM_NEG : 0) | (ult ? FM_ULT : 0) |
+           (hd ? FM_HD : 0);
+  if (trasc == SHOC_TR_QUICKEST) {
+    f.a = m.d - 0.5f * cr;
+    f.b = (1.f - cr * cr) * (1.f / 6.f);
+    if (cr > 0.f) {
+      f.A = m.Ap;
+      f.B = m.Bp;
+    } else {
+      f.A = m.Am;
+      f.B = m.Bm;
+    }
+  } else {
+    f.a = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
+    f.b = 0.f;
+    f.A = f.B = 0.f;
+  }
+  f.ircr = cr != 0.f ? 1.f / fabsf(cr) : 0.f;
+  f.U = U;
+  f.K = K;
+}
+
+// one face value: tm2..tp1 at i-2..i+1 of the face's cell
+__device__ __forceinline__ float face(const Face &f, int trasc, bool adv, bool hd, float tm2,
+                                      float tm1, float t0, float tp1) {
+  const int md = f.mode;
+  if (!(md & FM_ON)) return 0.f;
+  float F = 0.f;
+  if (!adv) {
+  } else if (trasc == SHOC_TR_QUICKEST) {
+    float curv = 0.f;
+    if (md & FM_POS)
+      curv = f.A * t0 + f.B * tm2 - 2.f * tm1;
+    else if (md & FM_NEG)
+      curv = f.A * tp1 + f.B * tm1 - 2.f * t0;
+    F = tm1 + f.a * (t0 - tm1) - f.b * curv;
+  } else if (md & FM_POS) {
+    float df = (tm1 - tm2) * (t0 - tm1);
+    df = df > 0.f ? 2.f * __fdividef(df, t0 - tm2) : 0.f;
+    F = tm1 + f.a * df;
+  } else if (md & FM_NEG) {
+    float df = (t0 - tm1) * (tp1 - t0);
+    df = df > 0.f ? 2.f * __fdividef(df, tp1 - tm1) : 0.f;
+    F = t0 - f.a * df;
+  }
+  if (adv && (md & FM_ULT) && (md & (FM_POS | FM_NEG))) {
+    float tc, tu, td;
+    if (md & FM_POS) {
+      tc = tm1;
+      tu = tm2;
+      td = t0;
+    } else {
+      tc = t0;
+      tu = tp1;
+      td = tm1;
+    }
+    const float diff = td - tu;
+    float nc = 0.f, nu = 0.f;
+    if (diff != 0.f) {
+      const float r = __frcp_rn(diff);
+      nc = (tc - tu) * r;
+      nu = (F - tu) * r;
+    }
+    if (nc >= 0.f && nc <= 1.f) {
+      if (nu > 1.f)
+        F = td;
+      else if (nu < nc)
+        F = tu + nc * diff;
+      else if (nu > nc * f.ircr)
+        F = tu + nc * diff * f.ircr;
+    } else {
+      F = tu + nc * diff;
+    }
+  }
+  F *= f.U;
+  if (hd && (md & FM_HD)) F -= f.K * (t0 - tm1);
+  return F;
+}
+
+// ---------------------------------------------------------------------------
+// Staging of one layer (FP32 policy).  part: 0 indices, 1 x faces, 2 y faces,
+// 3 z face, thickness and LU factors.  Every part walks its lane's column.
+
+struct Walk {   // per-lane column walk of one staging part
+  int c;        // cell at the current layer (0 when not started / inactive)
+  float dzm2, dzm1, dz0;  // thickness window of part 3
+};
+
+__device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, int kb, int ks,
+                                           int cbot, int c2, const Geo &G, const Flow32 &F3,
+                                           const Work &W, const Opt &O, bool any_hd,
+                                           double dtu, const Face2 *fx2, const Face2 *fy2,
+                                           Stage *st, int *colC, float4 *colLU, Walk &wk) {
+  const bool on = act && k >= kb;
+  int c = 0;
+  if (on) c = (k == kb) ? cbot : G.zp1[wk.c];
+  wk.c = c;
+  Stage &S = st[lane];
+  const float fdtu = (float)dtu;
+  if (part == 0) {
+    int zp1 = 0, xm1 = 0, xp1 = 0, ym1 = 0, yp1 = 0, xm2 = 0, xp2 = 0, ym2 = 0, yp2 = 0;
+    if (on) {
+      zp1 = G.zp1[c];
+      xm1 = G.xm1[c];
+      xp1 = G.xp1[c];
+      ym1 = G.ym1[c];
+      yp1 = G.yp1[c];
+      xm2 = G.xm1[xm1];
+      xp2 = G.xp1[xp1];
+      ym2 = G.ym1[ym1];
+      yp2 = G.yp1[yp1];
+    }
+    const int cu1 = __shfl_up_sync(0xffffffffu, c, 1), cu2 = __shfl_up_sync(0xffffffffu, c, 2);
+    const int cd1 = __shfl_down_sync(0xffffffffu, c, 1), cd2 = __shfl_down_sync(0xffffffffu, c, 2);
+    int sh = 0;
+    if (on) {
+      if (lane >= 1 && cu1 && xm1 == cu1) sh |= SH_XM1;
+      if (lane >= 2 && cu2 && xm2 == cu2) sh |= SH_XM2;
+      if (lane <= 30 && cd1 && xp1 == cd1) sh |= SH_XP1;
+      if (lane <= 29 && cd2 && xp2 == cd2) sh |= SH_XP2;
+    }
+    S.c = c;
+    S.zp1 = zp1;
+    S.xm1 = xm1; S.xm2 = xm2; S.xp1 = xp1; S.xp2 = xp2;
+    S.ym1 = ym1; S.ym2 = ym2; S.yp1 = yp1; S.yp2 = yp2;
+    S.share = sh;
+    colC[k * 32 + lane] = c;
+  } else if (part == 1 || part == 2) {
+    const bool x = part == 1;
+    Face &fw = x ? S.fxw : S.fys;
+    Face &fe = x ? S.fxe : S.fyn;
+    if (!on) {
+      fw.mode = 0;
+      fe.mode = 0;
+      return;
+    }
+    const uint8_t EB = x ? CF_E1 : CF_E2;
+    const float *vel = x ? F3.u1 : F3.u2;
+    const float *flx = x ? F3.u1flux3d : F3.u2flux3d;
+    const float *kh = x ? F3.khx : F3.khy;
+    const Face2 *m2 = x ? fx2 : fy2;
+    const uint8_t fc = G.cflag[c];
+    const bool quick = O.trasc == SHOC_TR_QUICKEST;
+    const Face2 mw = m2[c2];
+    const float crw = vel[c] * fdtu * mw.ih;
+    set_face_h(fw, quick ? true : (fc & EB) != 0, crw, mw, flx[c], O.ultimate && (fc & EB),
+               O.trasc, any_hd ? kh[c] : 0.f, any_hd);
+    const int cp = x ? G.xp1[c] : G.yp1[c];
+    const uint8_t fp = G.cflag[cp];
+    if (fp & CF_WET) {
+      const Face2 me = m2[G.m2d[cp]];
+      const float cre = vel[cp] * fdtu * me.ih;
+      set_face_h(fe, quick ? true : (fp & EB) != 0, cre, me, flx[cp], O.ultimate && (fp & EB),
+                 O.trasc, any_hd ? kh[cp] : 0.f, any_hd);
+    } else {
+      fe.mode = 0;
+    }
+  } else {
+    Face &fz = S.fzb;
+    if (!on) {
+      fz.mode = 0;
+      return;
+    }
+    const int zp1 = G.zp1[c];
+    if (k == kb) {
+      wk.dzm2 = 0.f;  // thickness of the sediment cell (never set by set_dz)
+      wk.dzm1 = 0.f;
+      wk.dz0 = W.dz32[c];
+    } else {
+      wk.dzm2 = wk.dzm1;
+      wk.dzm1 = wk.dz0;
+      wk.dz0 = W.dz32[c];
+    }
+    const float dzp1 = W.dz32[zp1];
+    S.idz = 1.0 / (double)wk.dz0;
+    if (k <= ks) {  // the cell is one of the cells to process: it has a z face
+      const float w9m = 0.5f * (wk.dzm1 + wk.dzm2);
+      const float w90 = 0.5f * (wk.dz0 + wk.dzm1);
+      const float w9p = 0.5f * (dzp1 + wk.dz0);
+      const float wv = F3.w[c] * fdtu;
+      const float cz = wv / w90;
+      fz.mode = FM_ON | (cz > 0.f ? FM_POS : 0) | (cz < 0.f ? FM_NEG : 0) |
+                (O.ultimate ? FM_ULT : 0);
+      if (O.trasc == SHOC_TR_QUICKEST) {
+        fz.a = wk.dzm1 / (wk.dzm1 + wk.dz0) - 0.5f * cz;
+        fz.b = (1.f - cz * cz) * (1.f / 6.f);
+        if (cz > 0.f) {
+          const float db = 2.f / (w9m + w90);
+          fz.A = db * w9m;
+          fz.B = db * w90;
+        } else {
+          const float df = 2.f / (w90 + w9p);
+          fz.A = df * w90;
+          fz.B = df * w9p;
+        }
+      } else {
+        fz.a = cz > 0.f ? 0.5f * (1.f - cz) : 0.5f * (1.f + cz);
+        fz.b = fz.A = fz.B = 0.f;
+      }
+      fz.ircr = cz != 0.f ? 1.f / fabsf(cz) : 0.f;
+      fz.U = wv;
+      fz.K = 0.f;
+    } else {
+      fz.mode = 0;
+    }
+    colLU[k * 32 + lane] = (k <= ks) ? W.lu32[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+__device__ __forceinline__ void neumaier_add(double &s, double &comp, double v) {
+  double u = s + v;
+  comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+  s = u;
+}
+
+}  // namespace f32
+
+// ---------------------------------------------------------------------------
+// The FP32-mixed staged transport kernel.
+//
+// Shared memory: Stage[2][32] | int colC[nz][32] | float4 colLU[nz][32] |
+// float Sv[nz][nw][32] (per tracer-lane Thomas storage).
+template <bool LAST>
+__global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work W, Opt O,
+                                                 TrSet T, SubStep ss, const f32::Face2 *fx2,
+                                                 const f32::Face2 *fy2,
+                                                 const float *__restrict__ tri,
+                                                 float *__restrict__ tro, int nw, int nchunk,
+                                                 int any_hd) {
+  using namespace f32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  Stage *stg = reinterpret_cast<Stage *>(smem);                       // [2][32]
+  int *colC = reinterpret_cast<int *>(stg + 64);                       // [nz][32]
+  float4 *colLU = reinterpret_cast<float4 *>(colC + G.nz * 32);        // [nz][32]
+  float *Sv = reinterpret_cast<float *>(colLU + G.nz * 32);            // [nz][nw][32]
+
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int tile = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int col = tile * 32 + lane;
+  const int slot = chunk * nw + wy;
+  const bool slot_ok = slot < T.nslot;
+
+  // column set-up (every warp holds its lane's column)
+  bool act = col < G.ncol;
+  ColInfo ci = {0, 0, 0, 0, 0};
+  int cbot = 0, c2 = 0, kb = G.nz, ks = 0;
+  if (act) {
+    ci = W.col[col];
+    cbot = G.col_bot[col];
+    c2 = G.col_top[col];
+    act = staged_column(ci, cbot);
+  }
+  if (act) {
+    kb = G.col_kb[col];
+    ks = kb;
+    for (int c = cbot, it = 0; c != ci.s && it < G.nz; ++it) {  // layer of the surface cell
+      c = G.zp1[c];
+      ++ks;
+    }
+  }
+  const int kstart = __reduce_min_sync(0xffffffffu, act ? kb : G.nz);
+  int kmin = kstart;
+  // block-wide minimum (all warps hold the same columns, so the warp value is it)
+
+  // tracer of this warp
+  const int n = slot_ok ? T.slot_tr[slot] : 0;
+  const uint8_t tf = slot_ok ? T.trf[n] : 0;
+  const bool tbdy = (tf & TR_TBDY) != 0;
+  const bool adv = tbdy && (tf & TR_ADV);
+  const bool hd = tbdy && (tf & TR_HDIFF);
+  const bool vdf = LAST && (tf & TR_VDIFF);
+  const bool single = (ci.flags & COL_SINGLE) != 0;
+  const double mn = slot_ok ? T.mintr[n] : 0.0, mx = slot_ok ? T.maxtr[n] : 0.0;
+  const float *tr = tri + (size_t)n * G.S;
+  float *to = tro + (size_t)n * G.S;
+  float *myS = Sv + wy * 32 + lane;
+  const int sstride = nw * 32;
+  const double dtu = ss.dtu;
+  double area = 1.0, ia = 1.0, sub = 0.0, osub = 0.0, botz2 = 0.0;
+  if (act) {
+    area = G.cellarea[c2];
+    ia = 1.0 / area;
+    double eta = F.eta[c2], oe = F.oldeta[c2];
+    sub = oe + ss.subeta_f * (eta - oe);
+    osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
+    botz2 = G.botz[c2];
+  }
+
+  // staging parts of this warp
+  Walk wk[4] = {{0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}};
+  const int nparts = (4 + nw - 1) / nw;
+  auto stage_layer = [&](int k) {
+    for (int q = 0; q < nparts; ++q) {
+      int part = wy + q * nw;
+      if (part < 4)
+        stage_part(part, k, lane, act, kb, ks, cbot, c2, G, F3, W, O, any_hd != 0, dtu, fx2, fy2,
+                   stg + (k & 1) * 32, colC, colLU, wk[q]);
+    }
+  };
+  if (kmin < G.nz) stage_layer(kmin);
+  __syncthreads();
+
+  // per tracer-lane walk state
+  float tm2 = 0.f, tm1 = 0.f, t0 = 0.f, tp1 = 0.f;
+  float Fzb_prev = 0.f;
+  double dtr_prev = 0.0, idz_prev = 0.0, t_prev = 0.0;
+  int c_prev = 0;
+  double a_below = 0.0;
+  double ssum = 0.0, scomp = 0.0;  // surface column mass (Neumaier)
+  float fwd_prev = 0.f;            // Thomas forward carry
+  double ts_old = 0.0, dtr_s = 0.0, Fzb_s = 0.0;
+  long long nwarn = 0;
+  const bool work = slot_ok && act;
+
+  for (int k = kmin; k < G.nz; ++k) {
+    if (k + 1 < G.nz) stage_layer(k + 1);
+    const Stage &S = stg[(k & 1) * 32 + lane];
+    const bool on = work && k >= kb;
+    // vertical window
+    if (on) {
+      if (k == kb) {
+        t0 = tr[S.c];
+        tm1 = t0;  // sediment ghost holds the bottom value (tracers.c:827-830)
+        tm2 = t0;
+      } else {
+        tm2 = tm1;
+        tm1 = t0;
+        t0 = tp1;
+      }
+      tp1 = tr[S.zp1];
+    }
+    // x-neighbour values from the neighbouring lanes
+    const float u1v = __shfl_up_sync(0xffffffffu, t0, 1);
+    const float u2v = __shfl_up_sync(0xffffffffu, t0, 2);
+    const float d1v = __shfl_down_sync(0xffffffffu, t0, 1);
+    const float d2v = __shfl_down_sync(0xffffffffu, t0, 2);
+    float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f;
+    if (on && tbdy && (adv || hd)) {
+      const int sh = S.share;
+      const float txm1 = (sh & SH_XM1) ? u1v : tr[S.xm1];
+      const float txm2 = (sh & SH_XM2) ? u2v : tr[S.xm2];
+      const float txp1 = (sh & SH_XP1) ? d1v : tr[S.xp1];
+      const float tym1 = tr[S.ym1], tym2 = tr[S.ym2], typ1 = tr[S.yp1], typ2 = tr[S.yp2];
+      if (adv || hd) {
+        Fxw = face(S.fxw, O.trasc, adv, hd, txm2, txm1, t0, txp1);
+        Fys = face(S.fys, O.trasc, adv, hd, tym2, tym1, t0, typ1);
+        Fyn = face(S.fyn, O.trasc, adv, hd, tym1, t0, typ1, typ2);
+        if (!(sh & SH_XP1)) {
+          const float txp2 = (sh & SH_XP2) ? d2v : tr[S.xp2];
+          Fxe = face(S.fxe, O.trasc, adv, hd, txm1, t0, txp1, txp2);
+        }
+        if (adv) Fzb = face(S.fzb, O.trasc, true, false, tm2, tm1, t0, tp1);
+      }
+    }
+    const float Fnext = __shfl_down_sync(0xffffffffu, Fxw, 1);
+    if (on) {
+      if (S.share & SH_XP1) Fxe = Fnext;
+      // FP64 flux divergence (tracers.c:888-892)
+      const double dtr =
+          (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+      // finish the cell below: its top-face flux is this cell's bottom face
+      if (tbdy && k > kb && c_prev) {
+        double a = t_prev - (dtr_prev * ia + ((double)Fzb - (double)Fzb_prev)) * idz_prev;
+        if (k == ks) a_below = a;
+        if (mn <= kClipEps && a < mn) a = mn;
+        if (a < mn || a > mx) ++nwarn;
+        const float a32 = (float)a;
+        to[c_prev] = a32;
+        if (vdf && !single) {  // Thomas forward (FP32) for layer k-1
+          const float4 lu = colLU[(k - 1) * 32 + lane];
+          const float s = (k - 1 == kb) ? lu.x * a32 * lu.z : (lu.x * a32 - lu.y * fwd_prev) * lu.z;
+          myS[(k - 1) * sstride] = s;
+          fwd_prev = s;
+        }
+      }
+      if (k == kb) to[G.zm1[S.c]] = tbdy ? t0 : tr[G.zm1[S.c]];  // sediment ghost
+      if (!tbdy) {
+        to[S.c] = t0;
+        if (vdf && !single && k <= ks) {
+          const float4 lu = colLU[k * 32 + lane];
+          const float s = (k == kb) ? lu.x * t0 * lu.z : (lu.x * t0 - lu.y * fwd_prev) * lu.z;
+          myS[k * sstride] = s;
+          fwd_prev = s;
+        }
+      } else if (k < ks) {
+        c_prev = S.c;
+        t_prev = (double)t0;
+        dtr_prev = dtr;
+        idz_prev = S.idz;
+        Fzb_prev = Fzb;
+      } else if (k == ks) {
+        // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
+        c_prev = 0;
+        ts_old = (double)t0;
+        Fzb_s = (double)Fzb;
+        dtr_s = dtr;
+        ssum = 0.0;
+        scomp = 0.0;
+        neumaier_add(ssum, scomp, Fzb_s * area);
+        const double wb = (S.c == cbot) ? botz2 : G.gridz[S.c];
+        neumaier_add(ssum, scomp, ts_old * area * (osub - wb));
+        neumaier_add(ssum, scomp, -dtr);
+      } else {
+        neumaier_add(ssum, scomp, -dtr);  // cells above the surface
+      }
+    }
+    __syncthreads();
+  }
+  if (!work) return;
+  if (!tbdy) {
+    if (vdf && single) {
+      const double h = (double)W.dz32[ci.s] > O.hmin ? (double)W.dz32[ci.s] : O.hmin;
+      to[ci.s] = (float)((double)to[ci.s] + F.dt * (0.0 - 0.0) / h);
+    }
+  } else {
+    // surface value
+    double vs = ts_old;
+    if (adv) {
+      const double wb = (ci.s == cbot) ? botz2 : G.gridz[ci.s];
+      const double dzs = sub - wb;
+      const double svol = dzs * area;
+      const double st = ssum + scomp;
+      const double sv = (svol == 0.0 || (st < 0.0 && dzs <= O.hmin)) ? 0.0 : st / svol;
+      vs = (botz2 > 0.0 && (double)W.dz32[ci.s] < O.hmin) ? ts_old : sv;
+    }
+    if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
+    if (mn <= kClipEps && vs < mn) vs = mn;
+    if (vs < mn || vs > mx) ++nwarn;
+    const float vs32 = (float)vs;
+    {
+      int cc = ci.s;
+      to[cc] = vs32;
+      for (int it = 0; cc != c2 && it < G.nz; ++it) {
+        cc = G.zp1[cc];
+        to[cc] = vs32;
+      }
+    }
+    if (vdf && single) {
+      const double h = (double)W.dz32[ci.s] > O.hmin ? (double)W.dz32[ci.s] : O.hmin;
+      to[ci.s] = (float)(vs + F.dt * (0.0 - 0.0) / h);
+    } else if (vdf) {
+      const float4 lu = colLU[ks * 32 + lane];
+      const float s = (ks == kb) ? lu.x * vs32 * lu.z : (lu.x * vs32 - lu.y * fwd_prev) * lu.z;
+      myS[ks * sstride] = s;
+    }
+  }
+  if (vdf && !single) {
+    // back substitution (FP32) with the FP64 residual of the row above
+    //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
+    // (the difference form of b - A x for A = dzdt I + the diffusion operator)
+    float xj1 = 0.f, xj2 = 0.f;  // x(k+1), x(k+2)
+    for (int k = ks; k >= kb; --k) {
+      const float4 lu = colLU[k * 32 + lane];
+      const float x = (k == ks) ? myS[k * sstride] : myS[k * sstride] - colLU[(k + 1) * 32 + lane].w * xj1;
+      if (k < ks) {
+        // residual of row j = k + 1
+        const int j = k + 1;
+        const float4 lj = colLU[j * 32 + lane];
+        const int cj = colC[j * 32 + lane];
+        const double aj = (j == ks) ? (double)(float)to[cj] : (double)to[cj];
+        const double xj = xj1;
+        double r = (double)lj.x * (aj - xj) - (double)lj.y * ((double)x - xj);
+        if (j < ks) r -= (double)colLU[(j + 1) * 32 + lane].y * ((double)xj2 - xj);
+        myS[j * sstride] = (float)r;
+        to[cj] = xj1;  // x(j) replaces a(j) in the tracer array
+      }
+      xj2 = xj1;
+      xj1 = x;
+      (void)lu;
+    }
+    {  // residual of the bottom row (cm1 = 0 there)
+      const int j = kb;
+      const float4 lj = colLU[j * 32 + lane];
+      const int cj = colC[j * 32 + lane];
+      const double aj = (double)to[cj], xj = xj1;
+      double r = (double)lj.x * (aj - xj);
+      if (j < ks) r -= (double)colLU[(j + 1) * 32 + lane].y * ((double)xj2 - xj);
+      myS[j * sstride] = (float)r;
+      to[cj] = xj1;
+    }
+    // correction solve (FP32 forward and back) and update in FP64
+    float up = 0.f;
+    for (int k = kb; k <= ks; ++k) {
+      const float4 lu = colLU[k * 32 + lane];
+      const float r = myS[k * sstride];
+      const float u = (k == kb) ? r * lu.z : (r - lu.y * up) * lu.z;
+      myS[k * sstride] = u;
+      up = u;
+    }
+    float dn = 0.f;
+    int stat = 0;
+    for (int k = ks; k >= kb; --k) {
+      const float d = (k == ks) ? myS[k * sstride] : myS[k * sstride] - colLU[(k + 1) * 32 + lane].w * dn;
+      const int c = colC[k * 32 + lane];
+      const float fin = (float)((double)to[c] + (double)d);
+      to[c] = fin;
+      if (isnan(fin)) stat = ST_NAN;
+      dn = d;
+    }
+    if (stat) atomicOr(W.status, stat);
+    // cells above the surface keep the surface value: the copy-up above
+  }
+  if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
+}
+
+}  // namespace shoc

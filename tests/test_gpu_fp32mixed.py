@@ -1,0 +1,75 @@
+"""FP32-mixed path against the FP64 oracle.
+
+FP32 tracers, face values and Thomas sweeps; FP64 flux divergence, surface
+column-mass sums, implicit-solve residual and one refinement step.  Error
+measure per tracer: max |gpu - oracle| / max |oracle| over the wet cells
+(scale-aware; tracers span 1e-3..1e2), bar 1e-5.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from ems_b200 import _abi, gpu, synth
+
+pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("need_gpu")]
+
+TOL = 1e-5
+
+
+def errors(case, got, ref):
+    c = case.win.wet_cells()
+    g, r = got[:, c], ref[:, c]
+    scale = np.abs(r).max(axis=1)
+    emax = np.abs(g - r).max(axis=1) / scale
+    erms = np.sqrt(((g - r) ** 2).mean(axis=1)) / np.sqrt((r ** 2).mean(axis=1))
+    return emax, erms
+
+
+def run(case, nsteps):
+    t = gpu.TracerStep(case, precision=gpu.FP32_MIXED)
+    t.start()
+    t.run(nsteps)
+    d = t.sync()
+    out = t.download()
+    sur, nsur = t.surface()
+    t.close()
+    return out, sur, nsur, d
+
+
+@pytest.mark.parametrize("kw", [
+    {}, dict(trasc=_abi.VANLEER, ultimate=0), dict(trasc=_abi.VANLEER, ultimate=1),
+    dict(ultimate=0), dict(dt=2000.0)])
+def test_small_windows_within_tolerance(kw):
+    case = synth.make("small", seed=61, **kw)
+    out, sur, nsur, d = run(case, 10)
+    ref = oracle.run_oracle(case, 10)
+    emax, erms = errors(case, out, ref[1])
+    assert np.all(emax <= TOL), (emax, erms)
+    np.testing.assert_array_equal(sur, ref[2])
+    np.testing.assert_array_equal(nsur, ref[3])
+
+
+def test_moving_surface_general_path():
+    # surface crossing layer faces: those columns take the general path
+    case = synth.make("small", seed=62, layers=np.linspace(-30, 2.0, 8), eta_offset=(1.9, -1.7))
+    out, sur, nsur, d = run(case, 6)
+    ref = oracle.run_oracle(case, 6)
+    emax, _ = errors(case, out, ref[1])
+    assert np.all(emax <= TOL), emax
+
+
+def test_basin64_fp32_mixed():
+    case = synth.make("basin64")
+    out, *_ = run(case, 100)
+    ref = oracle.run_oracle(case, 100)[1]
+    emax, erms = errors(case, out, ref)
+    assert np.all(emax <= TOL), (emax, erms)
+
+
+@pytest.mark.slow
+def test_drop512_fp32_mixed():
+    case = synth.make("drop512")
+    out, *_ = run(case, 3)
+    ref = oracle.run_oracle(case, 3)[1]
+    emax, erms = errors(case, out, ref)
+    assert np.all(emax <= TOL), (emax, erms)
