@@ -326,9 +326,14 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
   if (act) {
     kb = G.col_kb[col];
     ks = kb;
-    for (int c = cbot, it = 0; c != ci.s && it < G.nz; ++it) {  // layer of the surface cell
+    int c = cbot;
+    for (int it = 0; c != ci.s && it < G.nz; ++it) {  // layer of the surface cell
       c = G.zp1[c];
       ++ks;
+    }
+    if (c != ci.s || ks >= G.nz) {  // surface cell not in this column: leave it alone
+      act = false;
+      kb = G.nz;
     }
   }
   const int kstart = __reduce_min_sync(0xffffffffu, act ? kb : G.nz);
