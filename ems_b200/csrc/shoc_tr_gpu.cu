@@ -823,6 +823,10 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   int tw = 8;
   if (h->staged) {
     while (tw > 1 && stage32_smem(g->nz, tw) > 112 * 1024) tw--;
+    // balance the tracer chunks: the per-layer staging is shared by a block
+    int nch = (h->nslot + tw - 1) / std::max(tw, 1);
+    if (nch > 0) tw = (h->nslot + nch - 1) / nch;
+    if (tw < 1) tw = 1;
   } else {
     while (tw > 1 && (size_t)g->nz * tw * 32 * sizeof(double) > 200 * 1024) tw /= 2;
   }

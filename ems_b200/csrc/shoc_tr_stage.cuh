@@ -58,7 +58,8 @@ struct Stage {
   int share;
   int pad;
   Face fxw, fxe, fys, fyn, fzb;
-  double idz;
+  float idz;
+  int pad2;
 };
 
 // per-column metric factors of one horizontal direction (precomputed once)
@@ -88,7 +89,7 @@ __device__ __forceinline__ void set_face_h(Face &f, bool on, float cr, const Fac
     f.b = 0.f;
     f.A = f.B = 0.f;
   }
-  f.ircr = cr != 0.f ? 1.f / fabsf(cr) : 0.f;
+  f.ircr = cr != 0.f ? __fdividef(1.f, fabsf(cr)) : 0.f;
   f.U = U;
   f.K = K;
 }
@@ -98,54 +99,44 @@ __device__ __forceinline__ float face(const Face &f, int trasc, bool adv, bool h
                                       float tm1, float t0, float tp1) {
   const int md = f.mode;
   if (!(md & FM_ON)) return 0.f;
+  const bool pos = (md & FM_POS) != 0, neg = (md & FM_NEG) != 0;
   float F = 0.f;
-  if (!adv) {
-  } else if (trasc == SHOC_TR_QUICKEST) {
-    float curv = 0.f;
-    if (md & FM_POS)
-      curv = f.A * t0 + f.B * tm2 - 2.f * tm1;
-    else if (md & FM_NEG)
-      curv = f.A * tp1 + f.B * tm1 - 2.f * t0;
-    F = tm1 + f.a * (t0 - tm1) - f.b * curv;
-  } else if (md & FM_POS) {
-    float df = (tm1 - tm2) * (t0 - tm1);
-    df = df > 0.f ? 2.f * __fdividef(df, t0 - tm2) : 0.f;
-    F = tm1 + f.a * df;
-  } else if (md & FM_NEG) {
-    float df = (t0 - tm1) * (tp1 - t0);
-    df = df > 0.f ? 2.f * __fdividef(df, tp1 - tm1) : 0.f;
-    F = t0 - f.a * df;
+  if (adv) {
+    if (trasc == SHOC_TR_QUICKEST) {
+      // upwind-side curvature: A tX + B tY - 2 tZ
+      const float X = pos ? t0 : tp1, Y = pos ? tm2 : tm1, Z = pos ? tm1 : t0;
+      const float curv = (pos || neg) ? f.A * X + f.B * Y - 2.f * Z : 0.f;
+      F = tm1 + f.a * (t0 - tm1) - f.b * curv;
+    } else if (pos || neg) {
+      const float p = pos ? (tm1 - tm2) : (t0 - tm1), q = pos ? (t0 - tm1) : (tp1 - t0);
+      const float den = pos ? (t0 - tm2) : (tp1 - tm1);
+      float df = p * q;
+      df = df > 0.f ? 2.f * __fdividef(df, den) : 0.f;
+      F = pos ? tm1 + f.a * df : t0 - f.a * df;
+    }
+    if ((md & FM_ULT) && (pos || neg)) {
+      const float tc = pos ? tm1 : t0, tu = pos ? tm2 : tp1, td = pos ? t0 : tm1;
+      const float diff = td - tu;
+      float nc = 0.f, nu = 0.f;
+      if (diff != 0.f) {
+        const float r = __fdividef(1.f, diff);
+        nc = (tc - tu) * r;
+        nu = (F - tu) * r;
+      }
+      const float lim = tu + nc * diff;
+      if (nc >= 0.f && nc <= 1.f) {
+        if (nu > 1.f)
+          F = td;
+        else if (nu < nc)
+          F = lim;
+        else if (nu > nc * f.ircr)
+          F = tu + nc * diff * f.ircr;
+      } else {
+        F = lim;
+      }
+    }
+    F *= f.U;
   }
-  if (adv && (md & FM_ULT) && (md & (FM_POS | FM_NEG))) {
-    float tc, tu, td;
-    if (md & FM_POS) {
-      tc = tm1;
-      tu = tm2;
-      td = t0;
-    } else {
-      tc = t0;
-      tu = tp1;
-      td = tm1;
-    }
-    const float diff = td - tu;
-    float nc = 0.f, nu = 0.f;
-    if (diff != 0.f) {
-      const float r = __frcp_rn(diff);
-      nc = (tc - tu) * r;
-      nu = (F - tu) * r;
-    }
-    if (nc >= 0.f && nc <= 1.f) {
-      if (nu > 1.f)
-        F = td;
-      else if (nu < nc)
-        F = tu + nc * diff;
-      else if (nu > nc * f.ircr)
-        F = tu + nc * diff * f.ircr;
-    } else {
-      F = tu + nc * diff;
-    }
-  }
-  F *= f.U;
   if (hd && (md & FM_HD)) F -= f.K * (t0 - tm1);
   return F;
 }
@@ -159,8 +150,27 @@ struct Walk {   // per-lane column walk of one staging part
   float dzm2, dzm1, dz0;  // thickness window of part 3
 };
 
+constexpr int kParts = 7;  // 0 indices, 1-4 horizontal faces, 5 z face, 6 thickness + LU
+
+__device__ __forceinline__ void stage_hface(Face &f, int c, bool x, const Geo &G, const Flow32 &F3,
+                                            const Opt &O, bool any_hd, float fdtu,
+                                            const Face2 *m2) {
+  const uint8_t EB = x ? CF_E1 : CF_E2;
+  const uint8_t fc = G.cflag[c];
+  if (!(fc & CF_WET)) {  // a ghost: the face carries nothing
+    f.mode = 0;
+    return;
+  }
+  const Face2 m = m2[G.m2d[c]];
+  const float cr = (x ? F3.u1[c] : F3.u2[c]) * fdtu * m.ih;
+  const bool quick = O.trasc == SHOC_TR_QUICKEST;
+  set_face_h(f, quick ? true : (fc & EB) != 0, cr, m, x ? F3.u1flux3d[c] : F3.u2flux3d[c],
+             O.ultimate && (fc & EB), O.trasc, any_hd ? (x ? F3.khx[c] : F3.khy[c]) : 0.f,
+             any_hd);
+}
+
 __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, int kb, int ks,
-                                           int cbot, int c2, const Geo &G, const Flow32 &F3,
+                                           int cbot, const Geo &G, const Flow32 &F3,
                                            const Work &W, const Opt &O, bool any_hd,
                                            double dtu, const Face2 *fx2, const Face2 *fy2,
                                            Stage *st, int *colC, float4 *colLU, Walk &wk) {
@@ -170,99 +180,87 @@ __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, 
   wk.c = c;
   Stage &S = st[lane];
   const float fdtu = (float)dtu;
-  if (part == 0) {
-    int zp1 = 0, xm1 = 0, xp1 = 0, ym1 = 0, yp1 = 0, xm2 = 0, xp2 = 0, ym2 = 0, yp2 = 0;
-    if (on) {
-      zp1 = G.zp1[c];
-      xm1 = G.xm1[c];
-      xp1 = G.xp1[c];
-      ym1 = G.ym1[c];
-      yp1 = G.yp1[c];
-      xm2 = G.xm1[xm1];
-      xp2 = G.xp1[xp1];
-      ym2 = G.ym1[ym1];
-      yp2 = G.yp1[yp1];
+  switch (part) {
+    case 0: {
+      int zp1 = 0, xm1 = 0, xp1 = 0, ym1 = 0, yp1 = 0, xm2 = 0, xp2 = 0, ym2 = 0, yp2 = 0;
+      if (on) {
+        zp1 = G.zp1[c];
+        xm1 = G.xm1[c];
+        xp1 = G.xp1[c];
+        ym1 = G.ym1[c];
+        yp1 = G.yp1[c];
+        xm2 = G.xm1[xm1];
+        xp2 = G.xp1[xp1];
+        ym2 = G.ym1[ym1];
+        yp2 = G.yp1[yp1];
+      }
+      const int cu1 = __shfl_up_sync(0xffffffffu, c, 1), cu2 = __shfl_up_sync(0xffffffffu, c, 2);
+      const int cd1 = __shfl_down_sync(0xffffffffu, c, 1),
+                cd2 = __shfl_down_sync(0xffffffffu, c, 2);
+      int sh = 0;
+      if (on) {
+        if (lane >= 1 && cu1 && xm1 == cu1) sh |= SH_XM1;
+        if (lane >= 2 && cu2 && xm2 == cu2) sh |= SH_XM2;
+        if (lane <= 30 && cd1 && xp1 == cd1) sh |= SH_XP1;
+        if (lane <= 29 && cd2 && xp2 == cd2) sh |= SH_XP2;
+      }
+      S.c = c;
+      S.zp1 = zp1;
+      S.xm1 = xm1; S.xm2 = xm2; S.xp1 = xp1; S.xp2 = xp2;
+      S.ym1 = ym1; S.ym2 = ym2; S.yp1 = yp1; S.yp2 = yp2;
+      S.share = sh;
+      colC[k * 32 + lane] = c;
+      break;
     }
-    const int cu1 = __shfl_up_sync(0xffffffffu, c, 1), cu2 = __shfl_up_sync(0xffffffffu, c, 2);
-    const int cd1 = __shfl_down_sync(0xffffffffu, c, 1), cd2 = __shfl_down_sync(0xffffffffu, c, 2);
-    int sh = 0;
-    if (on) {
-      if (lane >= 1 && cu1 && xm1 == cu1) sh |= SH_XM1;
-      if (lane >= 2 && cu2 && xm2 == cu2) sh |= SH_XM2;
-      if (lane <= 30 && cd1 && xp1 == cd1) sh |= SH_XP1;
-      if (lane <= 29 && cd2 && xp2 == cd2) sh |= SH_XP2;
-    }
-    S.c = c;
-    S.zp1 = zp1;
-    S.xm1 = xm1; S.xm2 = xm2; S.xp1 = xp1; S.xp2 = xp2;
-    S.ym1 = ym1; S.ym2 = ym2; S.yp1 = yp1; S.yp2 = yp2;
-    S.share = sh;
-    colC[k * 32 + lane] = c;
-  } else if (part == 1 || part == 2) {
-    const bool x = part == 1;
-    Face &fw = x ? S.fxw : S.fys;
-    Face &fe = x ? S.fxe : S.fyn;
-    if (!on) {
-      fw.mode = 0;
-      fe.mode = 0;
-      return;
-    }
-    const uint8_t EB = x ? CF_E1 : CF_E2;
-    const float *vel = x ? F3.u1 : F3.u2;
-    const float *flx = x ? F3.u1flux3d : F3.u2flux3d;
-    const float *kh = x ? F3.khx : F3.khy;
-    const Face2 *m2 = x ? fx2 : fy2;
-    const uint8_t fc = G.cflag[c];
-    const bool quick = O.trasc == SHOC_TR_QUICKEST;
-    const Face2 mw = m2[c2];
-    const float crw = vel[c] * fdtu * mw.ih;
-    set_face_h(fw, quick ? true : (fc & EB) != 0, crw, mw, flx[c], O.ultimate && (fc & EB),
-               O.trasc, any_hd ? kh[c] : 0.f, any_hd);
-    const int cp = x ? G.xp1[c] : G.yp1[c];
-    const uint8_t fp = G.cflag[cp];
-    if (fp & CF_WET) {
-      const Face2 me = m2[G.m2d[cp]];
-      const float cre = vel[cp] * fdtu * me.ih;
-      set_face_h(fe, quick ? true : (fp & EB) != 0, cre, me, flx[cp], O.ultimate && (fp & EB),
-                 O.trasc, any_hd ? kh[cp] : 0.f, any_hd);
-    } else {
-      fe.mode = 0;
-    }
-  } else {
-    Face &fz = S.fzb;
-    if (!on) {
-      fz.mode = 0;
-      return;
-    }
-    const int zp1 = G.zp1[c];
-    if (k == kb) {
-      wk.dzm2 = 0.f;  // thickness of the sediment cell (never set by set_dz)
-      wk.dzm1 = 0.f;
+    case 1:
+      if (on) stage_hface(S.fxw, c, true, G, F3, O, any_hd, fdtu, fx2); else S.fxw.mode = 0;
+      break;
+    case 2:
+      if (on) stage_hface(S.fxe, G.xp1[c], true, G, F3, O, any_hd, fdtu, fx2); else S.fxe.mode = 0;
+      break;
+    case 3:
+      if (on) stage_hface(S.fys, c, false, G, F3, O, any_hd, fdtu, fy2); else S.fys.mode = 0;
+      break;
+    case 4:
+      if (on) stage_hface(S.fyn, G.yp1[c], false, G, F3, O, any_hd, fdtu, fy2); else S.fyn.mode = 0;
+      break;
+    case 5: {
+      Face &fz = S.fzb;
+      if (!on) {
+        fz.mode = 0;
+        break;
+      }
+      const int zp1 = G.zp1[c];
+      if (k == kb) {
+        wk.dzm2 = 0.f;  // thickness of the sediment cell (never set by set_dz)
+        wk.dzm1 = 0.f;
+      } else {
+        wk.dzm2 = wk.dzm1;
+        wk.dzm1 = wk.dz0;
+      }
       wk.dz0 = W.dz32[c];
-    } else {
-      wk.dzm2 = wk.dzm1;
-      wk.dzm1 = wk.dz0;
-      wk.dz0 = W.dz32[c];
-    }
-    const float dzp1 = W.dz32[zp1];
-    S.idz = 1.0 / (double)wk.dz0;
-    if (k <= ks) {  // the cell is one of the cells to process: it has a z face
+      if (k > ks) {  // above the surface: no z face
+        fz.mode = 0;
+        break;
+      }
+      const float dzp1 = W.dz32[zp1];
       const float w9m = 0.5f * (wk.dzm1 + wk.dzm2);
       const float w90 = 0.5f * (wk.dz0 + wk.dzm1);
-      const float w9p = 0.5f * (dzp1 + wk.dz0);
+      // w9 of the cell above; the surface-layer cell maps onto itself
+      const float w9p = (zp1 == c) ? w90 : 0.5f * (dzp1 + wk.dz0);
       const float wv = F3.w[c] * fdtu;
-      const float cz = wv / w90;
+      const float cz = __fdividef(wv, w90);
       fz.mode = FM_ON | (cz > 0.f ? FM_POS : 0) | (cz < 0.f ? FM_NEG : 0) |
                 (O.ultimate ? FM_ULT : 0);
       if (O.trasc == SHOC_TR_QUICKEST) {
-        fz.a = wk.dzm1 / (wk.dzm1 + wk.dz0) - 0.5f * cz;
+        fz.a = __fdividef(wk.dzm1, wk.dzm1 + wk.dz0) - 0.5f * cz;
         fz.b = (1.f - cz * cz) * (1.f / 6.f);
         if (cz > 0.f) {
-          const float db = 2.f / (w9m + w90);
+          const float db = __fdividef(2.f, w9m + w90);
           fz.A = db * w9m;
           fz.B = db * w90;
         } else {
-          const float df = 2.f / (w90 + w9p);
+          const float df = __fdividef(2.f, w90 + w9p);
           fz.A = df * w90;
           fz.B = df * w9p;
         }
@@ -270,13 +268,17 @@ __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, 
         fz.a = cz > 0.f ? 0.5f * (1.f - cz) : 0.5f * (1.f + cz);
         fz.b = fz.A = fz.B = 0.f;
       }
-      fz.ircr = cz != 0.f ? 1.f / fabsf(cz) : 0.f;
+      fz.ircr = cz != 0.f ? __fdividef(1.f, fabsf(cz)) : 0.f;
       fz.U = wv;
       fz.K = 0.f;
-    } else {
-      fz.mode = 0;
+      break;
     }
-    colLU[k * 32 + lane] = (k <= ks) ? W.lu32[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+    default: {  // 6
+      if (!on) break;
+      S.idz = __fdividef(1.f, W.dz32[c]);
+      colLU[k * 32 + lane] = (k <= ks) ? W.lu32[c] : make_float4(0.f, 0.f, 0.f, 0.f);
+      break;
+    }
   }
 }
 
@@ -365,13 +367,14 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
   }
 
   // staging parts of this warp
-  Walk wk[4] = {{0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}, {0, 0.f, 0.f, 0.f}};
-  const int nparts = (4 + nw - 1) / nw;
+  Walk wk[kParts];
+  for (int q = 0; q < kParts; ++q) wk[q] = {0, 0.f, 0.f, 0.f};
   auto stage_layer = [&](int k) {
-    for (int q = 0; q < nparts; ++q) {
-      int part = wy + q * nw;
-      if (part < 4)
-        stage_part(part, k, lane, act, kb, ks, cbot, c2, G, F3, W, O, any_hd != 0, dtu, fx2, fy2,
+#pragma unroll
+    for (int q = 0; q < kParts; ++q) {
+      const int part = wy + q * nw;
+      if (part < kParts)
+        stage_part(part, k, lane, act, kb, ks, cbot, G, F3, W, O, any_hd != 0, dtu, fx2, fy2,
                    stg + (k & 1) * 32, colC, colLU, wk[q]);
     }
   };
@@ -464,7 +467,7 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
         c_prev = S.c;
         t_prev = (double)t0;
         dtr_prev = dtr;
-        idz_prev = S.idz;
+        idz_prev = (double)S.idz;
         Fzb_prev = Fzb;
       } else if (k == ks) {
         // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
