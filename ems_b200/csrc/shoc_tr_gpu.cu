@@ -497,7 +497,7 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
 }
 
 size_t stage32_smem(int nz, int nw) {
-  return 64 * sizeof(f32::Stage) + (size_t)nz * 32 * sizeof(int) +
+  return 3 * 32 * sizeof(f32::Stage) + (size_t)nz * 32 * sizeof(int) +
          (size_t)nz * 32 * sizeof(float4) + (size_t)nz * nw * 32 * sizeof(float);
 }
 

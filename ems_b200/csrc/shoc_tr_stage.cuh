@@ -124,7 +124,14 @@ __device__ __forceinline__ float face(const Face &f, int trasc, bool adv, bool h
         nu = (F - tu) * r;
       }
       const float lim = tu + nc * diff;
-      if (nc >= 0.f && nc <= 1.f) {
+      if (diff == 0.f && tc != tu) {
+        // Upwind and downwind values equal in FP32.  In FP64 they almost
+        // always differ by a few ulps, nc is then huge and the limiter
+        // falls back to upwind (tc); follow that rather than the exact-tie
+        // case (which leaves the face unlimited), so FP32 rounding of the
+        // stored tracer does not flip the limiter's decision.
+        F = tc;
+      } else if (nc >= 0.f && nc <= 1.f) {
         if (nu > 1.f)
           F = td;
         else if (nu < nc)
@@ -293,7 +300,7 @@ __device__ __forceinline__ void neumaier_add(double &s, double &comp, double v) 
 // ---------------------------------------------------------------------------
 // The FP32-mixed staged transport kernel.
 //
-// Shared memory: Stage[2][32] | int colC[nz][32] | float4 colLU[nz][32] |
+// Shared memory: Stage[3][32] | int colC[nz][32] | float4 colLU[nz][32] |
 // float Sv[nz][nw][32] (per tracer-lane Thomas storage).
 template <bool LAST>
 __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work W, Opt O,
@@ -304,8 +311,8 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
                                                  int any_hd) {
   using namespace f32;
   extern __shared__ __align__(16) unsigned char smem[];
-  Stage *stg = reinterpret_cast<Stage *>(smem);                       // [2][32]
-  int *colC = reinterpret_cast<int *>(stg + 64);                       // [nz][32]
+  Stage *stg = reinterpret_cast<Stage *>(smem);                       // [3][32] ring
+  int *colC = reinterpret_cast<int *>(stg + 3 * 32);                   // [nz][32]
   float4 *colLU = reinterpret_cast<float4 *>(colC + G.nz * 32);        // [nz][32]
   float *Sv = reinterpret_cast<float *>(colLU + G.nz * 32);            // [nz][nw][32]
 
@@ -375,10 +382,13 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
       const int part = wy + q * nw;
       if (part < kParts)
         stage_part(part, k, lane, act, kb, ks, cbot, G, F3, W, O, any_hd != 0, dtu, fx2, fy2,
-                   stg + (k & 1) * 32, colC, colLU, wk[q]);
+                   stg + (k % 3) * 32, colC, colLU, wk[q]);
     }
   };
+  // layers are staged two ahead of the one being computed (3-slot ring);
+  // each iteration also prefetches the next layer's tracer values
   if (kmin < G.nz) stage_layer(kmin);
+  if (kmin + 1 < G.nz) stage_layer(kmin + 1);
   __syncthreads();
 
   // per tracer-lane walk state
@@ -392,15 +402,42 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
   double ts_old = 0.0, dtr_s = 0.0, Fzb_s = 0.0;
   long long nwarn = 0;
   const bool work = slot_ok && act;
+  const bool hor = tbdy && (adv || hd);
+
+  // tracer values of one layer, loaded one layer ahead of their use
+  struct Pre {
+    float t0, tp, xm1, xm2, xp1, xp2, ym1, ym2, yp1, yp2;
+  };
+  auto prefetch = [&](int k, Pre &p) {
+    if (!(work && k >= kb && k < G.nz)) return;
+    const Stage &S = stg[(k % 3) * 32 + lane];
+    if (k == kb) p.t0 = tr[S.c];
+    p.tp = tr[S.zp1];
+    if (hor) {
+      const int sh = S.share;
+      p.ym1 = tr[S.ym1];
+      p.ym2 = tr[S.ym2];
+      p.yp1 = tr[S.yp1];
+      p.yp2 = tr[S.yp2];
+      if (!(sh & SH_XM1)) p.xm1 = tr[S.xm1];
+      if (!(sh & SH_XM2)) p.xm2 = tr[S.xm2];
+      if (!(sh & SH_XP1)) p.xp1 = tr[S.xp1];
+      if (!(sh & (SH_XP1 | SH_XP2))) p.xp2 = tr[S.xp2];
+    }
+  };
+  Pre cur = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  Pre nxt = cur;
+  prefetch(kmin, cur);
 
   for (int k = kmin; k < G.nz; ++k) {
-    if (k + 1 < G.nz) stage_layer(k + 1);
-    const Stage &S = stg[(k & 1) * 32 + lane];
+    if (k + 2 < G.nz) stage_layer(k + 2);
+    prefetch(k + 1, nxt);
+    const Stage &S = stg[(k % 3) * 32 + lane];
     const bool on = work && k >= kb;
     // vertical window
     if (on) {
       if (k == kb) {
-        t0 = tr[S.c];
+        t0 = cur.t0;
         tm1 = t0;  // sediment ghost holds the bottom value (tracers.c:827-830)
         tm2 = t0;
       } else {
@@ -408,7 +445,7 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
         tm1 = t0;
         t0 = tp1;
       }
-      tp1 = tr[S.zp1];
+      tp1 = cur.tp;
     }
     // x-neighbour values from the neighbouring lanes
     const float u1v = __shfl_up_sync(0xffffffffu, t0, 1);
@@ -416,22 +453,19 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
     const float d1v = __shfl_down_sync(0xffffffffu, t0, 1);
     const float d2v = __shfl_down_sync(0xffffffffu, t0, 2);
     float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f;
-    if (on && tbdy && (adv || hd)) {
+    if (on && hor) {
       const int sh = S.share;
-      const float txm1 = (sh & SH_XM1) ? u1v : tr[S.xm1];
-      const float txm2 = (sh & SH_XM2) ? u2v : tr[S.xm2];
-      const float txp1 = (sh & SH_XP1) ? d1v : tr[S.xp1];
-      const float tym1 = tr[S.ym1], tym2 = tr[S.ym2], typ1 = tr[S.yp1], typ2 = tr[S.yp2];
-      if (adv || hd) {
-        Fxw = face(S.fxw, O.trasc, adv, hd, txm2, txm1, t0, txp1);
-        Fys = face(S.fys, O.trasc, adv, hd, tym2, tym1, t0, typ1);
-        Fyn = face(S.fyn, O.trasc, adv, hd, tym1, t0, typ1, typ2);
-        if (!(sh & SH_XP1)) {
-          const float txp2 = (sh & SH_XP2) ? d2v : tr[S.xp2];
-          Fxe = face(S.fxe, O.trasc, adv, hd, txm1, t0, txp1, txp2);
-        }
-        if (adv) Fzb = face(S.fzb, O.trasc, true, false, tm2, tm1, t0, tp1);
+      const float txm1 = (sh & SH_XM1) ? u1v : cur.xm1;
+      const float txm2 = (sh & SH_XM2) ? u2v : cur.xm2;
+      const float txp1 = (sh & SH_XP1) ? d1v : cur.xp1;
+      Fxw = face(S.fxw, O.trasc, adv, hd, txm2, txm1, t0, txp1);
+      Fys = face(S.fys, O.trasc, adv, hd, cur.ym2, cur.ym1, t0, cur.yp1);
+      Fyn = face(S.fyn, O.trasc, adv, hd, cur.ym1, t0, cur.yp1, cur.yp2);
+      if (!(sh & SH_XP1)) {
+        const float txp2 = (sh & SH_XP2) ? d2v : cur.xp2;
+        Fxe = face(S.fxe, O.trasc, adv, hd, txm1, t0, txp1, txp2);
       }
+      if (adv) Fzb = face(S.fzb, O.trasc, true, false, tm2, tm1, t0, tp1);
     }
     const float Fnext = __shfl_down_sync(0xffffffffu, Fxw, 1);
     if (on) {
@@ -485,6 +519,7 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
         neumaier_add(ssum, scomp, -dtr);  // cells above the surface
       }
     }
+    cur = nxt;
     __syncthreads();
   }
   if (!work) return;
