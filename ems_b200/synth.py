@@ -380,9 +380,12 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
         tracers = "done"
     ii, jj, kk = win.s2i[c], win.s2j[c], win.s2k[c]
     if tracers == "gauss":
+        # centre off the cell grid in every direction, so no two cells are
+        # mirror images and the limiter never sees exactly equal neighbours
         sig = 5.0
+        x0, y0, z0 = nx / 2 - 0.37, ny / 2 - 0.21, nz / 2 - 0.33
         for n in range(ntr):
-            r2 = ((ii - nx / 2 + 0.5) ** 2 + (jj - ny / 2 + 0.5) ** 2 + (kk - nz / 2) ** 2)
+            r2 = ((ii - x0) ** 2 + (jj - y0) ** 2 + (kk - z0) ** 2)
             tr[n, c] = np.exp(-r2 / (2 * sig * sig))
     elif tracers == "step":
         for n in range(ntr):
