@@ -24,6 +24,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "shoc_tr_gpu.h"
@@ -1273,6 +1274,92 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
     mass[n] = s + comp;
   }
   return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Mass reduction that allocates nothing.
+//
+// For callers that may not allocate device memory while they step: code that
+// runs while a stream is being captured into a CUDA graph (an allocation there
+// would become part of the graph, or fail), and host frameworks that hand all
+// device memory out of their own fixed pool and forbid allocations once the
+// run is going.  The block partials live in the fixed device array below
+// instead of a stream-ordered allocation; the caller passes the (already
+// allocated) handle and a host array for the result.
+namespace {
+
+constexpr int kNoAllocBlocks = 148 * 2;     // partial sums per tracer
+constexpr int kNoAllocMaxTracers = 64;      // largest tracer count it serves
+// [kNoAllocMaxTracers][kNoAllocBlocks] partials, then kNoAllocMaxTracers sums;
+// about 152 KB that every device loading the library holds until exit
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocMaxTracers * kNoAllocBlocks +
+                                                   kNoAllocMaxTracers];
+
+// Per-tracer compensated sum of the block partials, in the order the
+// allocating entry point sums them on the host (same result bit for bit).
+__global__ void k_mass_finish(const double *part, int nb, int ntr, double *sums) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= ntr) return;
+  double s = 0.0, comp = 0.0;
+  for (int b = 0; b < nb; b++) {
+    double v = part[(size_t)n * nb + b], u = s + v;
+    comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+    s = u;
+  }
+  sums[n] = s + comp;
+}
+
+std::mutex g_noalloc_mu;
+double *g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array for the current device, looked up once
+// per device (the symbol's host-side name is not a device address).
+int noalloc_scratch(int device, double **out) {
+  if (device < 0 || device >= 64) return SHOC_TR_EARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      fprintf(stderr, "shoc_tr_gpu: cudaGetSymbolAddress: %s\n", cudaGetErrorString(e));
+      return SHOC_TR_ECUDA;
+    }
+    g_noalloc_ptr[device] = (double *)p;
+  }
+  *out = g_noalloc_ptr[device];
+  return SHOC_TR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass) {
+  if (!h || !mass) return SHOC_TR_EARG;
+  if (h->ntr > kNoAllocMaxTracers) return SHOC_TR_ESCRATCH;
+  if (cudaSetDevice(h->device) != cudaSuccess) return SHOC_TR_ECUDA;
+  double *scr = nullptr;
+  int rc = noalloc_scratch(h->device, &scr);
+  if (rc) return rc;
+  if (h->ntr == 0) return SHOC_TR_OK;
+  // every partial and sum slot used below is written before it is read, so
+  // nothing left over from an earlier call needs clearing
+  double *part = scr, *sums = scr + (size_t)kNoAllocMaxTracers * kNoAllocBlocks;
+  if (h->esize == sizeof(float))
+    k_mass<float><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
+        h->G, h->F, h->W, (const float *)h->tr[h->cur], part);
+  else
+    k_mass<double><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
+        h->G, h->F, h->W, (const double *)h->tr[h->cur], part);
+  k_mass_finish<<<(h->ntr + 63) / 64, 64, 0, h->stream>>>(part, kNoAllocBlocks, h->ntr, sums);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(mass, sums, (size_t)h->ntr * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
 }
 
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h) { return h ? (void *)h->stream : nullptr; }

@@ -22,6 +22,7 @@ EXPORTS = (
     "shoc_tr_gpu_create", "shoc_tr_gpu_destroy", "shoc_tr_gpu_step",
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
+    "shoc_tr_gpu_mass_noalloc",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_launch_count", "shoc_tr_gpu_strerror",
 )
@@ -52,6 +53,7 @@ def lib(path=None):
     L.shoc_tr_gpu_run.argtypes = [H, C.c_int]
     L.shoc_tr_gpu_sync.argtypes = [H, C.POINTER(_abi.Diag)]
     L.shoc_tr_gpu_mass.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_stream.argtypes = [H]
     L.shoc_tr_gpu_stream.restype = C.c_void_p
     L.shoc_tr_gpu_set_tiling.argtypes = [H, C.c_int, C.c_int]
@@ -165,6 +167,12 @@ class TracerStep:
     def mass(self):
         m = np.zeros(self.case.ntr)
         _check("mass", self.L.shoc_tr_gpu_mass(self.h, _abi.dptr(m)))
+        return m
+
+    def mass_noalloc(self):
+        """mass() through the entry point that allocates no device memory."""
+        m = np.zeros(self.case.ntr)
+        _check("mass_noalloc", self.L.shoc_tr_gpu_mass_noalloc(self.h, _abi.dptr(m)))
         return m
 
     def stream(self):

@@ -84,6 +84,19 @@ int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag);
  * accumulated in FP64 with compensated (Neumaier) summation.  mass[ntr]. */
 int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
 
+/* The same mass reduction, allocating nothing (no counterpart in the
+ * reference: an addition of this library).  For callers that must not
+ * allocate device memory while they run -- code inside a stream capture, and
+ * host frameworks that serve all device memory from their own fixed pool.
+ * The per-block partial sums go to a fixed device array of about 152 KB
+ * (room for 64 tracers); with more tracers it returns SHOC_TR_ESCRATCH.
+ * The first call on a device looks the array's device address up once
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the one array: calls whose GPU work overlaps in time (two
+ * handles on different streams, say) race and must be serialised by the
+ * caller.  mass[ntr] is host memory; the call waits for the result. */
+int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass);
+
 /* cudaStream_t of the handle, for event timing by the caller. */
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
 
