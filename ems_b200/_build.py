@@ -17,7 +17,7 @@ INCLUDE = os.path.join(ROOT, "include")
 
 GRID_SRC = ["shoc_grid.c"]
 GPU_SRC = ["shoc_tr_gpu.cu"]
-GPU_HDR = ["shoc_tr_kernels.cuh"]
+GPU_HDR = ["shoc_tr_kernels.cuh", "shoc_tr_stage.cuh"]
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -497,6 +497,55 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
   }
 }
 
+template <bool L, bool Q, bool U>
+cudaError_t smem_attr_one() {
+  return cudaFuncSetAttribute(k_stage32<L, Q, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              227 * 1024);
+}
+cudaError_t set_smem_attr_stage32() {
+  cudaError_t e = cudaSuccess;
+  cudaError_t r[8] = {smem_attr_one<true, true, true>(),   smem_attr_one<true, true, false>(),
+                      smem_attr_one<true, false, true>(),  smem_attr_one<true, false, false>(),
+                      smem_attr_one<false, true, true>(),  smem_attr_one<false, true, false>(),
+                      smem_attr_one<false, false, true>(), smem_attr_one<false, false, false>()};
+  for (auto x : r)
+    if (x != cudaSuccess) e = x;
+  return e;
+}
+
+// the FP32-mixed transport kernel for this step's scheme / limiter / sub-step
+template <bool L>
+void launch_stage32_l(bool q, bool u, int grid, dim3 blk, size_t smem, cudaStream_t st,
+                      const Geo &G, const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
+                      const TrSet &T, const SubStep &ss, const f32::Face2 *fx2,
+                      const f32::Face2 *fy2, const float *tin, float *tout, int nw, int nchunk,
+                      int any_hd) {
+  if (q && u)
+    k_stage32<L, true, true><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
+                                                      nw, nchunk, any_hd);
+  else if (q)
+    k_stage32<L, true, false><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
+                                                       nw, nchunk, any_hd);
+  else if (u)
+    k_stage32<L, false, true><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
+                                                       nw, nchunk, any_hd);
+  else
+    k_stage32<L, false, false><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin,
+                                                        tout, nw, nchunk, any_hd);
+}
+void launch_stage32(bool last, bool q, bool u, int grid, dim3 blk, size_t smem, cudaStream_t st,
+                    const Geo &G, const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
+                    const TrSet &T, const SubStep &ss, const f32::Face2 *fx2,
+                    const f32::Face2 *fy2, const float *tin, float *tout, int nw, int nchunk,
+                    int any_hd) {
+  if (last)
+    launch_stage32_l<true>(q, u, grid, blk, smem, st, G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
+                           nw, nchunk, any_hd);
+  else
+    launch_stage32_l<false>(q, u, grid, blk, smem, st, G, F, F3, W, O, T, ss, fx2, fy2, tin,
+                            tout, nw, nchunk, any_hd);
+}
+
 size_t stage32_smem(int nz, int nw) {
   return 3 * 32 * sizeof(f32::Stage) + (size_t)nz * 32 * sizeof(int) +
          (size_t)nz * 32 * sizeof(float4) + (size_t)nz * nw * 32 * sizeof(float);
@@ -836,10 +885,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
                            227 * 1024) != cudaSuccess ||
       cudaFuncSetAttribute(k_transport<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
-      cudaFuncSetAttribute(k_stage32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           227 * 1024) != cudaSuccess ||
-      cudaFuncSetAttribute(k_stage32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           227 * 1024) != cudaSuccess)
+      set_smem_attr_stage32() != cudaSuccess)
     TRY(SHOC_TR_ECUDA);
 #undef TRY
   *out = h;
@@ -933,14 +979,9 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
         cudaEventCreate(&e1);
         cudaEventRecord(e0, st);
       }
-      if (last)
-        k_stage32<true><<<ntile * nchunk, blk32, smem32, st>>>(
-            h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2, tin, tout, nw, nchunk,
-            h->any_hdiff ? 1 : 0);
-      else
-        k_stage32<false><<<ntile * nchunk, blk32, smem32, st>>>(
-            h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2, tin, tout, nw, nchunk,
-            h->any_hdiff ? 1 : 0);
+      launch_stage32(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, ntile * nchunk,
+                     blk32, smem32, st, h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2,
+                     tin, tout, nw, nchunk, h->any_hdiff ? 1 : 0);
       if (prof) {
         cudaEventRecord(e1, st);
         h->ev.push_back({e0, e1});

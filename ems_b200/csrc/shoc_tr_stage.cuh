@@ -40,17 +40,22 @@ constexpr int SH_XM1 = 1, SH_XM2 = 2, SH_XP1 = 4, SH_XP2 = 8;
 
 namespace f32 {
 
-// F = tm1 + a (t0 - tm1) - b curv,   curv = A tX + B tY - 2 tZ
-// (the QUICKEST face value of quickest(), tracers.c:1870-1884, with the
-// tracer-independent factors folded: a = d - cr/2, b = (1 - cr^2)/6, A/B the
-// metric-weighted curvature factors of the upwind side), then ULTIMATE with
-// ircr = 1/|cr|, times the volume flux U, minus K (t0 - tm1) for horizontal
-// diffusion.  Van Leer uses a = 0.5 (1 -+ cr) and the flux-limiter form.
+// QUICKEST (quickest(), tracers.c:1870-1884) is, for a given sign of the
+// Courant number, linear in the four stencil values:
+//   F = w0 tm2 + w1 tm1 + w2 t0 + w3 tp1
+// with the tracer-independent weights folded by the staging warps from
+// a = d - cr/2, b = (1 - cr^2)/6 and the upwind curvature factors A, B:
+//   cr > 0: w0 = -b B, w1 = 1 - a + 2b, w2 = a - b A, w3 = 0
+//   cr < 0: w0 = 0,    w1 = 1 - a - b B, w2 = a + 2b, w3 = -b A
+//   cr = 0: w1 = 1 - d, w2 = d
+// Van Leer keeps w0 = (1 -+ cr)/2 and its flux-limiter form.  Then ULTIMATE
+// (ircr = 1/|cr|), times the volume flux U, minus K (t0 - tm1) for horizontal
+// diffusion.  A face that carries nothing has all weights, U and K zero.
 struct Face {
-  float a, b, A, B, ircr, U, K;
-  int mode;
+  float w0, w1, w2, w3, ircr, U, K;
+  int bits;
 };
-constexpr int FM_POS = 1, FM_NEG = 2, FM_ULT = 4, FM_ON = 8, FM_HD = 16;
+constexpr int FB_POS = 1, FB_NEG = 2, FB_ULT = 4;
 
 struct Stage {
   int c, zp1;
@@ -68,26 +73,38 @@ struct Face2 {
   float ih;                 // 1 / h1au1 (x) or 1 / h2au2 (y) of the face's column
 };
 
-__device__ __forceinline__ void set_face_h(Face &f, bool on, float cr, const Face2 &m, float U,
-                                           bool ult, int trasc, float K, bool hd) {
-  f.mode = 0;
-  if (!on) return;
-  f.mode = FM_ON | (cr > 0.f ? FM_POS : 0) | (cr < 0.f ? FM_NEG : 0) | (ult ? FM_ULT : 0) |
-           (hd ? FM_HD : 0);
-  if (trasc == SHOC_TR_QUICKEST) {
-    f.a = m.d - 0.5f * cr;
-    f.b = (1.f - cr * cr) * (1.f / 6.f);
+__device__ __forceinline__ void face_zero(Face &f) {
+  f.w0 = f.w1 = f.w2 = f.w3 = 0.f;
+  f.ircr = f.U = f.K = 0.f;
+  f.bits = 0;
+}
+
+// weights of one face from its Courant number and metric factors
+__device__ __forceinline__ void set_face(Face &f, bool quick, float cr, float d, float Ap,
+                                         float Bp, float Am, float Bm, float U, bool ult,
+                                         float K) {
+  f.bits = (cr > 0.f ? FB_POS : 0) | (cr < 0.f ? FB_NEG : 0) | ((ult && cr != 0.f) ? FB_ULT : 0);
+  if (quick) {
+    const float a = d - 0.5f * cr, b = (1.f - cr * cr) * (1.f / 6.f);
     if (cr > 0.f) {
-      f.A = m.Ap;
-      f.B = m.Bp;
+      f.w0 = -b * Bp;
+      f.w1 = 1.f - a + 2.f * b;
+      f.w2 = a - b * Ap;
+      f.w3 = 0.f;
+    } else if (cr < 0.f) {
+      f.w0 = 0.f;
+      f.w1 = 1.f - a - b * Bm;
+      f.w2 = a + 2.f * b;
+      f.w3 = -b * Am;
     } else {
-      f.A = m.Am;
-      f.B = m.Bm;
+      f.w0 = 0.f;
+      f.w1 = 1.f - d;
+      f.w2 = d;
+      f.w3 = 0.f;
     }
   } else {
-    f.a = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
-    f.b = 0.f;
-    f.A = f.B = 0.f;
+    f.w0 = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
+    f.w1 = f.w2 = f.w3 = 0.f;
   }
   f.ircr = cr != 0.f ? __fdividef(1.f, fabsf(cr)) : 0.f;
   f.U = U;
@@ -95,56 +112,45 @@ __device__ __forceinline__ void set_face_h(Face &f, bool on, float cr, const Fac
 }
 
 // one face value: tm2..tp1 at i-2..i+1 of the face's cell
-__device__ __forceinline__ float face(const Face &f, int trasc, bool adv, bool hd, float tm2,
-                                      float tm1, float t0, float tp1) {
-  const int md = f.mode;
-  if (!(md & FM_ON)) return 0.f;
-  const bool pos = (md & FM_POS) != 0, neg = (md & FM_NEG) != 0;
+template <bool QUICK, bool ULT>
+__device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm2, float tm1,
+                                      float t0, float tp1) {
   float F = 0.f;
   if (adv) {
-    if (trasc == SHOC_TR_QUICKEST) {
-      // upwind-side curvature: A tX + B tY - 2 tZ
-      const float X = pos ? t0 : tp1, Y = pos ? tm2 : tm1, Z = pos ? tm1 : t0;
-      const float curv = (pos || neg) ? f.A * X + f.B * Y - 2.f * Z : 0.f;
-      F = tm1 + f.a * (t0 - tm1) - f.b * curv;
-    } else if (pos || neg) {
+    const bool pos = (f.bits & FB_POS) != 0;
+    if (QUICK) {
+      F = f.w0 * tm2 + f.w1 * tm1 + f.w2 * t0 + f.w3 * tp1;
+    } else {
+      const bool neg = (f.bits & FB_NEG) != 0;
       const float p = pos ? (tm1 - tm2) : (t0 - tm1), q = pos ? (t0 - tm1) : (tp1 - t0);
       const float den = pos ? (t0 - tm2) : (tp1 - tm1);
-      float df = p * q;
-      df = df > 0.f ? 2.f * __fdividef(df, den) : 0.f;
-      F = pos ? tm1 + f.a * df : t0 - f.a * df;
+      const float pq = p * q;
+      const float df = pq > 0.f ? 2.f * __fdividef(pq, den) : 0.f;
+      F = pos ? tm1 + f.w0 * df : (neg ? t0 - f.w0 * df : 0.f);
     }
-    if ((md & FM_ULT) && (pos || neg)) {
+    if (ULT && (f.bits & FB_ULT)) {
+      // ulimate_filter (tracers.c:3526-3554) as selects
       const float tc = pos ? tm1 : t0, tu = pos ? tm2 : tp1, td = pos ? t0 : tm1;
       const float diff = td - tu;
-      float nc = 0.f, nu = 0.f;
-      if (diff != 0.f) {
-        const float r = __fdividef(1.f, diff);
-        nc = (tc - tu) * r;
-        nu = (F - tu) * r;
-      }
-      const float lim = tu + nc * diff;
-      if (diff == 0.f && tc != tu) {
-        // Upwind and downwind values equal in FP32.  In FP64 they almost
-        // always differ by a few ulps, nc is then huge and the limiter
-        // falls back to upwind (tc); follow that rather than the exact-tie
-        // case (which leaves the face unlimited), so FP32 rounding of the
-        // stored tracer does not flip the limiter's decision.
-        F = tc;
-      } else if (nc >= 0.f && nc <= 1.f) {
-        if (nu > 1.f)
-          F = td;
-        else if (nu < nc)
-          F = lim;
-        else if (nu > nc * f.ircr)
-          F = tu + nc * diff * f.ircr;
-      } else {
-        F = lim;
-      }
+      const float r = __fdividef(1.f, diff);
+      const float nc = (tc - tu) * r, nu = (F - tu) * r;
+      const float ncd = nc * diff;
+      const float lim = tu + ncd;
+      float G = F;
+      if (nu > nc * f.ircr) G = tu + ncd * f.ircr;
+      if (nu < nc) G = lim;
+      if (nu > 1.f) G = td;
+      if (!(nc >= 0.f && nc <= 1.f)) G = lim;
+      // Upwind and downwind values equal in FP32: in FP64 they almost always
+      // differ by a few ulps, nc is then huge and the limiter falls back to
+      // upwind (tc); follow that rather than the exact-tie case (which
+      // leaves the face unlimited), so FP32 rounding of the stored tracer
+      // does not flip the limiter's decision.
+      F = (diff == 0.f) ? (tc != tu ? tc : F) : G;
     }
     F *= f.U;
   }
-  if (hd && (md & FM_HD)) F -= f.K * (t0 - tm1);
+  if (hd) F -= f.K * (t0 - tm1);
   return F;
 }
 
@@ -164,16 +170,21 @@ __device__ __forceinline__ void stage_hface(Face &f, int c, bool x, const Geo &G
                                             const Face2 *m2) {
   const uint8_t EB = x ? CF_E1 : CF_E2;
   const uint8_t fc = G.cflag[c];
+  const bool quick = O.trasc == SHOC_TR_QUICKEST;
   if (!(fc & CF_WET)) {  // a ghost: the face carries nothing
-    f.mode = 0;
+    face_zero(f);
     return;
   }
   const Face2 m = m2[G.m2d[c]];
   const float cr = (x ? F3.u1[c] : F3.u2[c]) * fdtu * m.ih;
-  const bool quick = O.trasc == SHOC_TR_QUICKEST;
-  set_face_h(f, quick ? true : (fc & EB) != 0, cr, m, x ? F3.u1flux3d[c] : F3.u2flux3d[c],
-             O.ultimate && (fc & EB), O.trasc, any_hd ? (x ? F3.khx[c] : F3.khy[c]) : 0.f,
-             any_hd);
+  const float K = any_hd ? (x ? F3.khx[c] : F3.khy[c]) : 0.f;
+  if (!quick && !(fc & EB)) {  // Van Leer advects interior faces only
+    face_zero(f);
+    f.K = K;
+    return;
+  }
+  set_face(f, quick, cr, m.d, m.Ap, m.Bp, m.Am, m.Bm, x ? F3.u1flux3d[c] : F3.u2flux3d[c],
+           O.ultimate && (fc & EB), K);
 }
 
 __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, int kb, int ks,
@@ -220,21 +231,21 @@ __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, 
       break;
     }
     case 1:
-      if (on) stage_hface(S.fxw, c, true, G, F3, O, any_hd, fdtu, fx2); else S.fxw.mode = 0;
+      if (on) stage_hface(S.fxw, c, true, G, F3, O, any_hd, fdtu, fx2); else face_zero(S.fxw);
       break;
     case 2:
-      if (on) stage_hface(S.fxe, G.xp1[c], true, G, F3, O, any_hd, fdtu, fx2); else S.fxe.mode = 0;
+      if (on) stage_hface(S.fxe, G.xp1[c], true, G, F3, O, any_hd, fdtu, fx2); else face_zero(S.fxe);
       break;
     case 3:
-      if (on) stage_hface(S.fys, c, false, G, F3, O, any_hd, fdtu, fy2); else S.fys.mode = 0;
+      if (on) stage_hface(S.fys, c, false, G, F3, O, any_hd, fdtu, fy2); else face_zero(S.fys);
       break;
     case 4:
-      if (on) stage_hface(S.fyn, G.yp1[c], false, G, F3, O, any_hd, fdtu, fy2); else S.fyn.mode = 0;
+      if (on) stage_hface(S.fyn, G.yp1[c], false, G, F3, O, any_hd, fdtu, fy2); else face_zero(S.fyn);
       break;
     case 5: {
       Face &fz = S.fzb;
       if (!on) {
-        fz.mode = 0;
+        face_zero(fz);
         break;
       }
       const int zp1 = G.zp1[c];
@@ -247,7 +258,7 @@ __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, 
       }
       wk.dz0 = W.dz32[c];
       if (k > ks) {  // above the surface: no z face
-        fz.mode = 0;
+        face_zero(fz);
         break;
       }
       const float dzp1 = W.dz32[zp1];
@@ -257,27 +268,9 @@ __device__ __forceinline__ void stage_part(int part, int k, int lane, bool act, 
       const float w9p = (zp1 == c) ? w90 : 0.5f * (dzp1 + wk.dz0);
       const float wv = F3.w[c] * fdtu;
       const float cz = __fdividef(wv, w90);
-      fz.mode = FM_ON | (cz > 0.f ? FM_POS : 0) | (cz < 0.f ? FM_NEG : 0) |
-                (O.ultimate ? FM_ULT : 0);
-      if (O.trasc == SHOC_TR_QUICKEST) {
-        fz.a = __fdividef(wk.dzm1, wk.dzm1 + wk.dz0) - 0.5f * cz;
-        fz.b = (1.f - cz * cz) * (1.f / 6.f);
-        if (cz > 0.f) {
-          const float db = __fdividef(2.f, w9m + w90);
-          fz.A = db * w9m;
-          fz.B = db * w90;
-        } else {
-          const float df = __fdividef(2.f, w90 + w9p);
-          fz.A = df * w90;
-          fz.B = df * w9p;
-        }
-      } else {
-        fz.a = cz > 0.f ? 0.5f * (1.f - cz) : 0.5f * (1.f + cz);
-        fz.b = fz.A = fz.B = 0.f;
-      }
-      fz.ircr = cz != 0.f ? __fdividef(1.f, fabsf(cz)) : 0.f;
-      fz.U = wv;
-      fz.K = 0.f;
+      const float db = __fdividef(2.f, w9m + w90), df = __fdividef(2.f, w90 + w9p);
+      set_face(fz, O.trasc == SHOC_TR_QUICKEST, cz, __fdividef(wk.dzm1, wk.dzm1 + wk.dz0),
+               db * w9m, db * w90, df * w90, df * w9p, wv, O.ultimate != 0, 0.f);
       break;
     }
     default: {  // 6
@@ -302,7 +295,7 @@ __device__ __forceinline__ void neumaier_add(double &s, double &comp, double v) 
 //
 // Shared memory: Stage[3][32] | int colC[nz][32] | float4 colLU[nz][32] |
 // float Sv[nz][nw][32] (per tracer-lane Thomas storage).
-template <bool LAST>
+template <bool LAST, bool QUICK, bool ULT>
 __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work W, Opt O,
                                                  TrSet T, SubStep ss, const f32::Face2 *fx2,
                                                  const f32::Face2 *fy2,
@@ -458,14 +451,14 @@ __global__ void __launch_bounds__(256) k_stage32(Geo G, Flow F, Flow32 F3, Work 
       const float txm1 = (sh & SH_XM1) ? u1v : cur.xm1;
       const float txm2 = (sh & SH_XM2) ? u2v : cur.xm2;
       const float txp1 = (sh & SH_XP1) ? d1v : cur.xp1;
-      Fxw = face(S.fxw, O.trasc, adv, hd, txm2, txm1, t0, txp1);
-      Fys = face(S.fys, O.trasc, adv, hd, cur.ym2, cur.ym1, t0, cur.yp1);
-      Fyn = face(S.fyn, O.trasc, adv, hd, cur.ym1, t0, cur.yp1, cur.yp2);
+      Fxw = face<QUICK, ULT>(S.fxw, adv, hd, txm2, txm1, t0, txp1);
+      Fys = face<QUICK, ULT>(S.fys, adv, hd, cur.ym2, cur.ym1, t0, cur.yp1);
+      Fyn = face<QUICK, ULT>(S.fyn, adv, hd, cur.ym1, t0, cur.yp1, cur.yp2);
       if (!(sh & SH_XP1)) {
         const float txp2 = (sh & SH_XP2) ? d2v : cur.xp2;
-        Fxe = face(S.fxe, O.trasc, adv, hd, txm1, t0, txp1, txp2);
+        Fxe = face<QUICK, ULT>(S.fxe, adv, hd, txm1, t0, txp1, txp2);
       }
-      if (adv) Fzb = face(S.fzb, O.trasc, true, false, tm2, tm1, t0, tp1);
+      if (adv) Fzb = face<QUICK, ULT>(S.fzb, true, false, tm2, tm1, t0, tp1);
     }
     const float Fnext = __shfl_down_sync(0xffffffffu, Fxw, 1);
     if (on) {
