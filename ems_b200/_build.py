@@ -16,8 +16,9 @@ LIBDIR = os.path.join(HERE, "_lib")
 INCLUDE = os.path.join(ROOT, "include")
 
 GRID_SRC = ["shoc_grid.c"]
-GPU_SRC = ["shoc_tr_gpu.cu"]
-GPU_HDR = ["shoc_tr_kernels.cuh", "shoc_tr_stage.cuh"]
+# (source, FMA contraction): the FP64 reference path must not contract
+GPU_SRC = [("shoc_tr_gpu.cu", False), ("shoc_tr_f32.cu", True)]
+GPU_HDR = ["shoc_tr_kernels.cuh", "shoc_tr_stage.cuh", "shoc_tr_tile.cuh", "shoc_tr_launch.h"]
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -58,17 +59,24 @@ def grid_lib(force=False):
 def gpu_lib(force=False, verbose=False):
     os.makedirs(LIBDIR, exist_ok=True)
     out = os.path.join(LIBDIR, "libshoc_tr_gpu.so")
-    srcs = [os.path.join(CSRC, s) for s in GPU_SRC]
+    srcs = [os.path.join(CSRC, s) for s, _ in GPU_SRC]
     deps = srcs + [os.path.join(CSRC, h) for h in GPU_HDR] + [
         os.path.join(INCLUDE, "shoc_tr.h"), os.path.join(INCLUDE, "shoc_tr_gpu.h")]
     if force or _stale(out, deps):
-        cmd = [_nvcc()] + NVCC_ARCH + [
-            "-O3", "-lineinfo", "-std=c++17", "--fmad=false",
-            "-Xcompiler", "-fPIC", "-shared", "-I", INCLUDE, "-I", CSRC,
-            "-o", out] + srcs
-        if verbose:
-            cmd.insert(1, "-Xptxas=-v")
-        log = _run(cmd)
+        objs = []
+        log = ""
+        for (name, fmad), src in zip(GPU_SRC, srcs):
+            obj = os.path.join(LIBDIR, os.path.splitext(name)[0] + ".o")
+            cmd = [_nvcc()] + NVCC_ARCH + [
+                "-O3", "-lineinfo", "-std=c++17", "--fmad=%s" % ("true" if fmad else "false"),
+                "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC, "-c", "-o", obj, src]
+            if verbose:
+                cmd.insert(1, "-Xptxas=-v")
+            log += _run(cmd)
+            objs.append(obj)
+        log += _run([_nvcc()] + NVCC_ARCH + ["-shared", "-o", out] + objs)
+        for o in objs:
+            os.remove(o)
         if verbose:
             sys.stdout.write(log)
     return out

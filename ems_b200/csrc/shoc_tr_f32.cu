@@ -1,0 +1,64 @@
+// shoc_tr_f32.cu -- the FP32-mixed transport kernels' instances and their
+// launcher.  Compiled with FMA contraction on (the FP64 reference path in
+// shoc_tr_gpu.cu is compiled without it); the FP64 sums of the kernels use
+// explicitly rounded operations where contraction would change them.
+#include "shoc_tr_launch.h"
+
+namespace shoc {
+
+namespace {
+template <class K>
+cudaError_t attr(K k) {
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+template <bool Q, bool U>
+void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
+         const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
+         const float *tin, float *tout, float *fzs, int hd) {
+  k_adv32<Q, U><<<grid, kAdvBlock, 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+}
+}  // namespace
+
+cudaError_t tile32_set_smem_attr() {
+  cudaError_t e = cudaSuccess;
+  const cudaError_t r[6] = {attr(k_adv32<true, true>),  attr(k_adv32<true, false>),
+                            attr(k_adv32<false, true>), attr(k_adv32<false, false>),
+                            attr(k_vd32<true>),         attr(k_vd32<false>)};
+  for (auto x : r)
+    if (x != cudaSuccess) e = x;
+  return e;
+}
+
+void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo &G,
+                    const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
+                    const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
+                    const f32::Face2 *fy2, const float *tin, float *tout, float *fzs, int vd_nw,
+                    int any_hd, cudaEvent_t *ev) {
+  const int ntile = Tl.ncolp / 32;
+  if (ev) cudaEventRecord(ev[0], st);
+  if (T.ntb > 0 && Tl.nwet > 0) {
+    const int grid = (Tl.nwet + kAdvBlock - 1) / kAdvBlock;
+    if (quick && ult)
+      adv<true, true>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+    else if (quick)
+      adv<true, false>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+    else if (ult)
+      adv<false, true>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+    else
+      adv<false, false>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  const int nchunk = (T.nslot + vd_nw - 1) / vd_nw;
+  const size_t smem = vd32_smem(G.nz, vd_nw);
+  const dim3 blk(32, vd_nw);
+  if (last)
+    k_vd32<true><<<ntile * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
+                                                     tout, fzs, vd_nw, nchunk);
+  else
+    k_vd32<false><<<ntile * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
+                                                      tout, fzs, vd_nw, nchunk);
+  if (ev) cudaEventRecord(ev[2], st);
+}
+
+}  // namespace shoc

@@ -29,13 +29,14 @@
 
 #include "shoc_tr_gpu.h"
 #include "shoc_tr_kernels.cuh"
-#include "shoc_tr_stage.cuh"
+#include "shoc_tr_launch.h"
 
 using namespace shoc;
 
 namespace {
 
 constexpr int kItermax = 20;  // tracers.c:430
+constexpr int kSerialBlocks = 148 * 2;  // general-path kernel: one thread per listed column
 
 struct Sched {
   double dtm = 0.0;
@@ -64,7 +65,9 @@ struct shoc_tr_gpu {
   double *xfer = nullptr;             // one tracer of FP64, for FP32 upload / download
   Flow32 F3{};
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
-  bool staged = false;                // layer-synchronous fast path
+  Tile tl{};                          // static tables of the column-tile kernels
+  float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
+  bool staged = false;                // column-tile fast path
   int cur = 0;
   int *bpt = nullptr, *bin = nullptr;
   // host mirror of the per-tracer flags
@@ -74,6 +77,7 @@ struct shoc_tr_gpu {
   bool have_sched = false;
   Sched sched;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_launches[2] = {0, 0};
   int graph_nsub = -1;
   // tiling
   int tw = 8;
@@ -497,58 +501,99 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
   }
 }
 
-template <bool L, bool Q, bool U>
-cudaError_t smem_attr_one() {
-  return cudaFuncSetAttribute(k_stage32<L, Q, U>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              227 * 1024);
-}
-cudaError_t set_smem_attr_stage32() {
-  cudaError_t e = cudaSuccess;
-  cudaError_t r[8] = {smem_attr_one<true, true, true>(),   smem_attr_one<true, true, false>(),
-                      smem_attr_one<true, false, true>(),  smem_attr_one<true, false, false>(),
-                      smem_attr_one<false, true, true>(),  smem_attr_one<false, true, false>(),
-                      smem_attr_one<false, false, true>(), smem_attr_one<false, false, false>()};
-  for (auto x : r)
-    if (x != cudaSuccess) e = x;
-  return e;
-}
-
-// the FP32-mixed transport kernel for this step's scheme / limiter / sub-step
-template <bool L>
-void launch_stage32_l(bool q, bool u, int grid, dim3 blk, size_t smem, cudaStream_t st,
-                      const Geo &G, const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
-                      const TrSet &T, const SubStep &ss, const f32::Face2 *fx2,
-                      const f32::Face2 *fy2, const float *tin, float *tout, int nw, int nchunk,
-                      int any_hd) {
-  if (q && u)
-    k_stage32<L, true, true><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
-                                                      nw, nchunk, any_hd);
-  else if (q)
-    k_stage32<L, true, false><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
-                                                       nw, nchunk, any_hd);
-  else if (u)
-    k_stage32<L, false, true><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
-                                                       nw, nchunk, any_hd);
-  else
-    k_stage32<L, false, false><<<grid, blk, smem, st>>>(G, F, F3, W, O, T, ss, fx2, fy2, tin,
-                                                        tout, nw, nchunk, any_hd);
-}
-void launch_stage32(bool last, bool q, bool u, int grid, dim3 blk, size_t smem, cudaStream_t st,
-                    const Geo &G, const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
-                    const TrSet &T, const SubStep &ss, const f32::Face2 *fx2,
-                    const f32::Face2 *fy2, const float *tin, float *tout, int nw, int nchunk,
-                    int any_hd) {
-  if (last)
-    launch_stage32_l<true>(q, u, grid, blk, smem, st, G, F, F3, W, O, T, ss, fx2, fy2, tin, tout,
-                           nw, nchunk, any_hd);
-  else
-    launch_stage32_l<false>(q, u, grid, blk, smem, st, G, F, F3, W, O, T, ss, fx2, fy2, tin,
-                            tout, nw, nchunk, any_hd);
-}
-
-size_t stage32_smem(int nz, int nw) {
-  return 3 * 32 * sizeof(f32::Stage) + (size_t)nz * 32 * sizeof(int) +
-         (size_t)nz * 32 * sizeof(float4) + (size_t)nz * nw * 32 * sizeof(float);
+// Static tables of the column-tile kernel: the cell of every column at every
+// layer (cells are numbered layer by layer, so a column's cells are found by
+// walking zp1 up from its bottom cell), the first and second horizontal
+// neighbours of every cell, the 2D cells of its east and north neighbours and
+// their flags.
+int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<uint8_t> &cflag,
+                      const std::vector<int> &col_bot, const std::vector<int> &col_kb) {
+  const int S = h->S, nz = h->nz, ncol = h->ncol;
+  const int ncolp = (ncol + 31) / 32 * 32;
+  std::vector<int> cellk((size_t)nz * ncolp, 0);
+  for (int col = 0; col < ncol; col++) {
+    int c = col_bot[col];
+    for (int k = col_kb[col]; k < nz; k++) {
+      if (c <= 0 || c >= S) break;
+      cellk[(size_t)k * ncolp + col] = c;
+      c = g->zp1[c];
+    }
+  }
+  auto in = [S](int c) { return c >= 0 && c < S ? c : 0; };
+  const int S2 = h->S2;
+  auto in2 = [S2](int c) { return c >= 0 && c < S2 ? c : 0; };
+  std::vector<int4> nb1(S), nb2(S);
+  std::vector<int2> m2e(S);
+  std::vector<uint8_t> fl(S);
+  for (int c = 0; c < S; c++) {
+    const int xm = in(g->xm1[c]), xp = in(g->xp1[c]), ym = in(g->ym1[c]), yp = in(g->yp1[c]);
+    nb1[c] = make_int4(xm, xp, ym, yp);
+    nb2[c] = make_int4(in(g->xm1[xm]), in(g->xp1[xp]), in(g->ym1[ym]), in(g->yp1[yp]));
+    m2e[c] = make_int2(in2(g->m2d[xp]), in2(g->m2d[yp]));
+    uint8_t f = cflag[c] & (CF_WET | CF_E1 | CF_E2);
+    if (cflag[xp] & CF_WET) f |= FL_XP_WET;
+    if (cflag[xp] & CF_E1) f |= FL_XP_E1;
+    if (cflag[yp] & CF_WET) f |= FL_YP_WET;
+    if (cflag[yp] & CF_E2) f |= FL_YP_E2;
+    fl[c] = f;
+  }
+  // vertical neighbours and the column of each wet cell
+  std::vector<int4> nbz(S);
+  for (int c = 0; c < S; c++) {
+    const int zm = in(g->zm1[c]), zp = in(g->zp1[c]);
+    nbz[c] = make_int4(zm, in(g->zm1[zm]), zp, in(g->zp1[zp]));
+  }
+  std::vector<int> colof(S, 0);
+  for (int col = 0; col < ncol; col++)
+    for (int k = col_kb[col]; k < nz; k++) {
+      const int c = cellk[(size_t)k * ncolp + col];
+      if (c) colof[c] = col;
+    }
+  std::vector<int> wet;
+  wet.reserve(g->a3_t);
+  for (int i = 1; i <= g->a3_t; i++) {
+    const int c = g->w3_t[i];
+    if (c > 0 && c < S) wet.push_back(c);
+  }
+  // k_vd32 column order: deepest first, so a block's lanes span similar
+  // layer ranges
+  std::vector<int> vdcol(ncolp, -1);
+  {
+    std::vector<int> ord(ncol);
+    for (int i = 0; i < ncol; i++) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(),
+                     [&](int a, int b) { return col_kb[a] < col_kb[b]; });
+    for (int i = 0; i < ncol; i++) vdcol[i] = ord[i];
+  }
+  Tile &T = h->tl;
+  T.ncolp = ncolp;
+  T.nwet = (int)wet.size();
+  int *ip;
+  int rc;
+  if ((rc = dupload(h, &ip, cellk.data(), cellk.size()))) return rc;
+  T.cellk = ip;
+  int4 *i4;
+  if ((rc = dupload(h, &i4, nb1.data(), S))) return rc;
+  T.nb1 = i4;
+  if ((rc = dupload(h, &i4, nb2.data(), S))) return rc;
+  T.nb2 = i4;
+  int2 *i2;
+  if ((rc = dupload(h, &i2, m2e.data(), S))) return rc;
+  T.m2e = i2;
+  uint8_t *u8;
+  if ((rc = dupload(h, &u8, fl.data(), S))) return rc;
+  T.fl = u8;
+  if ((rc = dupload(h, &ip, g->s2k, S))) return rc;
+  T.kof = ip;
+  if ((rc = dupload(h, &i4, nbz.data(), S))) return rc;
+  T.nbz = i4;
+  if ((rc = dupload(h, &ip, colof.data(), S))) return rc;
+  T.colof = ip;
+  if ((rc = dupload(h, &ip, wet.data(), wet.size()))) return rc;
+  T.wet = ip;
+  if ((rc = dupload(h, &ip, vdcol.data(), vdcol.size()))) return rc;
+  T.vdcol = ip;
+  return 0;
 }
 
 int map_status(int st) {
@@ -778,6 +823,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TrSet &T = h->T;
   T.ntr = ntr;
   T.nslot = h->nslot;
+  T.ntb = o->ntbdy;
   TRY(dupload(h, &ip, slot.data(), slot.size())); T.slot_tr = ip;
   TRY(dupload(h, &u8, h->trf.data(), ntr)); T.trf = u8;
   TRY(dupload(h, &dp, o->mintr, ntr)); T.mintr = dp;
@@ -845,6 +891,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     }
     TRY(dupload(h, &h->fx2, ax.data(), S2));
     TRY(dupload(h, &h->fy2, ay.data(), S2));
+    TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
+    TRY(dupload<float>(h, &h->fzs, nullptr, (size_t)ntr * ncol));
   }
   // flow fields
   Flow &F = h->F;
@@ -872,8 +920,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   // tiling: tracers per block
   int tw = 8;
   if (h->staged) {
-    while (tw > 1 && stage32_smem(g->nz, tw) > 112 * 1024) tw--;
-    // balance the tracer chunks: the per-layer staging is shared by a block
+    // tracers per k_vd32 block: two blocks per SM, balanced chunks
+    while (tw > 1 && vd32_smem(g->nz, tw) > 113 * 1024) tw--;
     int nch = (h->nslot + tw - 1) / std::max(tw, 1);
     if (nch > 0) tw = (h->nslot + nch - 1) / nch;
     if (tw < 1) tw = 1;
@@ -885,7 +933,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
                            227 * 1024) != cudaSuccess ||
       cudaFuncSetAttribute(k_transport<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
-      set_smem_attr_stage32() != cudaSuccess)
+      tile32_set_smem_attr() != cudaSuccess)
     TRY(SHOC_TR_ECUDA);
 #undef TRY
   *out = h;
@@ -969,28 +1017,24 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
     if (h->staged && h->nslot > 0) {
       const float *tin = (const float *)h->tr[cur];
       float *tout = (float *)h->tr[cur ^ 1];
-      const int nw = tw;
-      size_t smem32 = stage32_smem(h->nz, nw);
-      dim3 blk32(32, nw);
       bool prof = h->profile && last;
-      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+      if (prof)
+        for (auto &e : ev) cudaEventCreate(&e);
+      tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
+                     h->F3, h->W, h->O, h->T, ss, h->tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
+                     h->any_hdiff ? 1 : 0, prof ? ev : nullptr);
       if (prof) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, st);
+        h->ev.push_back({ev[0], ev[2]});
+        cudaEventDestroy(ev[1]);
       }
-      launch_stage32(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, ntile * nchunk,
-                     blk32, smem32, st, h->G, h->F, h->F3, h->W, h->O, h->T, ss, h->fx2, h->fy2,
-                     tin, tout, nw, nchunk, h->any_hdiff ? 1 : 0);
-      if (prof) {
-        cudaEventRecord(e1, st);
-        h->ev.push_back({e0, e1});
-      }
-      h->launches++;
+      h->launches += 2;
       if (last)
-        k_serial<true, float><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                            tin, tout);
       else
-        k_serial<false, float><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<false, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                             tin, tout);
       h->launches++;
       cur ^= 1;
       continue;
@@ -1017,9 +1061,11 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
       }
       h->launches++;
       if (last)
-        k_serial<true, double><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<true, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                             tin, tout);
       else
-        k_serial<false, double><<<8, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tin, tout);
+        k_serial<false, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
+                                                              tin, tout);
       h->launches++;
     }
     cur ^= 1;
@@ -1098,11 +1144,11 @@ int step_async(shoc_tr_gpu *h) {
     CK(e);
     CK(cudaGraphInstantiate(&h->graph[gi], graph, 0));
     cudaGraphDestroy(graph);
+    h->graph_launches[gi] = h->launches - l0;  // kernels in the graph
     h->launches = l0;
   }
   CK(cudaGraphLaunch(h->graph[gi], h->stream));
-  h->launches += 2 + (h->nbpt > 0 ? 1 : 0) +
-                 (1 + (h->nslot > 0 ? 2 : 0)) * (long long)h->sched.sub.size();
+  h->launches += h->graph_launches[gi];
   if (h->sched.sub.size() & 1) h->cur ^= 1;
   return 0;
 }
@@ -1410,7 +1456,7 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
   if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
   if (tracers_per_block > 0) {
     if (tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
-    if (h->staged && stage32_smem(h->nz, tracers_per_block) > 227 * 1024)
+    if (h->staged && vd32_smem(h->nz, tracers_per_block) > 227 * 1024)
       return SHOC_TR_EUNSUPPORTED;
     if (!h->staged && (size_t)h->nz * tracers_per_block * 32 * sizeof(double) > 227 * 1024)
       return SHOC_TR_EUNSUPPORTED;

@@ -106,6 +106,7 @@ struct Opt {
 struct TrSet {
   int ntr;              // tracers in the handle
   int nslot;            // tracers this launch processes
+  int ntb;              // of which advected / diffused (tbdy), the first ntb slots
   const int *slot_tr;   // slot -> tracer number, tbdy order then the rest
   const uint8_t *trf;   // TR_* flags per tracer
   const double *mintr, *maxtr;

@@ -1,0 +1,499 @@
+// shoc_tr_tile.cuh -- the FP32-mixed transport kernels of the columns whose
+// surface cell stays in its layer during the step (staged columns).
+//
+// One sub-step is two launches:
+//
+//  k_adv32  advection and horizontal diffusion (advect_diffuse, tracers.c:
+//           849-925): one thread per wet cell, in SHOC's cell order (layer by
+//           layer, i fastest), so a warp's cells are adjacent cells of one
+//           layer and its loads coalesce.  The thread folds its cell's
+//           tracer-independent face coefficients once (QUICKEST weights,
+//           ULTIMATE 1/|cr|, volume flux, horizontal-diffusion factor) and
+//           then loops over the advected tracers, two at a time: the stencil
+//           values are independent loads, the west-face flux of the next
+//           lane's cell is this cell's east-face flux (shuffle).  Output, in
+//           the destination tracer array: the new value of cells below the
+//           surface, the FP64-summed horizontal flux divergence of the
+//           surface cell and the cells above it; the surface cell's
+//           bottom-face flux goes to a per-(tracer, column) array.
+//
+//  k_vd32   one thread per (column, tracer): tr_bounds (tracers.c:3217-3324),
+//           surf_conc's column-mass balance (:3097-3206, FP64 Neumaier), the
+//           copy above the surface and, on the last sub-step, the implicit
+//           vertical diffusion (implicit_vdiff_tr, :4067-4214) as an FP32
+//           Thomas sweep, an FP64 residual and one FP32 correction solve.
+//           A block owns 32 columns of similar depth (a static depth-sorted
+//           column order) so its lanes loop over similar layer ranges; the
+//           columns' values and LU factors are staged into shared memory in
+//           one batch of asynchronous copies.
+//
+// The cells of a column at every layer come from a static layer-by-column
+// table, so no thread walks a column to find them.
+#pragma once
+#include "shoc_tr_stage.cuh"
+
+namespace shoc {
+
+// Static per-cell / per-layer tables of the tile kernels (built once at
+// handle creation from the geometry maps).
+struct Tile {
+  const int *cellk;  // [nz][ncolp] cell of column col at layer k (0: none)
+  const int4 *nb1;   // [S] xm1, xp1, ym1, yp1
+  const int4 *nb2;   // [S] xm1(xm1), xp1(xp1), ym1(ym1), yp1(yp1)
+  const int2 *m2e;   // [S] m2d(xp1), m2d(yp1)
+  const uint8_t *fl; // [S] cflag(c) | xp1 wet, E1 | yp1 wet, E2 (FL_*)
+  const int *kof;    // [S] layer index of each cell (s2k)
+  const int4 *nbz;   // [S] zm1, zm1(zm1), zp1, zp1(zp1)
+  const int *colof;  // [S] 0-based column of each wet cell
+  const int *wet;    // [nwet] the wet cells (w3_t order)
+  const int *vdcol;  // [ncolp] columns in k_vd32 order (-1: padding)
+  int ncolp;         // columns rounded up to whole tiles
+  int nwet;
+};
+constexpr int FL_XP_WET = 8, FL_XP_E1 = 16, FL_YP_WET = 32, FL_YP_E2 = 64;
+
+// asynchronous global -> shared copies; a thread waits for its own copies
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// The column of lane `col` of a tile: whether the tile kernels handle it, its
+// bottom and surface layers, 2D cell and bottom cell.
+struct TileCol {
+  ColInfo ci;
+  int cbot, c2, kb, ks;
+  bool act;
+};
+__device__ __forceinline__ TileCol tile_column(const Geo &G, const Work &W, const Tile &Tl,
+                                               int col, bool report) {
+  TileCol t;
+  t.ci = {0, 0, 0, 0, 0};
+  t.cbot = t.c2 = t.ks = 0;
+  t.kb = G.nz;
+  t.act = col < G.ncol;
+  if (t.act) {
+    t.ci = W.col[col];
+    t.cbot = G.col_bot[col];
+    t.c2 = G.col_top[col];
+    t.act = staged_column(t.ci, t.cbot);
+  }
+  if (t.act) {
+    t.kb = G.col_kb[col];
+    t.ks = Tl.kof[t.ci.s];
+    // the surface cell must be this column's cell at its layer
+    if (t.ks < t.kb || t.ks >= G.nz || Tl.cellk[(size_t)t.ks * Tl.ncolp + col] != t.ci.s) {
+      t.act = false;
+      t.kb = G.nz;
+      if (report) atomicOr(W.status, ST_GEOM);
+    }
+  }
+  return t;
+}
+
+namespace f32 {
+
+// Face coefficients of one horizontal face at a cell with the given flags.
+__device__ __forceinline__ void hface(Face &f, bool wet, bool eb, bool quick, bool ult,
+                                      float cr, float U, float K, const Face2 &m) {
+  if (!wet) {  // a ghost: the face carries nothing
+    face_zero(f);
+    return;
+  }
+  if (!quick && !eb) {  // Van Leer advects interior faces only
+    face_zero(f);
+    f.K = K;
+    return;
+  }
+  set_face(f, quick, cr, m.d, m.Ap, m.Bp, m.Am, m.Bm, U, ult && eb, K);
+}
+
+// Vertical face at the bottom of a cell from the thicknesses of the two cells
+// below it (dzm2, dzm1), the cell (dz0) and the one above (dzp1; the
+// surface-layer cell maps onto itself, top != 0), and w * dtu.
+__device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2, float dzm1,
+                                      float dz0, float dzp1, bool top, float wv) {
+  const float w9m = 0.5f * (dzm1 + dzm2);
+  const float w90 = 0.5f * (dz0 + dzm1);
+  const float w9p = top ? w90 : 0.5f * (dzp1 + dz0);
+  const float cz = __fdividef(wv, w90);
+  const float db = __fdividef(2.f, w9m + w90), df = __fdividef(2.f, w90 + w9p);
+  set_face(f, quick, cz, __fdividef(dzm1, dzm1 + dz0), db * w9m, db * w90, df * w90, df * w9p,
+           wv, ult, 0.f);
+}
+
+}  // namespace f32
+
+// ---------------------------------------------------------------------------
+// k_adv32
+
+constexpr int kAdvBlock = 256;
+
+template <bool QUICK, bool ULT>
+__global__ void __launch_bounds__(kAdvBlock) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
+                                                     SubStep ss, Tile Tl,
+                                                     const f32::Face2 *__restrict__ fx2,
+                                                     const f32::Face2 *__restrict__ fy2,
+                                                     const float *__restrict__ tri,
+                                                     float *__restrict__ tro,
+                                                     float *__restrict__ fzs, int any_hd) {
+  using namespace f32;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int i = blockIdx.x * kAdvBlock + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int nz = G.nz;
+
+  // this thread's cell and its column
+  int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0;
+  if (i < Tl.nwet) {
+    c = Tl.wet[i];
+    col = Tl.colof[c];
+    const ColInfo ci = W.col[col];
+    const int cbot = G.col_bot[col];
+    if (staged_column(ci, cbot)) {
+      kb = G.col_kb[col];
+      ks = Tl.kof[ci.s];
+      k = Tl.kof[c];
+      c2 = G.col_top[col];
+      // the column's surface cell must be at its layer (k_vd32 reports it)
+      if (ks < kb || ks >= nz || k < kb || Tl.cellk[(size_t)ks * Tl.ncolp + col] != ci.s) c = 0;
+    } else {
+      c = 0;
+    }
+  }
+  const bool on = c != 0;
+  int4 n1 = make_int4(0, 0, 0, 0), n2 = n1, nzv = n1;
+  int2 me = make_int2(0, 0);
+  int fl = 0;
+  if (on) {
+    n1 = Tl.nb1[c];
+    n2 = Tl.nb2[c];
+    nzv = Tl.nbz[c];
+    me = Tl.m2e[c];
+    fl = Tl.fl[c];
+  }
+  // x-neighbours that are the cells of neighbouring lanes
+  const int cu1 = __shfl_up_sync(FULL, c, 1), cu2 = __shfl_up_sync(FULL, c, 2);
+  const int cd1 = __shfl_down_sync(FULL, c, 1), cd2 = __shfl_down_sync(FULL, c, 2);
+  const bool sxm1 = on && lane >= 1 && cu1 && n1.x == cu1;
+  const bool sxm2 = on && lane >= 2 && cu2 && n2.x == cu2;
+  const bool sxp1 = on && lane <= 30 && cd1 && n1.y == cd1;
+  const bool sxp2 = on && lane <= 29 && cd2 && n2.y == cd2;
+
+  // tracer-independent face coefficients
+  const double dtu = ss.dtu;
+  const float fdtu = (float)dtu;
+  const bool hdf = any_hd != 0;
+  Face fw, fs, fn, fe, fzb, fzt;
+  face_zero(fw);
+  face_zero(fs);
+  face_zero(fn);
+  face_zero(fe);
+  face_zero(fzb);
+  face_zero(fzt);
+  double idz = 0.0, ia = 0.0;
+  if (on) {
+    const Face2 mx = fx2[c2], my = fy2[c2];
+    hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT, F3.u1[c] * fdtu * mx.ih, F3.u1flux3d[c],
+          hdf ? F3.khx[c] : 0.f, mx);
+    hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT, F3.u2[c] * fdtu * my.ih, F3.u2flux3d[c],
+          hdf ? F3.khy[c] : 0.f, my);
+    if (fl & FL_YP_WET) {
+      const int yp = n1.w;
+      const Face2 mn = fy2[me.y];
+      hface(fn, true, fl & FL_YP_E2, QUICK, ULT, F3.u2[yp] * fdtu * mn.ih, F3.u2flux3d[yp],
+            hdf ? F3.khy[yp] : 0.f, mn);
+    }
+    if (!sxp1 && (fl & FL_XP_WET)) {
+      const int xp = n1.y;
+      const Face2 mxe = fx2[me.x];
+      hface(fe, true, fl & FL_XP_E1, QUICK, ULT, F3.u1[xp] * fdtu * mxe.ih, F3.u1flux3d[xp],
+            hdf ? F3.khx[xp] : 0.f, mxe);
+    }
+    const float dz0 = W.dz32[c];
+    if (k <= ks) {
+      // thicknesses below, at and above the cell (the sediment has none, the
+      // surface-layer cell maps onto itself)
+      const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
+      const bool top = (nzv.z == c);
+      const float dzp1 = W.dz32[nzv.z];
+      zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, F3.w[c] * fdtu);
+      if (k < ks) {  // the bottom face of the cell above
+        const bool top1 = (nzv.w == nzv.z);
+        const float dzp2 = W.dz32[nzv.w];
+        zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, F3.w[nzv.z] * fdtu);
+      }
+    }
+    idz = (double)__fdividef(1.f, dz0);
+    ia = 1.0 / G.cellarea[c2];
+  }
+  // vertical neighbours (bottom: the sediment ghost holds the bottom value,
+  // tracers.c:827-830)
+  const int vm1 = (k - 1 >= kb) ? nzv.x : c;
+  const int vm2 = (k - 2 >= kb) ? nzv.y : vm1;
+  const int vp1 = nzv.z, vp2 = nzv.w;
+  const int ntb = T.ntb;
+
+#pragma unroll 2
+  for (int s = 0; s < ntb; ++s) {
+    const int n = T.slot_tr[s];
+    const int tf = T.trf[n];
+    const bool adv = (tf & TR_ADV) != 0, hd = (tf & TR_HDIFF) != 0;
+    const float *__restrict__ tr = tri + (size_t)n * G.S;
+    const float t0 = on ? tr[c] : 0.f;
+    const float u1v = __shfl_up_sync(FULL, t0, 1), u2v = __shfl_up_sync(FULL, t0, 2);
+    const float d1v = __shfl_down_sync(FULL, t0, 1), d2v = __shfl_down_sync(FULL, t0, 2);
+    float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f, Fzt = 0.f;
+    if (on && (adv || hd)) {
+      const float txm1 = sxm1 ? u1v : tr[n1.x];
+      const float txm2 = sxm2 ? u2v : tr[n2.x];
+      const float txp1 = sxp1 ? d1v : tr[n1.y];
+      const float tym1 = tr[n1.z], tym2 = tr[n2.z], typ1 = tr[n1.w], typ2 = tr[n2.w];
+      Fxw = face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1);
+      Fys = face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1);
+      Fyn = face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2);
+      if (!sxp1) {
+        const float txp2 = sxp2 ? d2v : tr[n2.y];
+        Fxe = face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2);
+      }
+      if (adv && k <= ks) {
+        const float tm1 = tr[vm1], tm2 = tr[vm2], tp1 = tr[vp1];
+        Fzb = face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1);
+        if (k < ks) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tr[vp2]);
+      }
+    }
+    const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
+    if (!on) continue;
+    if (sxp1) Fxe = Fnext;
+    // FP64 flux divergence (tracers.c:888-892)
+    const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+    float val;
+    if (k < ks) {
+      val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
+    } else {
+      val = (float)dtr;
+      if (k == ks) fzs[(size_t)s * G.ncol + col] = Fzb;
+    }
+    tro[(size_t)n * G.S + c] = val;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_vd32
+
+// shared memory of k_vd32 (bytes): LU float4[nz][32], colC int[nz][32],
+// A, S float[nz][nw][32]
+inline size_t vd32_smem(int nz, int nw) {
+  return (size_t)nz * 32 * 16 + (size_t)nz * 32 * 4 + (size_t)2 * nz * nw * 32 * 4;
+}
+
+template <bool LAST>
+__global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSet T,
+                                              SubStep ss, Tile Tl,
+                                              const float4 *__restrict__ lu32,
+                                              const float *__restrict__ dz32,
+                                              const float *__restrict__ tri,
+                                              float *__restrict__ tro,
+                                              const float *__restrict__ fzs, int nw,
+                                              int nchunk) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nz = G.nz;
+  float4 *LU = reinterpret_cast<float4 *>(smem);        // [nz][32]
+  int *colC = reinterpret_cast<int *>(LU + nz * 32);     // [nz][32]
+  float *A = reinterpret_cast<float *>(colC + nz * 32);  // [nz][nw][32]
+  float *Sv = A + nz * nw * 32;                          // [nz][nw][32]
+
+  const int lane = threadIdx.x, wy = threadIdx.y;
+  const int tile = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int col = Tl.vdcol[tile * 32 + lane];
+  const int slot = chunk * nw + wy;
+  const int sa = nw * 32;
+
+  const TileCol tc = tile_column(G, W, Tl, col < 0 ? G.ncol : col, wy == 0 && chunk == 0);
+  const bool act = tc.act;
+  const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
+  const ColInfo ci = tc.ci;
+  const int kmin = __reduce_min_sync(0xffffffffu, act ? kb : nz);
+  for (int k = kmin + wy; k < nz; k += nw) {
+    const int c = (act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
+    colC[k * 32 + lane] = c;
+    if (LAST && c && k <= ks) cp_async16(&LU[k * 32 + lane], &lu32[c]);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+  if (!act || slot >= T.nslot) return;
+
+  const int n = T.slot_tr[slot];
+  const int tf = T.trf[n];
+  const bool tbdy = (tf & TR_TBDY) != 0;
+  const bool adv = tbdy && (tf & TR_ADV);
+  const bool vdf = LAST && (tf & TR_VDIFF);
+  const bool single = (ci.flags & COL_SINGLE) != 0;
+  const bool solve = vdf && !single;
+  const float *tr = tri + (size_t)n * G.S;
+  float *to = tro + (size_t)n * G.S;
+  float *Aj = A + wy * 32 + lane;
+  float *Sj = Sv + wy * 32 + lane;
+  // the column's values: advection results (advected tracers) or the old
+  // values (the rest)
+  {
+    const float *src = tbdy ? to : tr;
+    for (int k = kb; k < nz; ++k) cp_async4(&Aj[k * sa], src + colC[k * 32 + lane]);
+    cp_async_commit();
+  }
+  const double mn = T.mintr[n], mx = T.maxtr[n];
+  {  // sediment ghost (tracers.c:827-830)
+    const int sed = G.zm1[cbot];
+    to[sed] = tbdy ? tr[cbot] : tr[sed];
+  }
+  const double dzs_old = (double)dz32[ci.s];
+  const double ts_old = (double)tr[ci.s];  // surface value before the sub-step
+  const double area = G.cellarea[c2];
+  double Fzb_s = 0.0, wb = 0.0, osub = 0.0, sub = 0.0;
+  if (adv) {
+    Fzb_s = (double)fzs[(size_t)slot * G.ncol + col];
+    wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
+    const double eta = F.eta[c2], oe = F.oldeta[c2];
+    osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
+    sub = oe + ss.subeta_f * (eta - oe);
+  }
+  cp_async_wait<0>();
+
+  long long nwarn = 0;
+  float fwd = 0.f;  // Thomas forward carry
+  if (!tbdy) {
+    for (int k = kb; k < nz; ++k) to[colC[k * 32 + lane]] = Aj[k * sa];
+    if (vdf && single) {
+      const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
+      to[ci.s] = (float)((double)Aj[ks * sa] + F.dt * (0.0 - 0.0) / h);
+    } else if (solve) {
+#pragma unroll 4
+      for (int k = kb; k <= ks; ++k) {
+        const float4 lu = LU[k * 32 + lane];
+        const float a = Aj[k * sa];
+        const float s = (k == kb) ? lu.x * a * lu.z : (lu.x * a - lu.y * fwd) * lu.z;
+        Sj[k * sa] = s;
+        fwd = s;
+      }
+    }
+  } else {
+    double a_below = 0.0;
+    // a < mn and a > mx of a float a, exactly, as float comparisons
+    const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
+    const bool clip = mn <= kClipEps;
+#pragma unroll 4
+    for (int k = kb; k < ks; ++k) {
+      float a = Aj[k * sa];
+      if (k == ks - 1) a_below = (double)a;
+      // tr_bounds clip and range check (:3278-3293)
+      if (clip && a < mn_up) a = mnf;
+      if (a < mn_up || a > mx_dn) ++nwarn;
+      if (solve) {
+        const float4 lu = LU[k * 32 + lane];
+        Aj[k * sa] = a;
+        const float s = (k == kb) ? lu.x * a * lu.z : (lu.x * a - lu.y * fwd) * lu.z;
+        Sj[k * sa] = s;
+        fwd = s;
+      } else {
+        to[colC[k * 32 + lane]] = a;
+      }
+    }
+    // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
+    double vs = ts_old;
+    if (adv) {
+      double ssum = 0.0, scomp = 0.0;
+      f32::neumaier_add(ssum, scomp, __dmul_rn(Fzb_s, area));
+      f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
+      for (int k = ks; k < nz; ++k) f32::neumaier_add(ssum, scomp, -(double)Aj[k * sa]);
+      const double dzs = sub - wb;
+      const double svol = dzs * area;
+      const double st = ssum + scomp;
+      const double sv = (svol == 0.0 || (st < 0.0 && dzs <= O.hmin)) ? 0.0 : st / svol;
+      vs = (G.botz[c2] > 0.0 && dzs_old < O.hmin) ? ts_old : sv;
+    }
+    if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
+    if (mn <= kClipEps && vs < mn) vs = mn;
+    if (vs < mn || vs > mx) ++nwarn;
+    const float vs32 = (float)vs;
+    for (int k = ks; k < nz; ++k) to[colC[k * 32 + lane]] = vs32;
+    if (vdf && single) {
+      const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
+      to[ci.s] = (float)(vs + F.dt * (0.0 - 0.0) / h);
+    } else if (solve) {
+      const float4 lu = LU[ks * 32 + lane];
+      Aj[ks * sa] = vs32;
+      Sj[ks * sa] = (ks == kb) ? lu.x * vs32 * lu.z : (lu.x * vs32 - lu.y * fwd) * lu.z;
+    }
+  }
+  if (solve) {
+    // back substitution (FP32); x(k) replaces s(k).  Then the FP64 residual
+    //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
+    // (the difference form of b - A x for A = dzdt I + the diffusion
+    // operator, cp1(j) = cm1(j+1)) replaces a(j), the correction solve runs
+    // on it in FP32 and the update x + d is added in FP64.
+    float xj1 = 0.f;
+    float udp = 0.f;  // ud of the row above
+#pragma unroll 4
+    for (int k = ks; k >= kb; --k) {
+      const float4 lu = LU[k * 32 + lane];
+      const float x = (k < ks) ? Sj[k * sa] - udp * xj1 : Sj[k * sa];
+      Sj[k * sa] = x;
+      xj1 = x;
+      udp = lu.w;
+    }
+    float xm = 0.f, x0 = Sj[kb * sa];
+    float4 lj = LU[kb * 32 + lane];
+#pragma unroll 4
+    for (int j = kb; j <= ks; ++j) {
+      const float xp = (j < ks) ? Sj[(j + 1) * sa] : 0.f;
+      const float4 lp = (j < ks) ? LU[(j + 1) * 32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+      double r = (double)lj.x * ((double)Aj[j * sa] - (double)x0);
+      if (j > kb) r -= (double)lj.y * ((double)xm - (double)x0);
+      if (j < ks) r -= (double)lp.y * ((double)xp - (double)x0);
+      Aj[j * sa] = (float)r;
+      xm = x0;
+      x0 = xp;
+      lj = lp;
+    }
+    // correction solve (FP32 forward and back) and update in FP64
+    float up = 0.f;
+#pragma unroll 4
+    for (int k = kb; k <= ks; ++k) {
+      const float4 lu = LU[k * 32 + lane];
+      const float r = Aj[k * sa];
+      const float u = (k == kb) ? r * lu.z : (r - lu.y * up) * lu.z;
+      Aj[k * sa] = u;
+      up = u;
+    }
+    float dn = 0.f;
+    udp = 0.f;
+    int stat = 0;
+#pragma unroll 4
+    for (int k = ks; k >= kb; --k) {
+      const int cc = colC[k * 32 + lane];
+      const float4 lu = LU[k * 32 + lane];
+      const float d = (k < ks) ? Aj[k * sa] - udp * dn : Aj[k * sa];
+      const float fin = (float)((double)Sj[k * sa] + (double)d);
+      to[cc] = fin;
+      if (isnan(fin)) stat = ST_NAN;
+      dn = d;
+      udp = lu.w;
+    }
+    if (stat) atomicOr(W.status, stat);
+  }
+  if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
+}
+
+}  // namespace shoc
