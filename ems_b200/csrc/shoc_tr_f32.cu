@@ -22,9 +22,7 @@ void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &
 
 cudaError_t tile32_set_smem_attr() {
   cudaError_t e = cudaSuccess;
-  const cudaError_t r[6] = {attr(k_adv32<true, true>),  attr(k_adv32<true, false>),
-                            attr(k_adv32<false, true>), attr(k_adv32<false, false>),
-                            attr(k_vd32<true>),         attr(k_vd32<false>)};
+  const cudaError_t r[2] = {attr(k_vd32<true>), attr(k_vd32<false>)};
   for (auto x : r)
     if (x != cudaSuccess) e = x;
   return e;

@@ -83,9 +83,13 @@ struct shoc_tr_gpu {
   int tw = 8;
   // profiling
   bool profile = false;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
-  double prof_ms = 0.0;
-  int prof_n = 0;
+  struct ProfEv {
+    int part;  // 0 transport of the last sub-step, 1 advection kernel, 2 column kernel
+    cudaEvent_t a, b;
+  };
+  std::vector<ProfEv> ev;
+  double prof_ms[3] = {0.0, 0.0, 0.0};
+  int prof_n[3] = {0, 0, 0};
   long long launches = 0;
   // pinned readback
   unsigned long long *h_dtm = nullptr;
@@ -355,8 +359,10 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
     ci.cs = nsur;
     ci.cbs = cbs;
     ci.flags = flags;
+    ci.ks = G.kof[s];
+    if (staged_column(ci, bot)) ci.flags |= COL_STAGED;
     W.col[col] = ci;
-    if ((flags & COL_SERIAL) || (list_all && !staged_column(ci, bot))) {
+    if ((flags & COL_SERIAL) || (list_all && !(ci.flags & COL_STAGED))) {
       int i = atomicAdd(W.serial_count, 1);
       W.serial_list[i] = col;
     }
@@ -549,22 +555,32 @@ int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<u
       const int c = cellk[(size_t)k * ncolp + col];
       if (c) colof[c] = col;
     }
-  std::vector<int> wet;
-  wet.reserve(g->a3_t);
+  // k_adv32 cell order: tile by tile (32 adjacent columns), layer by layer
+  // within a tile, so the vertical and y-neighbours a block reads were read
+  // by blocks shortly before it (cache reuse) and a warp's cells are mostly
+  // adjacent cells of one layer
+  std::vector<uint8_t> is_wet(S, 0);
   for (int i = 1; i <= g->a3_t; i++) {
     const int c = g->w3_t[i];
-    if (c > 0 && c < S) wet.push_back(c);
+    if (c > 0 && c < S) is_wet[c] = 1;
   }
-  // k_vd32 column order: deepest first, so a block's lanes span similar
-  // layer ranges
+  std::vector<int> wet;
+  wet.reserve(g->a3_t);
+  for (int t = 0; t < ncolp / 32; t++)
+    for (int k = nz - 1; k >= 0; k--)
+      for (int l = 0; l < 32; l++) {
+        const int col = t * 32 + l;
+        if (col >= ncol) break;
+        const int c = cellk[(size_t)k * ncolp + col];
+        if (c && is_wet[c]) wet.push_back(c);
+      }
+  // k_vd32 column order: the columns' own (spatial) order, so a warp's lanes
+  // at one layer are adjacent cells and its loads and stores coalesce
   std::vector<int> vdcol(ncolp, -1);
-  {
-    std::vector<int> ord(ncol);
-    for (int i = 0; i < ncol; i++) ord[i] = i;
-    std::stable_sort(ord.begin(), ord.end(),
-                     [&](int a, int b) { return col_kb[a] < col_kb[b]; });
-    for (int i = 0; i < ncol; i++) vdcol[i] = ord[i];
-  }
+  for (int i = 0; i < ncol; i++) vdcol[i] = i;
+  std::vector<int4> colrec(ncolp, make_int4(0, 0, nz, 0));
+  for (int col = 0; col < ncol; col++)
+    colrec[col] = make_int4(col_bot[col], g->w2_t[col + 1], col_kb[col], 0);
   Tile &T = h->tl;
   T.ncolp = ncolp;
   T.nwet = (int)wet.size();
@@ -583,10 +599,11 @@ int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<u
   uint8_t *u8;
   if ((rc = dupload(h, &u8, fl.data(), S))) return rc;
   T.fl = u8;
-  if ((rc = dupload(h, &ip, g->s2k, S))) return rc;
-  T.kof = ip;
+  T.kof = h->G.kof;
   if ((rc = dupload(h, &i4, nbz.data(), S))) return rc;
   T.nbz = i4;
+  if ((rc = dupload(h, &i4, colrec.data(), colrec.size()))) return rc;
+  T.colrec = i4;
   if ((rc = dupload(h, &ip, colof.data(), S))) return rc;
   T.colof = ip;
   if ((rc = dupload(h, &ip, wet.data(), wet.size()))) return rc;
@@ -638,12 +655,16 @@ int check_geom(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr) {
     // bottom reaches the top through zp1 and sits on a self-mapping sediment
     int sed = g->zm1[bot];
     if (sed == bot || wet[sed] || g->zm1[sed] != sed || g->zp1[sed] != bot) return SHOC_TR_EGEOM;
+    // and every cell on the way sits one layer above the previous one
     int c = bot, steps = 0;
+    const int kb = g->s2k[bot];
+    if (kb < 0 || kb >= g->nz) return SHOC_TR_EGEOM;
     while (c != top && steps <= g->nz) {
+      if (g->s2k[c] != kb + steps) return SHOC_TR_EGEOM;
       c = g->zp1[c];
       steps++;
     }
-    if (c != top) return SHOC_TR_EGEOM;
+    if (c != top || kb + steps != g->nz - 1) return SHOC_TR_EGEOM;
   }
   for (int i = 1; i <= g->nbpt; i++)
     if (g->bpt[i] < 1 || g->bpt[i] >= S || g->bin[i] < 1 || g->bin[i] >= S) return SHOC_TR_EGEOM;
@@ -679,9 +700,12 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (int i = 0; i < 2; i++)
     if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
-  for (auto &e : h->ev) {
-    cudaEventDestroy(e.first);
-    cudaEventDestroy(e.second);
+  {
+    std::vector<cudaEvent_t> done;  // pairs may share events
+    for (auto &e : h->ev)
+      for (cudaEvent_t x : {e.a, e.b})
+        if (std::find(done.begin(), done.end(), x) == done.end()) done.push_back(x);
+    for (cudaEvent_t x : done) cudaEventDestroy(x);
   }
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_dtm) cudaFreeHost(h->h_dtm);
@@ -696,6 +720,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   int rc = check_geom(g, o, ntr);
   if (rc) return rc;
   if (precision != SHOC_TR_FP64 && precision != SHOC_TR_FP32_MIXED) return SHOC_TR_EUNSUPPORTED;
+  if (precision == SHOC_TR_FP32_MIXED && ntr > kMaxTracers) return SHOC_TR_EUNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || device < 0 || device >= ndev)
     return SHOC_TR_ECUDA;
@@ -774,6 +799,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload(h, &ip, col_top.data(), ncol)); G.col_top = ip;
   TRY(dupload(h, &ip, col_bot.data(), ncol)); G.col_bot = ip;
   TRY(dupload(h, &ip, col_kb.data(), ncol)); G.col_kb = ip;
+  TRY(dupload(h, &ip, g->s2k, S)); G.kof = ip;
   double *dp;
   TRY(dupload(h, &dp, g->h1au1, S2)); G.h1au1 = dp;
   TRY(dupload(h, &dp, g->h2au2, S2)); G.h2au2 = dp;
@@ -1024,9 +1050,10 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
       tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
                      h->F3, h->W, h->O, h->T, ss, h->tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
                      h->any_hdiff ? 1 : 0, prof ? ev : nullptr);
-      if (prof) {
-        h->ev.push_back({ev[0], ev[2]});
-        cudaEventDestroy(ev[1]);
+      if (prof) {  // pairs share events; sync destroys each event once
+        h->ev.push_back({0, ev[0], ev[2]});
+        h->ev.push_back({1, ev[0], ev[1]});
+        h->ev.push_back({2, ev[1], ev[2]});
       }
       h->launches += 2;
       if (last)
@@ -1057,7 +1084,7 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
                                                              tin, tout, tw, nchunk);
       if (prof) {
         cudaEventRecord(e1, st);
-        h->ev.push_back({e0, e1});
+        h->ev.push_back({0, e0, e1});
       }
       h->launches++;
       if (last)
@@ -1299,14 +1326,16 @@ int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag) {
     diag->vc = h->h_counts[1];
   }
   if (h->profile) {
+    std::vector<cudaEvent_t> done;
     for (auto &e : h->ev) {
       float ms = 0.f;
-      cudaEventElapsedTime(&ms, e.first, e.second);
-      h->prof_ms += ms;
-      h->prof_n++;
-      cudaEventDestroy(e.first);
-      cudaEventDestroy(e.second);
+      cudaEventElapsedTime(&ms, e.a, e.b);
+      h->prof_ms[e.part] += ms;
+      h->prof_n[e.part]++;
+      for (cudaEvent_t x : {e.a, e.b})
+        if (std::find(done.begin(), done.end(), x) == done.end()) done.push_back(x);
     }
+    for (cudaEvent_t x : done) cudaEventDestroy(x);
     h->ev.clear();
   }
   return rc;
@@ -1473,18 +1502,24 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
 int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable) {
   if (!h) return SHOC_TR_EARG;
   h->profile = enable != 0;
-  h->prof_ms = 0.0;
-  h->prof_n = 0;
+  for (int i = 0; i < 3; i++) {
+    h->prof_ms[i] = 0.0;
+    h->prof_n[i] = 0;
+  }
+  return 0;
+}
+
+int shoc_tr_gpu_kernel_time_part(shoc_tr_gpu *h, int part, double *ms, int *n) {
+  if (!h || part < 0 || part > 2) return SHOC_TR_EARG;
+  if (ms) *ms = h->prof_n[part] ? h->prof_ms[part] / h->prof_n[part] : 0.0;
+  if (n) *n = h->prof_n[part];
+  h->prof_ms[part] = 0.0;
+  h->prof_n[part] = 0;
   return 0;
 }
 
 int shoc_tr_gpu_kernel_time(shoc_tr_gpu *h, double *ms, int *n) {
-  if (!h) return SHOC_TR_EARG;
-  if (ms) *ms = h->prof_n ? h->prof_ms / h->prof_n : 0.0;
-  if (n) *n = h->prof_n;
-  h->prof_ms = 0.0;
-  h->prof_n = 0;
-  return 0;
+  return shoc_tr_gpu_kernel_time_part(h, 0, ms, n);
 }
 
 long long shoc_tr_gpu_launch_count(shoc_tr_gpu *h) { return h ? h->launches : 0; }

@@ -42,6 +42,7 @@ constexpr int COL_SINGLE = 2;   // one-layer column in vert_diffuse_3d
 constexpr int COL_SERIAL = 4;   // tr_bounds thin fix can couple tracers: serial path
 constexpr int COL_THIN = 8;     // tr_bounds thin-surface test is on
 constexpr int COL_NOSOLVE = 16; // degenerate implicit-solve range: status raised, no solve
+constexpr int COL_STAGED = 32;  // handled by the FP32-mixed column-tile kernels
 
 // 2D face metrics of one direction, precomputed per surface-layer cell:
 // d = d3/d4 weight, db/df = 2/(h_m+h_0), 2/(h_0+h_p), h_m/h_0/h_p = metric
@@ -56,6 +57,7 @@ struct ColInfo {
   int cs;      // new surface cell: top of the implicit solve (wincon->i2)
   int cbs;     // bottom of the implicit solve (cbt)
   int flags;
+  int ks;      // layer of s
 };
 
 struct Geo {
@@ -64,6 +66,7 @@ struct Geo {
   const uint8_t *cflag;
   const int *col_top, *col_bot;  // surface-layer and bottom cell per column
   const int *col_kb;             // layer index of the bottom cell per column
+  const int *kof;                // layer index of every cell (s2k)
   const double *h1au1, *h2au2, *h1au2, *h2au1, *h1acell, *h2acell, *cellarea, *botz;
   const double *gridz;
   const Face2D *fx, *fy;         // [S2]
@@ -303,7 +306,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
                                             TR *__restrict__ tro, int col, int n, int kstart,
                                             bool act, Sol &sol, bool &c3_moved,
                                             unsigned long long &warn, int &stat) {
-  ColInfo ci = {0, 0, 0, 0, 0};
+  ColInfo ci = {0, 0, 0, 0, 0, 0};
   int cbot = 0, ctop = 0, kb = G.nz;
   if (act) {
     ci = W.col[col];

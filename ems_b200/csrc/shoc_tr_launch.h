@@ -8,7 +8,7 @@
 
 namespace shoc {
 
-// allow every k_adv32 / k_vd32 instance the opt-in shared memory size
+// allow every k_vd32 instance the opt-in shared memory size
 cudaError_t tile32_set_smem_attr();
 
 // one FP32-mixed transport sub-step over the staged columns: k_adv32 then

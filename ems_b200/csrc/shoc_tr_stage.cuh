@@ -27,18 +27,19 @@ __device__ __forceinline__ bool staged_column(const ColInfo &ci, int cbot) {
 namespace f32 {
 
 // QUICKEST (quickest(), tracers.c:1870-1884) is, for a given sign of the
-// Courant number, linear in the four stencil values:
-//   F = w0 tm2 + w1 tm1 + w2 t0 + w3 tp1
+// Courant number, linear in the upwind-side value tu (tm2 for cr > 0, tp1 for
+// cr < 0) and the two values beside the face:
+//   F = wa tu + w1 tm1 + w2 t0
 // with the tracer-independent weights folded once per cell from
 // a = d - cr/2, b = (1 - cr^2)/6 and the upwind curvature factors A, B:
-//   cr > 0: w0 = -b B, w1 = 1 - a + 2b, w2 = a - b A, w3 = 0
-//   cr < 0: w0 = 0,    w1 = 1 - a - b B, w2 = a + 2b, w3 = -b A
-//   cr = 0: w1 = 1 - d, w2 = d
-// Van Leer keeps w0 = (1 -+ cr)/2 and its flux-limiter form.  Then ULTIMATE
+//   cr > 0: wa = -b B, w1 = 1 - a + 2b, w2 = a - b A
+//   cr < 0: wa = -b A, w1 = 1 - a - b B, w2 = a + 2b
+//   cr = 0: wa = 0,    w1 = 1 - d,      w2 = d
+// Van Leer keeps wa = (1 -+ cr)/2 and its flux-limiter form.  Then ULTIMATE
 // (ircr = 1/|cr|), times the volume flux U, minus K (t0 - tm1) for horizontal
 // diffusion.  A face that carries nothing has all weights, U and K zero.
 struct Face {
-  float w0, w1, w2, w3, ircr, U, K;
+  float wa, w1, w2, ircr, U, K;
   int bits;
 };
 constexpr int FB_POS = 1, FB_NEG = 2, FB_ULT = 4;
@@ -50,7 +51,7 @@ struct Face2 {
 };
 
 __device__ __forceinline__ void face_zero(Face &f) {
-  f.w0 = f.w1 = f.w2 = f.w3 = 0.f;
+  f.wa = f.w1 = f.w2 = 0.f;
   f.ircr = f.U = f.K = 0.f;
   f.bits = 0;
 }
@@ -63,24 +64,21 @@ __device__ __forceinline__ void set_face(Face &f, bool quick, float cr, float d,
   if (quick) {
     const float a = d - 0.5f * cr, b = (1.f - cr * cr) * (1.f / 6.f);
     if (cr > 0.f) {
-      f.w0 = -b * Bp;
+      f.wa = -b * Bp;
       f.w1 = 1.f - a + 2.f * b;
       f.w2 = a - b * Ap;
-      f.w3 = 0.f;
     } else if (cr < 0.f) {
-      f.w0 = 0.f;
+      f.wa = -b * Am;
       f.w1 = 1.f - a - b * Bm;
       f.w2 = a + 2.f * b;
-      f.w3 = -b * Am;
     } else {
-      f.w0 = 0.f;
+      f.wa = 0.f;
       f.w1 = 1.f - d;
       f.w2 = d;
-      f.w3 = 0.f;
     }
   } else {
-    f.w0 = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
-    f.w1 = f.w2 = f.w3 = 0.f;
+    f.wa = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
+    f.w1 = f.w2 = 0.f;
   }
   f.ircr = cr != 0.f ? __fdividef(1.f, fabsf(cr)) : 0.f;
   f.U = U;
@@ -94,15 +92,16 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
   float F = 0.f;
   if (adv) {
     const bool pos = (f.bits & FB_POS) != 0;
+    const float tu = pos ? tm2 : tp1;
     if (QUICK) {
-      F = f.w0 * tm2 + f.w1 * tm1 + f.w2 * t0 + f.w3 * tp1;
+      F = f.wa * tu + f.w1 * tm1 + f.w2 * t0;
     } else {
       const bool neg = (f.bits & FB_NEG) != 0;
       const float p = pos ? (tm1 - tm2) : (t0 - tm1), q = pos ? (t0 - tm1) : (tp1 - t0);
       const float den = pos ? (t0 - tm2) : (tp1 - tm1);
       const float pq = p * q;
       const float df = pq > 0.f ? 2.f * __fdividef(pq, den) : 0.f;
-      F = pos ? tm1 + f.w0 * df : (neg ? t0 - f.w0 * df : 0.f);
+      F = pos ? tm1 + f.wa * df : (neg ? t0 - f.wa * df : 0.f);
     }
     if (ULT && (f.bits & FB_ULT)) {
       // ulimate_filter (tracers.c:3526-3554) without its divisions: with
@@ -113,7 +112,7 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       // tc equals them too: in FP64 they almost always differ by a few ulps
       // and the limiter falls back to upwind, so FP32 rounding of the stored
       // tracer does not flip the limiter's decision.
-      const float tc = pos ? tm1 : t0, tu = pos ? tm2 : tp1, td = pos ? t0 : tm1;
+      const float tc = pos ? tm1 : t0, td = pos ? t0 : tm1;
       const float diff = td - tu;
       const float sg = diff < 0.f ? -1.f : 1.f;
       const float d = fabsf(diff), c = (tc - tu) * sg, a = (F - tu) * sg;

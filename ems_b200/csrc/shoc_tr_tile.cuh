@@ -47,6 +47,7 @@ struct Tile {
   const int *colof;  // [S] 0-based column of each wet cell
   const int *wet;    // [nwet] the wet cells (w3_t order)
   const int *vdcol;  // [ncolp] columns in k_vd32 order (-1: padding)
+  const int4 *colrec;  // [ncolp] bottom cell, surface-layer cell, bottom layer
   int ncolp;         // columns rounded up to whole tiles
   int nwet;
 };
@@ -69,34 +70,31 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// The column of lane `col` of a tile: whether the tile kernels handle it, its
-// bottom and surface layers, 2D cell and bottom cell.
+// The column `col` of a tile kernel: whether the tile kernels handle it this
+// step (k_set_dz decides, COL_STAGED), its bottom and surface layers, 2D cell
+// and bottom cell.  (The layer-by-column cell table agrees with the maps:
+// handle creation checks every column's layers.)
 struct TileCol {
   ColInfo ci;
   int cbot, c2, kb, ks;
   bool act;
 };
 __device__ __forceinline__ TileCol tile_column(const Geo &G, const Work &W, const Tile &Tl,
-                                               int col, bool report) {
+                                               int col) {
   TileCol t;
-  t.ci = {0, 0, 0, 0, 0};
+  t.ci = {0, 0, 0, 0, 0, 0};
   t.cbot = t.c2 = t.ks = 0;
   t.kb = G.nz;
-  t.act = col < G.ncol;
-  if (t.act) {
+  t.act = false;
+  if (col >= 0 && col < G.ncol) {
     t.ci = W.col[col];
-    t.cbot = G.col_bot[col];
-    t.c2 = G.col_top[col];
-    t.act = staged_column(t.ci, t.cbot);
-  }
-  if (t.act) {
-    t.kb = G.col_kb[col];
-    t.ks = Tl.kof[t.ci.s];
-    // the surface cell must be this column's cell at its layer
-    if (t.ks < t.kb || t.ks >= G.nz || Tl.cellk[(size_t)t.ks * Tl.ncolp + col] != t.ci.s) {
-      t.act = false;
-      t.kb = G.nz;
-      if (report) atomicOr(W.status, ST_GEOM);
+    const int4 r = Tl.colrec[col];
+    if (t.ci.flags & COL_STAGED) {
+      t.act = true;
+      t.cbot = r.x;
+      t.c2 = r.y;
+      t.kb = r.z;
+      t.ks = t.ci.ks;
     }
   }
   return t;
@@ -139,9 +137,11 @@ __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2,
 // k_adv32
 
 constexpr int kAdvBlock = 256;
+constexpr int kAdvGroup = 2;       // tracers whose loads a thread issues together
+constexpr int kMaxTracers = 256;   // tracers a handle of the FP32-mixed path may carry
 
 template <bool QUICK, bool ULT>
-__global__ void __launch_bounds__(kAdvBlock) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
+__global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
                                                      SubStep ss, Tile Tl,
                                                      const f32::Face2 *__restrict__ fx2,
                                                      const f32::Face2 *__restrict__ fy2,
@@ -150,24 +150,28 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv32(Geo G, Flow32 F3, Work W, T
                                                      float *__restrict__ fzs, int any_hd) {
   using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
+  __shared__ int sTr[kMaxTracers], sTf[kMaxTracers];
   const int i = blockIdx.x * kAdvBlock + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int nz = G.nz;
+  for (int s = threadIdx.x; s < T.ntb; s += kAdvBlock) {
+    const int n = T.slot_tr[s];
+    sTr[s] = n;
+    sTf[s] = T.trf[n];
+  }
+  __syncthreads();
 
   // this thread's cell and its column
   int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0;
   if (i < Tl.nwet) {
     c = Tl.wet[i];
     col = Tl.colof[c];
-    const ColInfo ci = W.col[col];
-    const int cbot = G.col_bot[col];
-    if (staged_column(ci, cbot)) {
-      kb = G.col_kb[col];
-      ks = Tl.kof[ci.s];
-      k = Tl.kof[c];
-      c2 = G.col_top[col];
-      // the column's surface cell must be at its layer (k_vd32 reports it)
-      if (ks < kb || ks >= nz || k < kb || Tl.cellk[(size_t)ks * Tl.ncolp + col] != ci.s) c = 0;
+    k = Tl.kof[c];
+    const TileCol tc = tile_column(G, W, Tl, col);
+    if (tc.act) {
+      kb = tc.kb;
+      ks = tc.ks;
+      c2 = tc.c2;
     } else {
       c = 0;
     }
@@ -243,49 +247,79 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv32(Geo G, Flow32 F3, Work W, T
   const int vm1 = (k - 1 >= kb) ? nzv.x : c;
   const int vm2 = (k - 2 >= kb) ? nzv.y : vm1;
   const int vp1 = nzv.z, vp2 = nzv.w;
+  const bool zf = k <= ks, zt = k < ks;
   const int ntb = T.ntb;
 
-#pragma unroll 2
-  for (int s = 0; s < ntb; ++s) {
-    const int n = T.slot_tr[s];
-    const int tf = T.trf[n];
-    const bool adv = (tf & TR_ADV) != 0, hd = (tf & TR_HDIFF) != 0;
-    const float *__restrict__ tr = tri + (size_t)n * G.S;
-    const float t0 = on ? tr[c] : 0.f;
-    const float u1v = __shfl_up_sync(FULL, t0, 1), u2v = __shfl_up_sync(FULL, t0, 2);
-    const float d1v = __shfl_down_sync(FULL, t0, 1), d2v = __shfl_down_sync(FULL, t0, 2);
-    float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f, Fzt = 0.f;
-    if (on && (adv || hd)) {
-      const float txm1 = sxm1 ? u1v : tr[n1.x];
-      const float txm2 = sxm2 ? u2v : tr[n2.x];
-      const float txp1 = sxp1 ? d1v : tr[n1.y];
-      const float tym1 = tr[n1.z], tym2 = tr[n2.z], typ1 = tr[n1.w], typ2 = tr[n2.w];
-      Fxw = face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1);
-      Fys = face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1);
-      Fyn = face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2);
-      if (!sxp1) {
-        const float txp2 = sxp2 ? d2v : tr[n2.y];
-        Fxe = face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2);
-      }
-      if (adv && k <= ks) {
-        const float tm1 = tr[vm1], tm2 = tr[vm2], tp1 = tr[vp1];
-        Fzb = face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1);
-        if (k < ks) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tr[vp2]);
-      }
+  // The advected tracers in groups of U: every stencil value of the group is
+  // loaded before any of it is used, so a thread has U tracers' loads in
+  // flight at once.
+  constexpr int U = kAdvGroup;
+  for (int s0 = 0; s0 < ntb; s0 += U) {
+    float v[U][13];  // t0, y-2..y+2, z-2..z+2, x-2..x+2 (off-tile x only)
+    int nn[U], tf[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int s = s0 + u;
+      nn[u] = s < ntb ? sTr[s] : 0;
+      tf[u] = s < ntb ? sTf[s] : 0;
+      const float *__restrict__ tr = tri + (size_t)nn[u] * G.S;
+      const bool hor = on && (tf[u] & (TR_ADV | TR_HDIFF));
+      const bool vz = on && (tf[u] & TR_ADV) && zf;
+      v[u][0] = on && s < ntb ? tr[c] : 0.f;
+      v[u][1] = hor ? tr[n1.z] : 0.f;
+      v[u][2] = hor ? tr[n2.z] : 0.f;
+      v[u][3] = hor ? tr[n1.w] : 0.f;
+      v[u][4] = hor ? tr[n2.w] : 0.f;
+      v[u][5] = vz ? tr[vm1] : 0.f;
+      v[u][6] = vz ? tr[vm2] : 0.f;
+      v[u][7] = vz ? tr[vp1] : 0.f;
+      v[u][8] = (vz && zt) ? tr[vp2] : 0.f;
+      v[u][9] = (hor && !sxm1) ? tr[n1.x] : 0.f;
+      v[u][10] = (hor && !sxm2) ? tr[n2.x] : 0.f;
+      v[u][11] = (hor && !sxp1) ? tr[n1.y] : 0.f;
+      v[u][12] = (hor && !sxp1 && !sxp2) ? tr[n2.y] : 0.f;
     }
-    const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
-    if (!on) continue;
-    if (sxp1) Fxe = Fnext;
-    // FP64 flux divergence (tracers.c:888-892)
-    const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
-    float val;
-    if (k < ks) {
-      val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
-    } else {
-      val = (float)dtr;
-      if (k == ks) fzs[(size_t)s * G.ncol + col] = Fzb;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int s = s0 + u;
+      if (s >= ntb) break;
+      const bool adv = (tf[u] & TR_ADV) != 0, hd = (tf[u] & TR_HDIFF) != 0;
+      const float t0 = v[u][0];
+      const float u1v = __shfl_up_sync(FULL, t0, 1), u2v = __shfl_up_sync(FULL, t0, 2);
+      const float d1v = __shfl_down_sync(FULL, t0, 1), d2v = __shfl_down_sync(FULL, t0, 2);
+      float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f, Fzt = 0.f;
+      if (on && (adv || hd)) {
+        const float txm1 = sxm1 ? u1v : v[u][9];
+        const float txm2 = sxm2 ? u2v : v[u][10];
+        const float txp1 = sxp1 ? d1v : v[u][11];
+        const float tym1 = v[u][1], tym2 = v[u][2], typ1 = v[u][3], typ2 = v[u][4];
+        Fxw = face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1);
+        Fys = face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1);
+        Fyn = face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2);
+        if (!sxp1) {
+          const float txp2 = sxp2 ? d2v : v[u][12];
+          Fxe = face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2);
+        }
+        if (adv && zf) {
+          const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7];
+          Fzb = face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1);
+          if (zt) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, v[u][8]);
+        }
+      }
+      const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
+      if (!on) continue;
+      if (sxp1) Fxe = Fnext;
+      // FP64 flux divergence (tracers.c:888-892)
+      const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+      float val;
+      if (zt) {
+        val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
+      } else {
+        val = (float)dtr;
+        if (k == ks) fzs[(size_t)nn[u] * G.ncol + col] = Fzb;
+      }
+      tro[(size_t)nn[u] * G.S + c] = val;
     }
-    tro[(size_t)n * G.S + c] = val;
   }
 }
 
@@ -320,7 +354,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   const int slot = chunk * nw + wy;
   const int sa = nw * 32;
 
-  const TileCol tc = tile_column(G, W, Tl, col < 0 ? G.ncol : col, wy == 0 && chunk == 0);
+  const TileCol tc = tile_column(G, W, Tl, col);
   const bool act = tc.act;
   const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
   const ColInfo ci = tc.ci;
@@ -363,7 +397,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   const double area = G.cellarea[c2];
   double Fzb_s = 0.0, wb = 0.0, osub = 0.0, sub = 0.0;
   if (adv) {
-    Fzb_s = (double)fzs[(size_t)slot * G.ncol + col];
+    Fzb_s = (double)fzs[(size_t)n * G.ncol + col];
     wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
     const double eta = F.eta[c2], oe = F.oldeta[c2];
     osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
@@ -371,43 +405,49 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   }
   cp_async_wait<0>();
 
+  // the column in shared memory, from its bottom layer up: value (A),
+  // Thomas storage (S), LU factors {dzdt, cm1, 1/div, ud} (L), cell (C)
+  float *const A0 = Aj + kb * sa;
+  float *const S0 = Sj + kb * sa;
+  const float4 *const L0 = LU + kb * 32 + lane;
+  const int *const C0 = colC + kb * 32 + lane;
+  const int nk = ks - kb;  // cells below the surface cell
   long long nwarn = 0;
-  float fwd = 0.f;  // Thomas forward carry
+  float fwd = 0.f;  // Thomas forward carry (the bottom row's cm1 is 0)
   if (!tbdy) {
-    for (int k = kb; k < nz; ++k) to[colC[k * 32 + lane]] = Aj[k * sa];
+    for (int j = 0; j < nz - kb; ++j) to[C0[j * 32]] = A0[j * sa];
     if (vdf && single) {
       const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-      to[ci.s] = (float)((double)Aj[ks * sa] + F.dt * (0.0 - 0.0) / h);
+      to[ci.s] = (float)((double)A0[nk * sa] + F.dt * (0.0 - 0.0) / h);
     } else if (solve) {
-#pragma unroll 4
-      for (int k = kb; k <= ks; ++k) {
-        const float4 lu = LU[k * 32 + lane];
-        const float a = Aj[k * sa];
-        const float s = (k == kb) ? lu.x * a * lu.z : (lu.x * a - lu.y * fwd) * lu.z;
-        Sj[k * sa] = s;
-        fwd = s;
+      for (int j = 0; j <= nk; ++j) {
+        const float4 lu = L0[j * 32];
+        fwd = (lu.x * A0[j * sa] - lu.y * fwd) * lu.z;
+        S0[j * sa] = fwd;
       }
     }
   } else {
-    double a_below = 0.0;
-    // a < mn and a > mx of a float a, exactly, as float comparisons
+    // tr_bounds clip and range check (:3278-3293) of the cells below the
+    // surface; a < mn and a > mx of a float a, exactly, as float compares
+    const double a_below = nk > 0 ? (double)A0[(nk - 1) * sa] : 0.0;
     const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
     const bool clip = mn <= kClipEps;
-#pragma unroll 4
-    for (int k = kb; k < ks; ++k) {
-      float a = Aj[k * sa];
-      if (k == ks - 1) a_below = (double)a;
-      // tr_bounds clip and range check (:3278-3293)
-      if (clip && a < mn_up) a = mnf;
-      if (a < mn_up || a > mx_dn) ++nwarn;
-      if (solve) {
-        const float4 lu = LU[k * 32 + lane];
-        Aj[k * sa] = a;
-        const float s = (k == kb) ? lu.x * a * lu.z : (lu.x * a - lu.y * fwd) * lu.z;
-        Sj[k * sa] = s;
-        fwd = s;
-      } else {
-        to[colC[k * 32 + lane]] = a;
+    if (solve) {
+      for (int j = 0; j < nk; ++j) {
+        float a = A0[j * sa];
+        if (clip && a < mn_up) a = mnf;
+        nwarn += (a < mn_up || a > mx_dn);
+        A0[j * sa] = a;
+        const float4 lu = L0[j * 32];
+        fwd = (lu.x * a - lu.y * fwd) * lu.z;
+        S0[j * sa] = fwd;
+      }
+    } else {
+      for (int j = 0; j < nk; ++j) {
+        float a = A0[j * sa];
+        if (clip && a < mn_up) a = mnf;
+        nwarn += (a < mn_up || a > mx_dn);
+        to[C0[j * 32]] = a;
       }
     }
     // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
@@ -416,7 +456,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
       double ssum = 0.0, scomp = 0.0;
       f32::neumaier_add(ssum, scomp, __dmul_rn(Fzb_s, area));
       f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
-      for (int k = ks; k < nz; ++k) f32::neumaier_add(ssum, scomp, -(double)Aj[k * sa]);
+      for (int j = nk; j < nz - kb; ++j) f32::neumaier_add(ssum, scomp, -(double)A0[j * sa]);
       const double dzs = sub - wb;
       const double svol = dzs * area;
       const double st = ssum + scomp;
@@ -427,14 +467,14 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
     if (mn <= kClipEps && vs < mn) vs = mn;
     if (vs < mn || vs > mx) ++nwarn;
     const float vs32 = (float)vs;
-    for (int k = ks; k < nz; ++k) to[colC[k * 32 + lane]] = vs32;
+    for (int j = nk; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
     if (vdf && single) {
       const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
       to[ci.s] = (float)(vs + F.dt * (0.0 - 0.0) / h);
     } else if (solve) {
-      const float4 lu = LU[ks * 32 + lane];
-      Aj[ks * sa] = vs32;
-      Sj[ks * sa] = (ks == kb) ? lu.x * vs32 * lu.z : (lu.x * vs32 - lu.y * fwd) * lu.z;
+      const float4 lu = L0[nk * 32];
+      A0[nk * sa] = vs32;
+      S0[nk * sa] = (lu.x * vs32 - lu.y * fwd) * lu.z;
     }
   }
   if (solve) {
@@ -443,55 +483,47 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
     // (the difference form of b - A x for A = dzdt I + the diffusion
     // operator, cp1(j) = cm1(j+1)) replaces a(j), the correction solve runs
     // on it in FP32 and the update x + d is added in FP64.
-    float xj1 = 0.f;
-    float udp = 0.f;  // ud of the row above
-#pragma unroll 4
-    for (int k = ks; k >= kb; --k) {
-      const float4 lu = LU[k * 32 + lane];
-      const float x = (k < ks) ? Sj[k * sa] - udp * xj1 : Sj[k * sa];
-      Sj[k * sa] = x;
-      xj1 = x;
-      udp = lu.w;
+    float x = S0[nk * sa];
+    for (int j = nk - 1; j >= 0; --j) {
+      x = S0[j * sa] - L0[(j + 1) * 32].w * x;
+      S0[j * sa] = x;
     }
-    float xm = 0.f, x0 = Sj[kb * sa];
-    float4 lj = LU[kb * 32 + lane];
-#pragma unroll 4
-    for (int j = kb; j <= ks; ++j) {
-      const float xp = (j < ks) ? Sj[(j + 1) * sa] : 0.f;
-      const float4 lp = (j < ks) ? LU[(j + 1) * 32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-      double r = (double)lj.x * ((double)Aj[j * sa] - (double)x0);
-      if (j > kb) r -= (double)lj.y * ((double)xm - (double)x0);
-      if (j < ks) r -= (double)lp.y * ((double)xp - (double)x0);
-      Aj[j * sa] = (float)r;
+    float xm = S0[0], x0 = xm;  // the bottom row has no cm1 term
+    float4 lj = L0[0];
+    for (int j = 0; j < nk; ++j) {
+      const float xp = S0[(j + 1) * sa];
+      const float4 lp = L0[(j + 1) * 32];
+      const double r = (double)lj.x * ((double)A0[j * sa] - (double)x0) -
+                       (double)lj.y * ((double)xm - (double)x0) -
+                       (double)lp.y * ((double)xp - (double)x0);
+      A0[j * sa] = (float)r;
       xm = x0;
       x0 = xp;
       lj = lp;
     }
+    A0[nk * sa] = (float)((double)lj.x * ((double)A0[nk * sa] - (double)x0) -
+                          (double)lj.y * ((double)xm - (double)x0));
     // correction solve (FP32 forward and back) and update in FP64
-    float up = 0.f;
-#pragma unroll 4
-    for (int k = kb; k <= ks; ++k) {
-      const float4 lu = LU[k * 32 + lane];
-      const float r = Aj[k * sa];
-      const float u = (k == kb) ? r * lu.z : (r - lu.y * up) * lu.z;
-      Aj[k * sa] = u;
-      up = u;
+    float u = 0.f;
+    for (int j = 0; j <= nk; ++j) {
+      const float4 lu = L0[j * 32];
+      u = (A0[j * sa] - lu.y * u) * lu.z;
+      A0[j * sa] = u;
     }
-    float dn = 0.f;
-    udp = 0.f;
-    int stat = 0;
-#pragma unroll 4
-    for (int k = ks; k >= kb; --k) {
-      const int cc = colC[k * 32 + lane];
-      const float4 lu = LU[k * 32 + lane];
-      const float d = (k < ks) ? Aj[k * sa] - udp * dn : Aj[k * sa];
-      const float fin = (float)((double)Sj[k * sa] + (double)d);
-      to[cc] = fin;
-      if (isnan(fin)) stat = ST_NAN;
-      dn = d;
-      udp = lu.w;
+    float d = A0[nk * sa];
+    bool bad = false;
+    {
+      const float fin = (float)((double)S0[nk * sa] + (double)d);
+      to[C0[nk * 32]] = fin;
+      bad |= isnan(fin);
     }
-    if (stat) atomicOr(W.status, stat);
+    for (int j = nk - 1; j >= 0; --j) {
+      d = A0[j * sa] - L0[(j + 1) * 32].w * d;
+      const float fin = (float)((double)S0[j * sa] + (double)d);
+      to[C0[j * 32]] = fin;
+      bad |= isnan(fin);
+    }
+    if (bad) atomicOr(W.status, ST_NAN);
   }
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
 }

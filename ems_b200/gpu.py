@@ -24,7 +24,8 @@ EXPORTS = (
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
     "shoc_tr_gpu_mass_noalloc",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_profile",
-    "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_launch_count", "shoc_tr_gpu_strerror",
+    "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
+    "shoc_tr_gpu_strerror",
 )
 
 _lib = None
@@ -59,6 +60,8 @@ def lib(path=None):
     L.shoc_tr_gpu_set_tiling.argtypes = [H, C.c_int, C.c_int]
     L.shoc_tr_gpu_profile.argtypes = [H, C.c_int]
     L.shoc_tr_gpu_kernel_time.argtypes = [H, C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.shoc_tr_gpu_kernel_time_part.argtypes = [H, C.c_int, C.POINTER(C.c_double),
+                                               C.POINTER(C.c_int)]
     L.shoc_tr_gpu_launch_count.argtypes = [H]
     L.shoc_tr_gpu_launch_count.restype = C.c_longlong
     L.shoc_tr_gpu_strerror.argtypes = [C.c_int]
@@ -184,10 +187,13 @@ class TracerStep:
     def profile(self, on=True):
         _check("profile", self.L.shoc_tr_gpu_profile(self.h, 1 if on else 0))
 
-    def kernel_time(self):
+    def kernel_time(self, part=0):
+        """(ms per step, steps) of the last sub-step's transport (part 0), the
+        advection kernel (1) or the column kernel (2) since the last call."""
         ms = C.c_double()
         n = C.c_int()
-        _check("kernel_time", self.L.shoc_tr_gpu_kernel_time(self.h, C.byref(ms), C.byref(n)))
+        _check("kernel_time", self.L.shoc_tr_gpu_kernel_time_part(self.h, part, C.byref(ms),
+                                                                   C.byref(n)))
         return ms.value, n.value
 
     def launches(self):

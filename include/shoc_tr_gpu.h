@@ -104,11 +104,18 @@ void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
  * 0 keeps the current value.  Takes effect at the next step. */
 int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block);
 
-/* Time of the transport kernel per launch, averaged over the launches since
- * the last call (CUDA events on the handle's stream; enabled by
- * shoc_tr_gpu_profile(h, 1)). */
+/* Time of the transport of a step's last sub-step (the transport kernels
+ * of the precision: one launch for SHOC_TR_FP64, the advection and the column
+ * kernel for SHOC_TR_FP32_MIXED), averaged over the steps since the last call
+ * (CUDA events on the handle's stream; enabled by shoc_tr_gpu_profile(h, 1)).
+ * No reference counterpart: measurement hooks of this library. */
 int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable);
 int shoc_tr_gpu_kernel_time(shoc_tr_gpu *h, double *ms_per_launch, int *launches);
+/* The same for one part: 0 the whole transport (as above), 1 the advection
+ * kernel, 2 the column kernel (tr_bounds, surf_conc, vertical diffusion) of
+ * SHOC_TR_FP32_MIXED. */
+int shoc_tr_gpu_kernel_time_part(shoc_tr_gpu *h, int part, double *ms_per_launch,
+                                 int *launches);
 
 /* Counts of kernels this library launched since creation. */
 long long shoc_tr_gpu_launch_count(shoc_tr_gpu *h);
