@@ -12,11 +12,23 @@ cudaError_t attr(K k) {
   return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 }
 
-template <bool Q, bool U>
+template <bool Q, bool U, int M>
 void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
          const float *tin, float *tout, float *fzs, int hd) {
-  k_adv32<Q, U><<<grid, kAdvBlock, 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+  k_adv32<Q, U, M><<<grid, kAdvBlock, 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+}
+template <bool Q, bool U>
+void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F3,
+              const Work &W, const TrSet &T, const SubStep &ss, const Tile &Tl,
+              const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin, float *tout,
+              float *fzs, int hd) {
+  if (mode == 1)
+    adv<Q, U, 1>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+  else if (mode == 2)
+    adv<Q, U, 2>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+  else
+    adv<Q, U, 0>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
 }
 }  // namespace
 
@@ -32,19 +44,23 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *fzs, int vd_nw,
-                    int any_hd, cudaEvent_t *ev) {
+                    int any_hd, int adv_flags, cudaEvent_t *ev) {
   const int ntile = Tl.ncolp / 32;
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {
     const int grid = (Tl.nwet + kAdvBlock - 1) / kAdvBlock;
     if (quick && ult)
-      adv<true, true>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+      adv_mode<true, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
+                           any_hd);
     else if (quick)
-      adv<true, false>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+      adv_mode<true, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
+                            any_hd);
     else if (ult)
-      adv<false, true>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+      adv_mode<false, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
+                            any_hd);
     else
-      adv<false, false>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, any_hd);
+      adv_mode<false, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
+                             any_hd);
   }
   if (ev) cudaEventRecord(ev[1], st);
   const int nchunk = (T.nslot + vd_nw - 1) / vd_nw;

@@ -67,6 +67,7 @@ struct shoc_tr_gpu {
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
   Tile tl{};                          // static tables of the column-tile kernels
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
+  int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
   bool staged = false;                // column-tile fast path
   int cur = 0;
   int *bpt = nullptr, *bin = nullptr;
@@ -845,6 +846,16 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   }
   for (int n = 0; n < ntr; n++)
     if (!(h->trf[n] & TR_TBDY)) slot.push_back(n);
+  {
+    bool all_a = true, all_h = true, no_h = true;
+    for (int i = 0; i < o->ntbdy; i++) {
+      const uint8_t f = h->trf[o->tbdy[i]];
+      all_a = all_a && (f & TR_ADV);
+      all_h = all_h && (f & TR_HDIFF);
+      no_h = no_h && !(f & TR_HDIFF);
+    }
+    h->adv_flags = !all_a ? 0 : (no_h ? 1 : (all_h ? 2 : 0));
+  }
   h->nslot = (int)slot.size();
   TrSet &T = h->T;
   T.ntr = ntr;
@@ -1049,7 +1060,7 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
         for (auto &e : ev) cudaEventCreate(&e);
       tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
                      h->F3, h->W, h->O, h->T, ss, h->tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
-                     h->any_hdiff ? 1 : 0, prof ? ev : nullptr);
+                     h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
       if (prof) {  // pairs share events; sync destroys each event once
         h->ev.push_back({0, ev[0], ev[2]});
         h->ev.push_back({1, ev[0], ev[1]});

@@ -140,7 +140,9 @@ constexpr int kAdvBlock = 256;
 constexpr int kAdvGroup = 2;       // tracers whose loads a thread issues together
 constexpr int kMaxTracers = 256;   // tracers a handle of the FP32-mixed path may carry
 
-template <bool QUICK, bool ULT>
+// MODE: 0 tracers with their own advect / diffuse flags, 1 every advected
+// tracer advected without horizontal diffusion, 2 advected with it.
+template <bool QUICK, bool ULT, int MODE>
 __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
                                                      SubStep ss, Tile Tl,
                                                      const f32::Face2 *__restrict__ fx2,
@@ -254,6 +256,53 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
   // loaded before any of it is used, so a thread has U tracers' loads in
   // flight at once.
   constexpr int U = kAdvGroup;
+  if (MODE != 0) {
+    // uniform flags: every stencil value is loaded (threads without a cell,
+    // and neighbours a cell does not use, read valid cells) and the face
+    // code has no per-tracer branches
+    constexpr bool HD = MODE == 2;
+    const int idx[13] = {c,    n1.z, n2.z, n1.w, n2.w, vm1, vm2,
+                         vp1,  vp2,  n1.x, n2.x, n1.y, n2.y};
+    for (int s0 = 0; s0 < ntb; s0 += U) {
+      float v[U][13];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int s = s0 + u < ntb ? s0 + u : s0;
+        const float *__restrict__ tr = tri + (size_t)sTr[s] * G.S;
+#pragma unroll
+        for (int q = 0; q < 13; ++q) v[u][q] = tr[idx[q]];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int s = s0 + u;
+        if (s >= ntb) break;
+        const float t0 = v[u][0];
+        const float tym1 = v[u][1], tym2 = v[u][2], typ1 = v[u][3], typ2 = v[u][4];
+        const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7], tp2 = v[u][8];
+        const float txm1 = v[u][9], txm2 = v[u][10], txp1 = v[u][11], txp2 = v[u][12];
+        const float Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
+        const float Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
+        const float Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
+        const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
+        const float Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
+        const float Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+        if (!on) continue;
+        const int n = sTr[s];
+        // FP64 flux divergence (tracers.c:888-892)
+        const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+        float val;
+        if (zt) {
+          const float Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
+          val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
+        } else {
+          val = (float)dtr;
+          if (zf) fzs[(size_t)n * G.ncol + col] = Fzb;
+        }
+        tro[(size_t)n * G.S + c] = val;
+      }
+    }
+    return;
+  }
   for (int s0 = 0; s0 < ntb; s0 += U) {
     float v[U][13];  // t0, y-2..y+2, z-2..z+2, x-2..x+2 (off-tile x only)
     int nn[U], tf[U];
