@@ -5,7 +5,12 @@ sub-stepping, surf_conc, tr_bounds, implicit vertical diffusion) over every
 wet cell and tracer of the workload window.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload stiff2048] [--precision fp32mixed|fp64]
+                  [--workload stiff2048] [--precision fp32mixed|fp64] [--no-fp64]
+
+The headline is the FP32-mixed path; the same line carries the plain FP64
+path run on the same inputs (its throughput, the speed-up, and the largest
+per-tracer error max|x32 - x64| / max|x64| after the same steps) and the
+FP64 mass drift of both over the run.
 
 Multi-GPU (torchrun, one process per GPU): every rank steps its own
 independent basin (a differently seeded copy of the workload), with no
@@ -24,6 +29,8 @@ import sys
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -38,7 +45,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="stiff2048")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32mixed"])
+    p.add_argument("--precision", default="fp32mixed", choices=["fp64", "fp32mixed"])
+    p.add_argument("--no-fp64", action="store_true",
+                   help="skip the plain FP64 arm that the mixed-precision line compares with")
+    p.add_argument("--size", default="",
+                   help="NXxNY: the workload's grid at another horizontal size (profiling)")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", default="512x256")
     p.add_argument("--no-cpu", action="store_true")
@@ -176,6 +187,54 @@ def run_reference(args, rank, world):
                     "d2h_bytes_per_step": 0}}
 
 
+def kernel_bytes(case, part, fp64):
+    """Algorithmic HBM bytes of one launch of a transport kernel: every tracer
+    value read once and written once, plus its per-cell fields (advection:
+    u1flux3d, u2flux3d, w, dz; column kernel: the four LU factors)."""
+    s = 8 if fp64 else 4
+    return case.nwet * case.ntr * 2 * s + case.nwet * 4 * s
+
+
+def time_arm(case, prec, local, args, pg, dev, clocks=None):
+    """Warm up, then time args.steps graph-replayed steps on the library's
+    stream (CUDA events, barrier + synchronize on both sides, max over
+    ranks); then one profiled pass for the per-kernel split."""
+    import torch
+    from ems_b200 import gpu
+    step = gpu.TracerStep(case, precision=prec, device=local)
+    step.start()
+    m0 = step.mass()
+    stream = torch.cuda.ExternalStream(step.stream(), device=dev)
+    step.run(max(args.warmup, 3))
+    step.sync()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    l0 = step.launches()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    step.run(args.steps)
+    e1.record(stream)
+    diag = step.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    launches = step.launches() - l0
+    ms_step = max_over_ranks(pg, e0.elapsed_time(e1), dev) / args.steps
+    # per-kernel times (profile mode launches the same kernels with events)
+    step.profile(True)
+    step.run(args.steps)
+    step.sync()
+    parts = [step.kernel_time(p)[0] for p in range(3)]
+    step.profile(False)
+    m1 = step.mass()
+    drift = float(np.max(np.abs(m1 - m0) / np.maximum(np.abs(m0), 1e-300)))
+    return dict(step=step, ms_step=ms_step, launches=launches, clocks=clk, diag=diag,
+                parts=parts, mass_drift=drift, nsteps=max(args.warmup, 3) + 2 * args.steps)
+
+
 def main():
     args = parse()
     world, rank, local, pg = dist_init()
@@ -187,62 +246,60 @@ def main():
             pg.destroy_process_group()
         return
 
-    import numpy as np
     import torch
 
     from ems_b200 import gpu, synth
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    prec = gpu.FP32_MIXED if args.precision == "fp32mixed" else gpu.FP64
-    case = synth.make(args.workload, seed=2048 + rank)
-    step = gpu.TracerStep(case, precision=prec, device=local)
-    step.start()
-    stream = torch.cuda.ExternalStream(step.stream(), device=dev)
-
-    # warm-up (also learns the sub-step schedule and captures the step graph)
-    step.run(max(args.warmup, 3))
-    step.sync()
-
-    # timed region: per-step transport kernels are bracketed by CUDA events on
-    # the library's stream (profile mode launches the same kernels directly)
-    step.profile(True)
-    if pg is not None:
-        pg.barrier()
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    l0 = step.launches()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    step.run(args.steps)
-    e1.record(stream)
-    diag = step.sync()
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    launches = step.launches() - l0
-    ms_total = e0.elapsed_time(e1)
-    kern_ms, kern_n = step.kernel_time()
-    step.profile(False)
-    ms_total = max_over_ranks(pg, ms_total, dev)
-    ms_step = ms_total / args.steps
-
-    # graph-replay timing of the same steps (no per-kernel events)
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    step.run(args.steps)
-    g1.record(stream)
-    step.sync()
-    graph_ms_step = max_over_ranks(pg, g0.elapsed_time(g1), dev) / args.steps
-
+    mixed = args.precision == "fp32mixed"
+    kw = {}
+    if args.size:
+        kw["nx"], kw["ny"] = (int(v) for v in args.size.split("x"))
+    case = synth.make(args.workload, seed=2048 + rank, **kw)
     units = case.nwet * case.ntr
-    value = units * world / (ms_step / 1000.0)
-    fp64 = prec == gpu.FP64
-    bytes_step = case.bytes_per_step(fp64=fp64)
+
+    # the headline arm (timed with clocks sampled), then the plain FP64 arm on
+    # the same inputs for the speed-up and the error of the mixed precision
+    arm = time_arm(case, gpu.FP32_MIXED if mixed else gpu.FP64, local, args, pg, dev,
+                   ClockSampler(local))
+    step = arm["step"]
+    fp64 = None
+    if mixed and not args.no_fp64:
+        ref = time_arm(case, gpu.FP64, local, args, pg, dev)
+        t32, t64 = step.download(), ref["step"].download()
+        err = [float(np.max(np.abs(t32[n] - t64[n])) / max(float(np.max(np.abs(t64[n]))), 1e-300))
+               for n in range(case.ntr)]
+        fp64 = {"value": units * world / (ref["ms_step"] / 1000.0),
+                "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
+                "mass_rel_drift": ref["mass_drift"],
+                "speedup_fp32mixed": ref["ms_step"] / arm["ms_step"],
+                "max_rel_err_fp32mixed": max(err),
+                "steps_compared": arm["nsteps"]}
+        ref["step"].close()
+        del t32, t64
+
+    value = units * world / (arm["ms_step"] / 1000.0)
     hbm, peak_kind = peaks()
-    achieved = bytes_step / (kern_ms / 1000.0) / 1e9 if kern_ms > 0 else 0.0
+    f64b = not mixed
+    # the dominant transport kernel and its roofline
+    if mixed:
+        kern = {"k_adv32": arm["parts"][1], "k_vd32": arm["parts"][2]}
+    else:
+        kern = {"k_transport": arm["parts"][0]}
+    kname = max(kern, key=kern.get)
+    kms = kern[kname]
+    kb = kernel_bytes(case, 1, f64b) if mixed else case.bytes_per_step(fp64=True)
+    achieved = kb / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f).get("%s/%s/%s" % (kname, args.workload, args.precision))
+        if t:
+            traffic = t
+    except Exception:
+        pass
+    step_bytes = case.bytes_per_step(fp64=f64b)
 
     # end to end through the drop-in C-ABI call on pinned host buffers
     S = case.win.sgsiz
@@ -265,34 +322,38 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        ref = run_reference(argparse.Namespace(**dict(vars(args), steps=1, warmup=0)), 0, 1)
-        if ref and "value" in ref:
-            cpu = ref["cpu_baseline"]
+        rr = run_reference(argparse.Namespace(**dict(vars(args), steps=1, warmup=0)), 0, 1)
+        if rr and "value" in rr:
+            cpu = rr["cpu_baseline"]
 
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": arm["ms_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if fp64 else "f32-mixed", "data": "synthetic",
+        "dtype": "f32-mixed" if mixed else "f64", "data": "synthetic",
         "config": {
-            "workload": args.workload, "nx": case.win.nx, "ny": case.win.ny,
+            "workload": args.workload + ("@" + args.size if args.size else ""), "nx": case.win.nx, "ny": case.win.ny,
             "nz": case.win.nz, "tracers": case.ntr, "wet_cells": case.nwet,
             "columns": case.win.ncol, "precision": args.precision, "dt": case.dt,
-            "substeps": diag.nsub, "seed": case.seed,
-            "l2": "inputs larger than L2 (%.1f GB of tracers per step)" % (bytes_step / 1e9),
+            "substeps": arm["diag"].nsub, "seed": case.seed,
+            "l2": "inputs larger than L2 (%.1f GB of tracers and fields per step)" % (
+                step_bytes / 1e9),
             "parallelism": "independent basin per GPU" if world > 1 else "single GPU",
         },
-        "graph_ms_per_step": graph_ms_step,
-        "clocks": clk,
-        "e2e": {"value": units / e2e_s if e2e_s == e2e_s else None, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h,
+        "fp64": fp64,
+        "mass_rel_drift": arm["mass_drift"],
+        "clocks": arm["clocks"],
+        "e2e": {"value": units / e2e_s if e2e_s == e2e_s else None, "unit": UNIT,
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "shoc_tr_gpu_step on pinned host arrays (copies inside the timing)"},
-        "gpu_launches": launches,
+        "gpu_launches": arm["launches"],
+        "kernels_ms": dict(kern, transport=arm["parts"][0]),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "kernel": "k_transport<LAST>", "kernel_ms": kern_ms,
-                     "kernel_launches": kern_n, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": bytes_step},
+                     "frac": achieved / hbm, "traffic": traffic, "kernel": kname,
+                     "kernel_ms": kms, "algorithmic_bytes_per_launch": kb,
+                     "peak_source": peak_kind,
+                     "step_achieved": step_bytes / (arm["ms_step"] / 1000.0) / 1e9,
+                     "step_frac": step_bytes / (arm["ms_step"] / 1000.0) / 1e9 / hbm},
         "cpu_baseline": cpu,
     }
     if rank == 0:
