@@ -1,0 +1,90 @@
+"""Accuracy of the FP32-mixed step against the plain FP64 step.
+
+Both precisions step the same window from the same state on the GPU; every
+`every` steps the tracers are compared cell by cell over the wet cells:
+
+  max relative error  = max |x32 - x64| / max |x64|          (per tracer)
+  RMS relative error  = sqrt(sum (x32 - x64)^2 / sum x64^2)    (per tracer)
+
+and each path's tracer mass (FP64 compensated sum over the water columns) is
+compared with its initial value.  The FP64 path is bitwise equal to the
+reference's tracers.c on the parity cases, so it stands in for the FP64
+oracle at sizes the CPU cannot run for many steps.
+
+  python -m ems_b200.accuracy --workload stiff2048 --steps 1000 --every 100
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import gpu, synth
+
+
+def compare(case, steps, every, device=0, log=None):
+    """Per-tracer errors of FP32-mixed vs FP64 after every `every` steps."""
+    wet = case.win.wet_cells()
+    s64 = gpu.TracerStep(case, precision=gpu.FP64, device=device)
+    s32 = gpu.TracerStep(case, precision=gpu.FP32_MIXED, device=device)
+    s64.start()
+    s32.start()
+    m64_0, m32_0 = s64.mass(), s32.mass()
+    rows = []
+    done = 0
+    while done < steps:
+        k = min(every, steps - done)
+        s64.run(k)
+        s32.run(k)
+        s64.sync()
+        s32.sync()
+        done += k
+        a = s64.download()[:, wet]
+        b = s32.download()[:, wet]
+        d = b - a
+        mx = np.max(np.abs(d), axis=1) / np.maximum(np.max(np.abs(a), axis=1), 1e-300)
+        rms = np.sqrt(np.sum(d * d, axis=1) / np.maximum(np.sum(a * a, axis=1), 1e-300))
+        m64, m32 = s64.mass(), s32.mass()
+        row = {"step": done,
+               "max_rel": mx.tolist(), "rms_rel": rms.tolist(),
+               "mass_drift_fp64": (np.abs(m64 - m64_0) / np.abs(m64_0)).tolist(),
+               "mass_drift_fp32mixed": (np.abs(m32 - m32_0) / np.abs(m32_0)).tolist()}
+        rows.append(row)
+        if log:
+            log("step %d: max rel %.3g, RMS rel %.3g, mass drift fp64 %.3g, fp32-mixed %.3g" % (
+                done, mx.max(), rms.max(), max(row["mass_drift_fp64"]),
+                max(row["mass_drift_fp32mixed"])))
+    s64.close()
+    s32.close()
+    return rows
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--workload", default="stiff2048")
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--every", type=int, default=100)
+    p.add_argument("--seed", type=int, default=2048)
+    p.add_argument("--size", default="", help="NXxNY: the workload at another size")
+    p.add_argument("--json", default="")
+    a = p.parse_args()
+    kw = {}
+    if a.size:
+        kw["nx"], kw["ny"] = (int(v) for v in a.size.split("x"))
+    case = synth.make(a.workload, seed=a.seed, **kw)
+    t0 = time.time()
+    rows = compare(case, a.steps, a.every, log=lambda s: print(s, flush=True))
+    out = {"workload": a.workload + ("@" + a.size if a.size else ""), "seed": a.seed,
+           "steps": a.steps, "tracers": case.ntr, "wet_cells": case.nwet,
+           "seconds": time.time() - t0, "checkpoints": rows}
+    if a.json:
+        with open(a.json, "w") as f:
+            json.dump(out, f)
+    last = rows[-1]
+    print("per tracer after %d steps (max rel / RMS rel):" % last["step"])
+    for n in range(case.ntr):
+        print("  %2d  %.3e  %.3e" % (n, last["max_rel"][n], last["rms_rel"][n]))
+
+
+if __name__ == "__main__":
+    main()

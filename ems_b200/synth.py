@@ -321,7 +321,7 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
                land_frac=0.0, cell=(1000.0, 1000.0), curvilinear=False, umax=0.5,
                baroclinic=0.2, kz=("exp", 1e-2, 1e-5), tracers="gauss", nsteps=1,
                trasc=_abi.QUICKEST, ultimate=1, stab=_abi.SUB_STEP, hmin=0.07,
-               mintr=None, maxtr=None, eta_offset=None):
+               mintr=None, maxtr=None, eta_offset=None, hdiff=None):
     rng = np.random.default_rng(seed)
     layers = np.asarray(layers, np.float64)
     nz = len(layers) - 1
@@ -391,10 +391,21 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
         for n in range(ntr):
             tr[n, c] = np.where((ii + jj + n) % 7 < 3, 1.0 + n, 0.0)
 
+    # horizontal diffusion (hor_diffuse): hdiff = (Kh in m^2/s, per-tracer
+    # on/off); Kh on the wet cells' u1 and u2 faces
+    u1kh = u2kh = diffuse = None
+    if hdiff is not None:
+        u1kh = np.zeros(S)
+        u1kh[c] = hdiff[0]
+        u2kh = u1kh.copy()
+        diffuse = np.asarray(hdiff[1], np.int32)
+        assert len(diffuse) == ntr
+
     # ghost / above-surface values are filled by the step itself
     return Case(name, win, ntr, dt, u1, u2, w, u1flux3d, u2flux3d, Kz, eta, oldeta, tr,
                 trasc=trasc, ultimate=ultimate, stab=stab, hmin=hmin, seed=seed,
-                nsteps=nsteps, dzu1=dzu1, dzu2=dzu2, mintr=mintr, maxtr=maxtr)
+                nsteps=nsteps, dzu1=dzu1, dzu2=dzu2, mintr=mintr, maxtr=maxtr,
+                u1kh=u1kh, u2kh=u2kh, diffuse=diffuse)
 
 
 def uniform_layers(nz, depth):

@@ -24,6 +24,10 @@ CASES = {
                                  maxtr=[1.0, 2.0, 2.5]), 20),
     "small_thin_surface": ("small", dict(eta_offset=(1.9, -1.7), hmin=1.5,
                                          maxtr=[0.5, 0.5, 0.5], **MOVING), 4),
+    "small_hdiff": ("small", dict(hdiff=(40.0, [1, 1, 1])), 10),
+    "small_hdiff_mixed": ("small", dict(hdiff=(40.0, [1, 0, 1])), 10),
+    "small_vanleer_hdiff": ("small", dict(trasc=_abi.VANLEER, ultimate=0,
+                                          hdiff=(40.0, [0, 1, 1])), 10),
     "basin64": ("basin64", {}, 100),
 }
 

@@ -38,7 +38,8 @@ def run(case, nsteps):
 
 @pytest.mark.parametrize("kw", [
     {}, dict(trasc=_abi.VANLEER, ultimate=0), dict(trasc=_abi.VANLEER, ultimate=1),
-    dict(ultimate=0), dict(dt=2000.0)])
+    dict(ultimate=0), dict(dt=2000.0), dict(hdiff=(40.0, [1, 1, 1])),
+    dict(hdiff=(40.0, [1, 0, 1])), dict(trasc=_abi.VANLEER, ultimate=0, hdiff=(40.0, [0, 1, 1]))])
 def test_small_windows_within_tolerance(kw):
     case = synth.make("small", seed=61, **kw)
     out, sur, nsur, d = run(case, 10)
@@ -73,3 +74,15 @@ def test_drop512_fp32_mixed():
     ref = oracle.run_oracle(case, 3)[1]
     emax, erms = errors(case, out, ref)
     assert np.all(emax <= TOL), (emax, erms)
+
+
+def test_accuracy_report_small():
+    """ems_b200.accuracy: FP32-mixed against the FP64 GPU path over 20 steps;
+    the FP64 path conserves the tracer mass to round-off."""
+    from ems_b200 import accuracy
+    case = synth.make("small")
+    rows = accuracy.compare(case, 20, 10)
+    assert [r["step"] for r in rows] == [10, 20]
+    assert max(rows[-1]["max_rel"]) <= TOL
+    assert max(rows[-1]["rms_rel"]) <= TOL
+    assert max(rows[-1]["mass_drift_fp64"]) <= 1e-12
