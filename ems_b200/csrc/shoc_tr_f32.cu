@@ -45,7 +45,6 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *fzs, int vd_nw,
                     int any_hd, int adv_flags, cudaEvent_t *ev) {
-  const int ntile = Tl.ncolp / 32;
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {
     const int grid = (Tl.nwet + kAdvBlock - 1) / kAdvBlock;
@@ -64,14 +63,18 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
   }
   if (ev) cudaEventRecord(ev[1], st);
   const int nchunk = (T.nslot + vd_nw - 1) / vd_nw;
-  const size_t smem = vd32_smem(G.nz, vd_nw);
   const dim3 blk(32, vd_nw);
-  if (last)
-    k_vd32<true><<<ntile * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
-                                                     tout, fzs, vd_nw, nchunk);
-  else
-    k_vd32<false><<<ntile * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
-                                                      tout, fzs, vd_nw, nchunk);
+  for (int i = 0; i < Tl.nclass; i++) {
+    const int t0 = Tl.ctile[i], nt = Tl.ctile[i + 1] - t0, kbase = Tl.cbase[i];
+    if (nt <= 0) continue;
+    const size_t smem = vd32_smem(G.nz - kbase, vd_nw);
+    if (last)
+      k_vd32<true><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
+                                                   tout, fzs, vd_nw, nchunk, t0, kbase);
+    else
+      k_vd32<false><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
+                                                    tout, fzs, vd_nw, nchunk, t0, kbase);
+  }
   if (ev) cudaEventRecord(ev[2], st);
 }
 

@@ -68,6 +68,7 @@ struct shoc_tr_gpu {
   Tile tl{};                          // static tables of the column-tile kernels
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
+  std::vector<int> vd_depth;          // layers of the k_vd32 tiles, in their (sorted) order
   bool staged = false;                // column-tile fast path
   int cur = 0;
   int *bpt = nullptr, *bin = nullptr;
@@ -575,10 +576,25 @@ int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<u
         const int c = cellk[(size_t)k * ncolp + col];
         if (c && is_wet[c]) wet.push_back(c);
       }
-  // k_vd32 column order: the columns' own (spatial) order, so a warp's lanes
-  // at one layer are adjacent cells and its loads and stores coalesce
+  // k_vd32 column order: tiles of 32 adjacent columns (a warp's lanes at one
+  // layer are adjacent cells: coalesced loads and stores), the tiles sorted
+  // by depth so launches per depth class size shared memory to their tiles
+  const int ntile = ncolp / 32;
+  std::vector<int> tdepth(ntile, 0), tord(ntile);
+  for (int t = 0; t < ntile; t++) {
+    int kmin = nz;
+    for (int l = 0; l < 32 && t * 32 + l < ncol; l++) kmin = std::min(kmin, col_kb[t * 32 + l]);
+    tdepth[t] = nz - kmin;
+    tord[t] = t;
+  }
+  std::stable_sort(tord.begin(), tord.end(), [&](int a, int b) { return tdepth[a] < tdepth[b]; });
   std::vector<int> vdcol(ncolp, -1);
-  for (int i = 0; i < ncol; i++) vdcol[i] = i;
+  h->vd_depth.resize(ntile);
+  for (int i = 0; i < ntile; i++) {
+    const int t = tord[i];
+    h->vd_depth[i] = tdepth[t];
+    for (int l = 0; l < 32; l++) vdcol[i * 32 + l] = (t * 32 + l < ncol) ? t * 32 + l : -1;
+  }
   std::vector<int4> colrec(ncolp, make_int4(0, 0, nz, 0));
   for (int col = 0; col < ncol; col++)
     colrec[col] = make_int4(col_bot[col], g->w2_t[col + 1], col_kb[col], 0);
@@ -1036,6 +1052,31 @@ int launch_part_a(shoc_tr_gpu *h) {
   return 0;
 }
 
+// Depth classes of the k_vd32 launches for nw tracers per block: the deepest
+// tile that still lets 4, 3 and 2 blocks share an SM's shared memory bounds
+// a class; each class is launched with shared memory for its own depth.
+Tile vd_classes(const shoc_tr_gpu *h, int nw) {
+  Tile t = h->tl;
+  const int ntile = (int)h->vd_depth.size();
+  const size_t per_layer = vd32_smem(1, nw);
+  const size_t sm = 233472, rsv = 1024;
+  t.nclass = 0;
+  t.ctile[0] = 0;
+  int start = 0;
+  for (int blocks = 4; blocks >= 1 && start < ntile; blocks--) {
+    int dmax = (int)((sm / blocks - rsv) / per_layer);
+    if (blocks == 1 || dmax >= h->nz) dmax = h->nz;
+    int end = start;
+    while (end < ntile && h->vd_depth[end] <= dmax) end++;
+    if (end == start) continue;
+    t.cbase[t.nclass] = h->nz - h->vd_depth[end - 1];
+    t.ctile[++t.nclass] = end;
+    start = end;
+    if (dmax == h->nz) break;
+  }
+  return t;
+}
+
 int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
   cudaStream_t st = h->stream;
   int cur = cur0;
@@ -1058,15 +1099,17 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
       cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
       if (prof)
         for (auto &e : ev) cudaEventCreate(&e);
+      const Tile tl = vd_classes(h, tw);
       tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
-                     h->F3, h->W, h->O, h->T, ss, h->tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
+                     h->F3, h->W, h->O, h->T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
                      h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
       if (prof) {  // pairs share events; sync destroys each event once
         h->ev.push_back({0, ev[0], ev[2]});
         h->ev.push_back({1, ev[0], ev[1]});
         h->ev.push_back({2, ev[1], ev[2]});
       }
-      h->launches += 2;
+      h->launches += (h->T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
+      for (int i = 0; i < tl.nclass; i++) h->launches += tl.ctile[i + 1] > tl.ctile[i] ? 1 : 0;
       if (last)
         k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
                                                             tin, tout);

@@ -46,7 +46,11 @@ struct Tile {
   const int4 *nbz;   // [S] zm1, zm1(zm1), zp1, zp1(zp1)
   const int *colof;  // [S] 0-based column of each wet cell
   const int *wet;    // [nwet] the wet cells (w3_t order)
-  const int *vdcol;  // [ncolp] columns in k_vd32 order (-1: padding)
+  const int *vdcol;  // [ncolp] columns in k_vd32 order: whole tiles of 32
+                     // adjacent columns, shallow tiles first (-1: padding)
+  int nclass;        // k_vd32 depth classes: tiles [ctile[i], ctile[i+1]) have
+  int ctile[5];      //   no cell below layer cbase[i]
+  int cbase[4];
   const int4 *colrec;  // [ncolp] bottom cell, surface-layer cell, bottom layer
   int ncolp;         // columns rounded up to whole tiles
   int nwet;
@@ -256,7 +260,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
   // loaded before any of it is used, so a thread has U tracers' loads in
   // flight at once.
   constexpr int U = kAdvGroup;
-  if (MODE != 0) {
+  if constexpr (MODE != 0) {
     // uniform flags: every stencil value is loaded (threads without a cell,
     // and neighbours a cell does not use, read valid cells) and the face
     // code has no per-tracer branches
@@ -301,8 +305,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
         tro[(size_t)n * G.S + c] = val;
       }
     }
-    return;
-  }
+  } else {
   for (int s0 = 0; s0 < ntb; s0 += U) {
     float v[U][13];  // t0, y-2..y+2, z-2..z+2, x-2..x+2 (off-tile x only)
     int nn[U], tf[U];
@@ -370,15 +373,16 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
       tro[(size_t)nn[u] * G.S + c] = val;
     }
   }
+  }
 }
 
 // ---------------------------------------------------------------------------
 // k_vd32
 
-// shared memory of k_vd32 (bytes): LU float4[nz][32], colC int[nz][32],
-// A, S float[nz][nw][32]
-inline size_t vd32_smem(int nz, int nw) {
-  return (size_t)nz * 32 * 16 + (size_t)nz * 32 * 4 + (size_t)2 * nz * nw * 32 * 4;
+// shared memory of k_vd32 (bytes) for columns of at most nd layers:
+// LU float4[nd][32], colC int[nd][32], A, S float[nd][nw][32]
+inline size_t vd32_smem(int nd, int nw) {
+  return (size_t)nd * 32 * 16 + (size_t)nd * 32 * 4 + (size_t)2 * nd * nw * 32 * 4;
 }
 
 template <bool LAST>
@@ -389,29 +393,36 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
                                               const float *__restrict__ tri,
                                               float *__restrict__ tro,
                                               const float *__restrict__ fzs, int nw,
-                                              int nchunk) {
+                                              int nchunk, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int nz = G.nz;
-  float4 *LU = reinterpret_cast<float4 *>(smem);        // [nz][32]
-  int *colC = reinterpret_cast<int *>(LU + nz * 32);     // [nz][32]
-  float *A = reinterpret_cast<float *>(colC + nz * 32);  // [nz][nw][32]
-  float *Sv = A + nz * nw * 32;                          // [nz][nw][32]
+  // the arrays hold layers kbase .. nz-1 (every column of this launch's
+  // tiles starts at or above kbase), row r = layer - kbase
+  const int nz = G.nz, nd = nz - kbase;
+  float4 *LU = reinterpret_cast<float4 *>(smem);        // [nd][32]
+  int *colC = reinterpret_cast<int *>(LU + nd * 32);     // [nd][32]
+  float *A = reinterpret_cast<float *>(colC + nd * 32);  // [nd][nw][32]
+  float *Sv = A + nd * nw * 32;                          // [nd][nw][32]
 
   const int lane = threadIdx.x, wy = threadIdx.y;
-  const int tile = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int tile = tile0 + blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
   const int col = Tl.vdcol[tile * 32 + lane];
   const int slot = chunk * nw + wy;
   const int sa = nw * 32;
 
   const TileCol tc = tile_column(G, W, Tl, col);
-  const bool act = tc.act;
+  bool act = tc.act;
+  if (act && tc.kb < kbase) {  // not in this launch's depth class
+    act = false;
+    if (chunk == 0 && wy == 0) atomicOr(W.status, ST_GEOM);
+  }
   const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
   const ColInfo ci = tc.ci;
   const int kmin = __reduce_min_sync(0xffffffffu, act ? kb : nz);
   for (int k = kmin + wy; k < nz; k += nw) {
     const int c = (act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
-    colC[k * 32 + lane] = c;
-    if (LAST && c && k <= ks) cp_async16(&LU[k * 32 + lane], &lu32[c]);
+    const int r = k - kbase;
+    colC[r * 32 + lane] = c;
+    if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &lu32[c]);
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -433,7 +444,8 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   // values (the rest)
   {
     const float *src = tbdy ? to : tr;
-    for (int k = kb; k < nz; ++k) cp_async4(&Aj[k * sa], src + colC[k * 32 + lane]);
+    for (int k = kb; k < nz; ++k)
+      cp_async4(&Aj[(k - kbase) * sa], src + colC[(k - kbase) * 32 + lane]);
     cp_async_commit();
   }
   const double mn = T.mintr[n], mx = T.maxtr[n];
@@ -456,10 +468,10 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
 
   // the column in shared memory, from its bottom layer up: value (A),
   // Thomas storage (S), LU factors {dzdt, cm1, 1/div, ud} (L), cell (C)
-  float *const A0 = Aj + kb * sa;
-  float *const S0 = Sj + kb * sa;
-  const float4 *const L0 = LU + kb * 32 + lane;
-  const int *const C0 = colC + kb * 32 + lane;
+  float *const A0 = Aj + (kb - kbase) * sa;
+  float *const S0 = Sj + (kb - kbase) * sa;
+  const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
+  const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const int nk = ks - kb;  // cells below the surface cell
   long long nwarn = 0;
   float fwd = 0.f;  // Thomas forward carry (the bottom row's cm1 is 0)
