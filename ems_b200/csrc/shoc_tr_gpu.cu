@@ -1553,6 +1553,36 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
   return 0;
 }
 
+int shoc_tr_gpu_autotune(shoc_tr_gpu *h, int steps, int *tracers_per_block) {
+  if (!h || steps < 1) return SHOC_TR_EARG;
+  static const int cand[] = {2, 3, 4, 5, 6, 8};
+  const bool prof0 = h->profile;
+  int best_tw = h->tw;
+  double best = 1e300;
+  for (int c : cand) {
+    if (shoc_tr_gpu_set_tiling(h, 0, c) != SHOC_TR_OK) continue;
+    shoc_tr_gpu_profile(h, 1);
+    int rc = shoc_tr_gpu_run(h, steps);
+    if (!rc) rc = shoc_tr_gpu_sync(h, nullptr);
+    if (rc) {
+      shoc_tr_gpu_set_tiling(h, 0, best_tw);
+      h->profile = prof0;
+      return rc;
+    }
+    double ms = 0.0;
+    int n = 0;
+    shoc_tr_gpu_kernel_time(h, &ms, &n);
+    if (n > 0 && ms < best) {
+      best = ms;
+      best_tw = c;
+    }
+  }
+  shoc_tr_gpu_set_tiling(h, 0, best_tw);
+  shoc_tr_gpu_profile(h, prof0 ? 1 : 0);
+  if (tracers_per_block) *tracers_per_block = best_tw;
+  return SHOC_TR_OK;
+}
+
 int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable) {
   if (!h) return SHOC_TR_EARG;
   h->profile = enable != 0;

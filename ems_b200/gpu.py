@@ -23,7 +23,7 @@ EXPORTS = (
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
     "shoc_tr_gpu_mass_noalloc",
-    "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_profile",
+    "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
 )
@@ -58,6 +58,7 @@ def lib(path=None):
     L.shoc_tr_gpu_stream.argtypes = [H]
     L.shoc_tr_gpu_stream.restype = C.c_void_p
     L.shoc_tr_gpu_set_tiling.argtypes = [H, C.c_int, C.c_int]
+    L.shoc_tr_gpu_autotune.argtypes = [H, C.c_int, C.POINTER(C.c_int)]
     L.shoc_tr_gpu_profile.argtypes = [H, C.c_int]
     L.shoc_tr_gpu_kernel_time.argtypes = [H, C.POINTER(C.c_double), C.POINTER(C.c_int)]
     L.shoc_tr_gpu_kernel_time_part.argtypes = [H, C.c_int, C.POINTER(C.c_double),
@@ -183,6 +184,13 @@ class TracerStep:
 
     def set_tiling(self, cols=0, tracers=0):
         _check("set_tiling", self.L.shoc_tr_gpu_set_tiling(self.h, cols, tracers))
+
+    def autotune(self, steps=2):
+        """Pick the tracers per block with the fastest transport (runs
+        `steps` real steps per candidate); returns the choice."""
+        tw = C.c_int()
+        _check("autotune", self.L.shoc_tr_gpu_autotune(self.h, int(steps), C.byref(tw)))
+        return tw.value
 
     def profile(self, on=True):
         _check("profile", self.L.shoc_tr_gpu_profile(self.h, 1 if on else 0))

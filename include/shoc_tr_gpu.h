@@ -104,6 +104,14 @@ void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
  * 0 keeps the current value.  Takes effect at the next step. */
 int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block);
 
+/* Autotuner: runs `steps` steps (real steps: the tracers advance exactly as
+ * with shoc_tr_gpu_run, and the results do not depend on the tiling) with
+ * each candidate number of tracers per block, times the transport kernels
+ * with CUDA events, and keeps the fastest; returns it in *tracers_per_block
+ * (may be NULL).  Call after the flow is set.  No reference counterpart
+ * (launch tuning of this library). */
+int shoc_tr_gpu_autotune(shoc_tr_gpu *h, int steps, int *tracers_per_block);
+
 /* Time of the transport of a step's last sub-step (the transport kernels
  * of the precision: one launch for SHOC_TR_FP64, the advection and the column
  * kernel for SHOC_TR_FP32_MIXED), averaged over the steps since the last call

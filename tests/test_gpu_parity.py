@@ -138,3 +138,25 @@ def test_substep_limit_raises():
         t.run(1)
     assert e.value.code == 1
     t.close()
+
+
+@pytest.mark.parametrize("prec", [gpu.FP64, gpu.FP32_MIXED])
+def test_autotune_keeps_results(prec):
+    """The autotuner's trial steps are real steps: 6 candidates x 1 step plus
+    2 more steps give the same tracers as 8 plain steps, bit for bit."""
+    case = synth.make("small", seed=48)
+    ref = gpu.TracerStep(case, precision=prec)
+    ref.start()
+    ref.run(8)
+    ref.sync()
+    a = ref.download()
+    ref.close()
+    t = gpu.TracerStep(case, precision=prec)
+    t.start()
+    tw = t.autotune(1)
+    assert tw in (2, 3, 4, 5, 6, 8)
+    t.run(2)
+    t.sync()
+    b = t.download()
+    t.close()
+    np.testing.assert_array_equal(a[:, 1:], b[:, 1:])
