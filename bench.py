@@ -272,6 +272,7 @@ def main():
                for n in range(case.ntr)]
         fp64 = {"value": units * world / (ref["ms_step"] / 1000.0),
                 "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
+                "kernels_ms": {"k_adv64": ref["parts"][1], "k_vd64": ref["parts"][2]},
                 "mass_rel_drift": ref["mass_drift"],
                 "speedup_fp32mixed": ref["ms_step"] / arm["ms_step"],
                 "max_rel_err_fp32mixed": max(err),
@@ -286,10 +287,10 @@ def main():
     if mixed:
         kern = {"k_adv32": arm["parts"][1], "k_vd32": arm["parts"][2]}
     else:
-        kern = {"k_transport": arm["parts"][0]}
+        kern = {"k_adv64": arm["parts"][1], "k_vd64": arm["parts"][2]}
     kname = max(kern, key=kern.get)
     kms = kern[kname]
-    kb = kernel_bytes(case, 1, f64b) if mixed else case.bytes_per_step(fp64=True)
+    kb = kernel_bytes(case, 1, f64b)
     achieved = kb / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
     traffic = None
     try:

@@ -10,10 +10,14 @@
 //               and the tracer-independent tridiagonal LU factors of
 //               vert_diffuse_3d / implicit_vdiff_tr (:3841-3889, :4185-4195)
 //   per sub-step:
-//     k_courant   w6/w7/w8 (:726-737)
-//     k_transport all (column, tracer) pairs: see column_pass
-//     k_serial    the rare columns whose tr_bounds thin-surface fix couples
-//                 tracers, one thread per column looping over tracers
+//     k_courant   w6/w7/w8 (:726-737) of the general-path columns
+//     k_adv32 + k_vd32 (FP32-mixed, shoc_tr_tile.cuh) or k_adv64 + k_vd64
+//                 (FP64, shoc_tr_tile64.cuh): the columns whose surface cell
+//                 stays in its layer, one thread per cell, then one per
+//                 (column, tracer)
+//     k_serial    the other columns (surface crossing a layer face, thin-
+//                 surface fix coupling tracers, degenerate solve range), one
+//                 thread per column looping over tracers: column_pass
 // Tracers ping-pong between two buffers; a step is captured in a CUDA graph
 // once its sub-step schedule is known.
 #include <cuda_runtime.h>
@@ -30,6 +34,7 @@
 #include "shoc_tr_gpu.h"
 #include "shoc_tr_kernels.cuh"
 #include "shoc_tr_launch.h"
+#include "shoc_tr_tile64.cuh"
 
 using namespace shoc;
 
@@ -67,6 +72,7 @@ struct shoc_tr_gpu {
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
   Tile tl{};                          // static tables of the column-tile kernels
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
+  double *fzs64 = nullptr;            // the same, FP64 path
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
   std::vector<int> vd_depth;          // layers of the k_vd32 tiles, in their (sorted) order
   bool staged = false;                // column-tile fast path
@@ -390,39 +396,6 @@ __global__ void k_courant(Geo G, Flow F, Work W, double dtu, int only_listed) {
   }
 }
 
-// Main transport kernel: block = 32 adjacent columns x tw tracers; the tw
-// tracer warps of one block share the columns' per-cell data through L1.
-template <bool LAST>
-__global__ void __launch_bounds__(256) k_transport(Geo G, Flow F, Work W, Opt O, TrSet T,
-                                                   SubStep ss, const double *__restrict__ tr_in,
-                                                   double *__restrict__ tr_out, int tw,
-                                                   int nchunk) {
-  extern __shared__ double sol_s[];
-  const int lane = threadIdx.x, wy = threadIdx.y;
-  const int tile = blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
-  const int col = tile * 32 + lane;
-  const int slot = chunk * tw + wy;
-  if (slot >= T.nslot) return;  // warp-uniform
-  bool act = col < G.ncol;
-  if (act && (W.col[col].flags & COL_SERIAL)) act = false;
-  int kb = act ? G.col_kb[col] : G.nz;
-  int kstart = __reduce_min_sync(0xffffffffu, kb);
-  const int n = T.slot_tr[slot];
-  SmemSol sol{sol_s + wy * 32 + lane, tw * 32};
-  bool c3 = false;
-  unsigned long long warn = 0;
-  int stat = 0;
-  column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S, col,
-                    n, kstart, act, sol, c3, warn, stat);
-  unsigned long long wsum = warn;
-  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
-  int sor = (int)__reduce_or_sync(0xffffffffu, (unsigned)stat);
-  if (lane == 0) {
-    if (wsum) atomicAdd(W.nwarn, wsum);
-    if (sor) atomicOr(W.status, sor);
-  }
-}
-
 // Columns where tr_bounds' thin-surface cursor can move between tracers:
 // one thread per column, tracers in tbdy order, as the reference loops.
 template <bool LAST, class TR>
@@ -507,6 +480,11 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
     for (int i = 0; i < (int)(blockDim.x >> 5); i++) neumaier(b, bc, part[i]);
     out[(size_t)n * gridDim.x + blockIdx.x] = b + bc;
   }
+}
+
+// shared memory of the column kernel of the handle's precision
+size_t vd_smem(const shoc_tr_gpu *h, int nd, int nw) {
+  return h->esize == sizeof(float) ? vd32_smem(nd, nw) : vd64_smem(nd, nw);
 }
 
 // Static tables of the column-tile kernel: the cell of every column at every
@@ -907,7 +885,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<int>(h, &h->d_counts, nullptr, 2));
   const bool f32p = precision == SHOC_TR_FP32_MIXED;
   h->esize = f32p ? sizeof(float) : sizeof(double);
-  h->staged = f32p;
+  h->staged = true;
   for (int b = 0; b < 2; b++) {
     if (f32p) {
       float *fp = nullptr;
@@ -944,9 +922,11 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     }
     TRY(dupload(h, &h->fx2, ax.data(), S2));
     TRY(dupload(h, &h->fy2, ay.data(), S2));
-    TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
     TRY(dupload<float>(h, &h->fzs, nullptr, (size_t)ntr * ncol));
+  } else {
+    TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   }
+  TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
   // flow fields
   Flow &F = h->F;
   TRY(dupload<double>(h, (double **)&F.u1, nullptr, S));
@@ -972,19 +952,18 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   h->h_counts = (int *)((char *)pin + 24);
   // tiling: tracers per block
   int tw = 8;
-  if (h->staged) {
-    // tracers per k_vd32 block: two blocks per SM, balanced chunks
-    while (tw > 1 && vd32_smem(g->nz, tw) > 113 * 1024) tw--;
+  {
+    // tracers per column-kernel block: two blocks per SM at full depth,
+    // balanced chunks
+    while (tw > 1 && vd_smem(h, g->nz, tw) > 113 * 1024) tw--;
     int nch = (h->nslot + tw - 1) / std::max(tw, 1);
     if (nch > 0) tw = (h->nslot + nch - 1) / nch;
     if (tw < 1) tw = 1;
-  } else {
-    while (tw > 1 && (size_t)g->nz * tw * 32 * sizeof(double) > 200 * 1024) tw /= 2;
   }
   h->tw = tw;
-  if (cudaFuncSetAttribute(k_transport<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_vd64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
-      cudaFuncSetAttribute(k_transport<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(k_vd64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
       tile32_set_smem_attr() != cudaSuccess)
     TRY(SHOC_TR_ECUDA);
@@ -1052,13 +1031,68 @@ int launch_part_a(shoc_tr_gpu *h) {
   return 0;
 }
 
+// One FP64 transport sub-step over the staged columns: k_adv64, then one
+// k_vd64 launch per depth class.  Returns the kernels launched.
+template <bool Q, bool U, int M>
+void adv64(const shoc_tr_gpu *h, int grid, const SubStep &ss, const Tile &tl, const double *tin,
+           double *tout) {
+  k_adv64<Q, U, M><<<grid, kAdvBlock, 0, h->stream>>>(h->G, h->F, h->W, h->T, ss, tl, tin,
+                                                      tout, h->fzs64, h->any_hdiff ? 1 : 0);
+}
+template <bool Q, bool U>
+void adv64_mode(const shoc_tr_gpu *h, int grid, const SubStep &ss, const Tile &tl,
+                const double *tin, double *tout) {
+  if (h->adv_flags == 1)
+    adv64<Q, U, 1>(h, grid, ss, tl, tin, tout);
+  else if (h->adv_flags == 2)
+    adv64<Q, U, 2>(h, grid, ss, tl, tin, tout);
+  else
+    adv64<Q, U, 0>(h, grid, ss, tl, tin, tout);
+}
+int tile64_substep(const shoc_tr_gpu *h, bool last, const SubStep &ss, const Tile &tl,
+                   const double *tin, double *tout, int nw, cudaEvent_t *ev) {
+  cudaStream_t st = h->stream;
+  int nl = 0;
+  if (ev) cudaEventRecord(ev[0], st);
+  if (h->T.ntb > 0 && tl.nwet > 0) {
+    const int grid = (tl.nwet + kAdvBlock - 1) / kAdvBlock;
+    const bool q = h->O.trasc == SHOC_TR_QUICKEST, u = h->O.ultimate != 0;
+    if (q && u)
+      adv64_mode<true, true>(h, grid, ss, tl, tin, tout);
+    else if (q)
+      adv64_mode<true, false>(h, grid, ss, tl, tin, tout);
+    else if (u)
+      adv64_mode<false, true>(h, grid, ss, tl, tin, tout);
+    else
+      adv64_mode<false, false>(h, grid, ss, tl, tin, tout);
+    nl++;
+  }
+  if (ev) cudaEventRecord(ev[1], st);
+  const int nchunk = (h->T.nslot + nw - 1) / nw;
+  const dim3 blk(32, nw);
+  for (int i = 0; i < tl.nclass; i++) {
+    const int t0 = tl.ctile[i], nt = tl.ctile[i + 1] - t0, kbase = tl.cbase[i];
+    if (nt <= 0) continue;
+    const size_t smem = vd64_smem(h->nz - kbase, nw);
+    if (last)
+      k_vd64<true><<<nt * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tl, tin,
+                                                   tout, h->fzs64, nw, nchunk, t0, kbase);
+    else
+      k_vd64<false><<<nt * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tl, tin,
+                                                    tout, h->fzs64, nw, nchunk, t0, kbase);
+    nl++;
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  return nl;
+}
+
 // Depth classes of the k_vd32 launches for nw tracers per block: the deepest
 // tile that still lets 4, 3 and 2 blocks share an SM's shared memory bounds
 // a class; each class is launched with shared memory for its own depth.
 Tile vd_classes(const shoc_tr_gpu *h, int nw) {
   Tile t = h->tl;
   const int ntile = (int)h->vd_depth.size();
-  const size_t per_layer = vd32_smem(1, nw);
+  const size_t per_layer = vd_smem(h, 1, nw);
   const size_t sm = 233472, rsv = 1024;
   t.nclass = 0;
   t.ctile[0] = 0;
@@ -1082,17 +1116,13 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
   int cur = cur0;
   const int nsub = (int)s.sub.size();
   const int tw = h->tw;
-  const int nchunk = (h->nslot + tw - 1) / tw;
-  const int ntile = (h->ncol + 31) / 32;
-  dim3 blk(32, tw);
-  size_t smem = (size_t)h->nz * tw * 32 * sizeof(double);
   int cblocks = std::min((h->S + 255) / 256, 148 * 32);
   for (int i = 0; i < nsub; i++) {
     const SubStep &ss = s.sub[i];
     bool last = (i == nsub - 1);
     k_courant<<<cblocks, 256, 0, st>>>(h->G, h->F, h->W, ss.dtu, h->staged ? 1 : 0);
     h->launches++;
-    if (h->staged && h->nslot > 0) {
+    if (h->esize == sizeof(float) && h->nslot > 0) {  // FP32-mixed
       const float *tin = (const float *)h->tr[cur];
       float *tout = (float *)h->tr[cur ^ 1];
       bool prof = h->profile && last;
@@ -1124,23 +1154,17 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
     double *tout = (double *)h->tr[cur ^ 1];
     if (h->nslot > 0) {
       bool prof = h->profile && last;
-      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+      if (prof)
+        for (auto &e : ev) cudaEventCreate(&e);
+      const Tile tl = vd_classes(h, tw);
+      const int nl = tile64_substep(h, last, ss, tl, tin, tout, tw, prof ? ev : nullptr);
       if (prof) {
-        cudaEventCreate(&e0);
-        cudaEventCreate(&e1);
-        cudaEventRecord(e0, st);
+        h->ev.push_back({0, ev[0], ev[2]});
+        h->ev.push_back({1, ev[0], ev[1]});
+        h->ev.push_back({2, ev[1], ev[2]});
       }
-      if (last)
-        k_transport<true><<<ntile * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                            tin, tout, tw, nchunk);
-      else
-        k_transport<false><<<ntile * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                             tin, tout, tw, nchunk);
-      if (prof) {
-        cudaEventRecord(e1, st);
-        h->ev.push_back({0, e0, e1});
-      }
-      h->launches++;
+      h->launches += nl;
       if (last)
         k_serial<true, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
                                                              tin, tout);
@@ -1539,10 +1563,7 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
   if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
   if (tracers_per_block > 0) {
     if (tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
-    if (h->staged && vd32_smem(h->nz, tracers_per_block) > 227 * 1024)
-      return SHOC_TR_EUNSUPPORTED;
-    if (!h->staged && (size_t)h->nz * tracers_per_block * 32 * sizeof(double) > 227 * 1024)
-      return SHOC_TR_EUNSUPPORTED;
+    if (vd_smem(h, h->nz, tracers_per_block) > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
     h->tw = tracers_per_block;
     for (int i = 0; i < 2; i++)
       if (h->graph[i]) {
