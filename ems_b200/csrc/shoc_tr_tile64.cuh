@@ -56,43 +56,28 @@ __device__ __forceinline__ double hface64(bool eb, bool adv, bool hd, double cr,
   return v;
 }
 
-// The vertical face of flux_z with its Courant number, work-array values and
-// w dtu.
-struct ZFace64 {
-  double cz, w5, db, df, w9m, w90, w9p, vel, wdtu;
-};
+// The vertical face of flux_z at cell c (below it zm, above it zp) with its
+// Courant number cz = w dtu / w9 and w dtu precomputed; the work-array
+// values are read here (cached loads) to keep them out of registers.
 template <bool QUICK, bool ULT>
-__device__ __forceinline__ double zface64(const ZFace64 &z, double tm2, double tm1, double t0,
-                                          double tp1) {
+__device__ __forceinline__ double zface64(const Flow &F, const Work &W, int c, int zm, int zp,
+                                          double cz, double wdtu, double tm2, double tm1,
+                                          double t0, double tp1) {
   double v;
   if (QUICK)
-    v = quickest_zface(z.cz, z.w5, z.db, z.df, z.w9m, z.w90, z.w9p, tm2, tm1, t0, tp1);
+    v = quickest_zface(cz, W.w5[c], W.dbz[c], W.dfz[c], W.w9[zm], W.w9[c], W.w9[zp], tm2, tm1,
+                       t0, tp1);
   else
-    v = vanleer_face(z.vel, z.cz, tm2, tm1, t0, tp1);
-  if (ULT) v = ultimate_face(z.cz, v, tm2, tm1, t0, tp1);
-  return v * z.wdtu;
-}
-
-__device__ __forceinline__ ZFace64 zface64_at(const Flow &F, const Work &W, int c, int zm, int zp,
-                                              double dtu) {
-  ZFace64 z;
-  z.vel = F.w[c];
-  z.cz = F.w[c] * dtu / (W.w9[c] * 1.0);  // tracers.c:735
-  z.w5 = W.w5[c];
-  z.db = W.dbz[c];
-  z.df = W.dfz[c];
-  z.w9m = W.w9[zm];  // the sediment cell's w9 is 0
-  z.w90 = W.w9[c];
-  z.w9p = W.w9[zp];
-  z.wdtu = F.w[c] * dtu;
-  return z;
+    v = vanleer_face(F.w[c], cz, tm2, tm1, t0, tp1);
+  if (ULT) v = ultimate_face(cz, v, tm2, tm1, t0, tp1);
+  return v * wdtu;
 }
 
 // ---------------------------------------------------------------------------
 // k_adv64
 
 template <bool QUICK, bool ULT, int MODE>
-__global__ void __launch_bounds__(kAdvBlock) k_adv64(Geo G, Flow F, Work W, TrSet T,
+__global__ void __launch_bounds__(kAdvBlock, 2) k_adv64(Geo G, Flow F, Work W, TrSet T,
                                                      SubStep ss, Tile Tl,
                                                      const double *__restrict__ tri,
                                                      double *__restrict__ tro,
@@ -137,18 +122,16 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv64(Geo G, Flow F, Work W, TrSe
   const int cd1 = __shfl_down_sync(FULL, c, 1);
   const bool sxp1 = on && lane <= 30 && cd1 && n1.y == cd1;
 
-  // tracer-independent face data
+  // tracer-independent face data: Courant numbers and volume fluxes (the
+  // metric factors and work arrays are read per face from cache)
   const double dtu = ss.dtu;
   const bool hdf = any_hd != 0;
-  const int xp = n1.y, yp = n1.w, zp = nzv.z;
+  const int xp = n1.y, yp = n1.w, zp = nzv.z, zm = nzv.x;
   const bool e1 = fl & CF_E1, e2 = fl & CF_E2;
   const bool ewet = !sxp1 && (fl & FL_XP_WET), nwet = fl & FL_YP_WET;
   const bool e1e = fl & FL_XP_E1, e2n = fl & FL_YP_E2;
-  double crw = 0.0, crs = 0.0, crn = 0.0, cre = 0.0;
-  double Uw = 0.0, Us = 0.0, Un = 0.0, Ue = 0.0;
-  double Pw = 0.0, Ps = 0.0, Pn = 0.0, Pe = 0.0, Hw = 1.0, Hs = 1.0, Hn = 1.0, He = 1.0;
-  double area = 1.0, dzc = 1.0;
-  ZFace64 zb{}, zt{};
+  double crw = 0.0, crs = 0.0, crn = 0.0, cre = 0.0, czb = 0.0, czt = 0.0;
+  double Uw = 0.0, Us = 0.0, Un = 0.0, Ue = 0.0, wdb = 0.0, wdt = 0.0;
   const bool zf = on && k <= ks, ztop = on && k < ks;
   if (on) {
     // Courant numbers as tracers.c:730-736 (w6, w7, w8)
@@ -164,32 +147,19 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv64(Geo G, Flow F, Work W, TrSe
       cre = F.u1[xp] * dtu / G.h1au1[me.x];
       Ue = F.u1flux3d[xp];
     }
-    if (hdf) {
-      // hor_diffuse (tracers.c:3654-3667): csx = dzu1 h2au1 mdx, then
-      // csx u1kh (t0 - tm1) / h1au1
-      Pw = F.dzu1[c] * G.h2au1[c2] * 1.0 * F.u1kh[c];
-      Hw = G.h1au1[c2];
-      Ps = F.dzu2[c] * G.h1au2[c2] * 1.0 * F.u2kh[c];
-      Hs = G.h2au2[c2];
-      if (nwet) {
-        Pn = F.dzu2[yp] * G.h1au2[me.y] * 1.0 * F.u2kh[yp];
-        Hn = G.h2au2[me.y];
-      }
-      if (ewet) {
-        Pe = F.dzu1[xp] * G.h2au1[me.x] * 1.0 * F.u1kh[xp];
-        He = G.h1au1[me.x];
-      }
+    if (zf) {
+      czb = F.w[c] * dtu / (W.w9[c] * 1.0);
+      wdb = F.w[c] * dtu;
     }
-    if (zf) zb = zface64_at(F, W, c, nzv.x, zp, dtu);
-    if (ztop) zt = zface64_at(F, W, zp, c, nzv.w, dtu);
-    area = G.cellarea[c2];
-    dzc = W.dz[c];
+    if (ztop) {
+      czt = F.w[zp] * dtu / (W.w9[zp] * 1.0);
+      wdt = F.w[zp] * dtu;
+    }
   }
-  const Face2D mxw = on ? G.fx[c2] : Face2D{}, mys = on ? G.fy[c2] : Face2D{};
-  const Face2D myn = (on && nwet) ? G.fy[me.y] : Face2D{};
-  const Face2D mxe = (on && ewet) ? G.fx[me.x] : Face2D{};
-  const double u1c = on ? F.u1[c] : 0.0, u2c = on ? F.u2[c] : 0.0;
-  const double u2n = (on && nwet) ? F.u2[yp] : 0.0, u1e = (on && ewet) ? F.u1[xp] : 0.0;
+  // hor_diffuse (tracers.c:3654-3667): csx = dzu1 h2au1 mdx, then
+  // csx u1kh (t0 - tm1) / h1au1 (the e2 analogue for y)
+  auto Px = [&](int cc, int cc2) { return F.dzu1[cc] * G.h2au1[cc2] * 1.0 * F.u1kh[cc]; };
+  auto Py = [&](int cc, int cc2) { return F.dzu2[cc] * G.h1au2[cc2] * 1.0 * F.u2kh[cc]; };
   // vertical neighbours (bottom: the sediment ghost holds the bottom value)
   const int vm1 = (k - 1 >= kb) ? nzv.x : c;
   const int vm2 = (k - 2 >= kb) ? nzv.y : vm1;
@@ -213,14 +183,17 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv64(Geo G, Flow F, Work W, TrSe
     const bool hor = adv || hd;
     double Fxw = 0.0, Fys = 0.0, Fyn = 0.0, Fxe = 0.0;
     if (on && hor) {
-      Fxw = hface64<QUICK, ULT>(e1, adv, hd, crw, u1c, mxw, Uw, Pw, Hw, txm2, txm1, t0, txp1);
-      Fys = hface64<QUICK, ULT>(e2, adv, hd, crs, u2c, mys, Us, Ps, Hs, tym2, tym1, t0, typ1);
+      const bool h = hdf && hd;
+      Fxw = hface64<QUICK, ULT>(e1, adv, hd, crw, F.u1[c], G.fx[c2], Uw, h ? Px(c, c2) : 0.0,
+                                G.h1au1[c2], txm2, txm1, t0, txp1);
+      Fys = hface64<QUICK, ULT>(e2, adv, hd, crs, F.u2[c], G.fy[c2], Us, h ? Py(c, c2) : 0.0,
+                                G.h2au2[c2], tym2, tym1, t0, typ1);
       if (nwet)
-        Fyn = hface64<QUICK, ULT>(e2n, adv, hd, crn, u2n, myn, Un, Pn, Hn, tym1, t0, typ1,
-                                  typ2);
+        Fyn = hface64<QUICK, ULT>(e2n, adv, hd, crn, F.u2[yp], G.fy[me.y], Un,
+                                  h ? Py(yp, me.y) : 0.0, G.h2au2[me.y], tym1, t0, typ1, typ2);
       if (ewet)
-        Fxe = hface64<QUICK, ULT>(e1e, adv, hd, cre, u1e, mxe, Ue, Pe, He, txm1, t0, txp1,
-                                  txp2);
+        Fxe = hface64<QUICK, ULT>(e1e, adv, hd, cre, F.u1[xp], G.fx[me.x], Ue,
+                                  h ? Px(xp, me.x) : 0.0, G.h1au1[me.x], txm1, t0, txp1, txp2);
     }
     const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
     if (!on) continue;
@@ -230,16 +203,19 @@ __global__ void __launch_bounds__(kAdvBlock) k_adv64(Geo G, Flow F, Work W, TrSe
     double val;
     if (ztop) {
       // interior cell (tracers.c:912-925); Ds = Hn1 = 1 in z coordinates
-      const double Fzb = adv ? zface64<QUICK, ULT>(zb, tm2, tm1, t0, tp1) : 0.0;
-      const double Fzt = adv ? zface64<QUICK, ULT>(zt, tm1, t0, tp1, tp2) : 0.0;
+      const double Fzb =
+          adv ? zface64<QUICK, ULT>(F, W, c, zm, zp, czb, wdb, tm2, tm1, t0, tp1) : 0.0;
+      const double Fzt =
+          adv ? zface64<QUICK, ULT>(F, W, zp, c, nzv.w, czt, wdt, tm1, t0, tp1, tp2) : 0.0;
       double a = t0 * 1.0;
-      a -= ((dtr / area + (Fzt - Fzb)) / dzc);
+      a -= ((dtr / G.cellarea[c2] + (Fzt - Fzb)) / W.dz[c]);
       a /= 1.0;
       val = a;
     } else {
       val = dtr;
       if (k == ks)
-        fzs[(size_t)n * G.ncol + col] = adv ? zface64<QUICK, ULT>(zb, tm2, tm1, t0, tp1) : 0.0;
+        fzs[(size_t)n * G.ncol + col] =
+            adv ? zface64<QUICK, ULT>(F, W, c, zm, zp, czb, wdb, tm2, tm1, t0, tp1) : 0.0;
     }
     tro[(size_t)n * G.S + c] = val;
   }
