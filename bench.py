@@ -192,7 +192,7 @@ def kernel_bytes(case, part, fp64):
     value read once and written once, plus its per-cell fields (advection:
     u1flux3d, u2flux3d, w, dz; column kernel: the four LU factors)."""
     s = 8 if fp64 else 4
-    return case.nwet * case.ntr * 2 * s + case.nwet * 4 * s
+    return case.cell_tracers() * 2 * s + case.nwet * 4 * s
 
 
 def time_arm(case, prec, local, args, pg, dev, clocks=None):
@@ -257,7 +257,8 @@ def main():
     if args.size:
         kw["nx"], kw["ny"] = (int(v) for v in args.size.split("x"))
     case = synth.make(args.workload, seed=2048 + rank, **kw)
-    units = case.nwet * case.ntr
+    units = case.cell_tracers()
+    host_gb = case.ntr * case.win.sgsiz * 8 / 1e9  # one FP64 copy of all tracers
 
     # the headline arm (timed with clocks sampled), then the plain FP64 arm on
     # the same inputs for the speed-up and the error of the mixed precision
@@ -267,18 +268,27 @@ def main():
     fp64 = None
     if mixed and not args.no_fp64:
         ref = time_arm(case, gpu.FP64, local, args, pg, dev)
-        t32, t64 = step.download(), ref["step"].download()
-        err = [float(np.max(np.abs(t32[n] - t64[n])) / max(float(np.max(np.abs(t64[n]))), 1e-300))
-               for n in range(case.ntr)]
+        err = [None]
+        if host_gb <= 16.0:  # the comparison holds both results on the host
+            t32, t64 = step.download(), ref["step"].download()
+            wet = case.win.wet_cells()
+            if case.ntr2d is None:
+                sel = [wet] * case.ntr
+            else:
+                nt = case.ntr2d[case.win.m2d[wet]]
+                sel = [wet[nt > n] for n in range(case.ntr)]
+            err = [float(np.max(np.abs(t32[n, c] - t64[n, c])) /
+                         max(float(np.max(np.abs(t64[n, c]))), 1e-300))
+                   for n, c in enumerate(sel) if len(c)]
+            del t32, t64
         fp64 = {"value": units * world / (ref["ms_step"] / 1000.0),
                 "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
                 "kernels_ms": {"k_adv64": ref["parts"][1], "k_vd64": ref["parts"][2]},
                 "mass_rel_drift": ref["mass_drift"],
                 "speedup_fp32mixed": ref["ms_step"] / arm["ms_step"],
-                "max_rel_err_fp32mixed": max(err),
+                "max_rel_err_fp32mixed": max(err) if err[0] is not None else None,
                 "steps_compared": arm["nsteps"]}
         ref["step"].close()
-        del t32, t64
 
     value = units * world / (arm["ms_step"] / 1000.0)
     hbm, peak_kind = peaks()
@@ -304,12 +314,12 @@ def main():
 
     # end to end through the drop-in C-ABI call on pinned host buffers
     S = case.win.sgsiz
-    pin = torch.empty((case.ntr, S), dtype=torch.float64, pin_memory=True)
-    tr_host = pin.numpy()
-    tr_host[:] = case.tr
-    sur, nsur = case.sur_t.copy(), case.nsur_t.copy()
     e2e_s = float("nan")
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and host_gb <= 16.0:
+        pin = torch.empty((case.ntr, S), dtype=torch.float64, pin_memory=True)
+        tr_host = pin.numpy()
+        tr_host[:] = case.tr
+        sur, nsur = case.sur_t.copy(), case.nsur_t.copy()
         step.step(tr_host, sur, nsur)  # warm: the drop-in call re-uploads everything
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -335,6 +345,8 @@ def main():
         "config": {
             "workload": args.workload + ("@" + args.size if args.size else ""), "nx": case.win.nx, "ny": case.win.ny,
             "nz": case.win.nz, "tracers": case.ntr, "wet_cells": case.nwet,
+            "cell_tracers": units,
+            "basins": [list(b) for b in getattr(case, "basins", [])] or None,
             "columns": case.win.ncol, "precision": args.precision, "dt": case.dt,
             "substeps": arm["diag"].nsub, "seed": case.seed,
             "l2": "inputs larger than L2 (%.1f GB of tracers and fields per step)" % (

@@ -64,6 +64,7 @@ class Opts(C.Structure):
         ("hmin", C.c_double),
         ("ntbdy", C.c_int), ("tbdy", IP), ("ntdif_v", C.c_int), ("tdif_v", IP),
         ("advect", IP), ("diffuse", IP), ("mintr", DP), ("maxtr", DP),
+        ("ntr2d", IP),
     ]
 
 

@@ -410,6 +410,7 @@ __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
     int stat = 0;
     for (int sl = 0; sl < T.nslot; ++sl) {
       int n = T.slot_tr[sl];
+      if (n >= G.colntr[col]) continue;  // not carried in this column
       column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S,
                         col, n, G.col_kb[col], true, sol, c3, warn, stat);
     }
@@ -459,6 +460,7 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
     const int top = G.col_top[col], bot = G.col_bot[col];
     int c = W.nsur_t[col];
     if (c == G.zm1[c]) continue;  // surface below the bottom: dry
+    if (n >= G.colntr[col]) continue;  // tracer not carried in this column
     const double area = G.cellarea[top];
     double tz = F.eta[top];
     for (int it = 0; it <= G.nz; ++it) {
@@ -623,6 +625,10 @@ int check_geom(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr) {
   if (g->v3_t != g->b3_t || g->b3_t != g->a3_t) return SHOC_TR_EUNSUPPORTED;  // OBC / aux cells
   if (g->v2_t != g->b2_t || g->b2_t != g->a2_t) return SHOC_TR_EUNSUPPORTED;
   if (g->nz < 1 || g->nz > kSerialMaxLayers) return SHOC_TR_EUNSUPPORTED;
+  if (o->ntr2d) {  // per-column tracer counts: the advected tracers in ascending order
+    for (int i = 1; i < o->ntbdy; i++)
+      if (o->tbdy[i] <= o->tbdy[i - 1]) return SHOC_TR_EARG;
+  }
   if (g->sgsiz < 2 || g->sgsizS < 2 || g->b2_t < 1) return SHOC_TR_EGEOM;
   const int S = g->sgsiz;
   std::vector<uint8_t> wet(S, 0);
@@ -795,6 +801,13 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload(h, &ip, col_bot.data(), ncol)); G.col_bot = ip;
   TRY(dupload(h, &ip, col_kb.data(), ncol)); G.col_kb = ip;
   TRY(dupload(h, &ip, g->s2k, S)); G.kof = ip;
+  {
+    std::vector<int> colntr(ncol, ntr);
+    if (o->ntr2d)
+      for (int col = 0; col < ncol; col++)
+        colntr[col] = std::max(0, std::min(ntr, o->ntr2d[col_top[col]]));
+    TRY(dupload(h, &ip, colntr.data(), ncol)); G.colntr = ip;
+  }
   double *dp;
   TRY(dupload(h, &dp, g->h1au1, S2)); G.h1au1 = dp;
   TRY(dupload(h, &dp, g->h2au2, S2)); G.h2au2 = dp;
@@ -1075,11 +1088,13 @@ int tile64_substep(const shoc_tr_gpu *h, bool last, const SubStep &ss, const Til
     if (nt <= 0) continue;
     const size_t smem = vd64_smem(h->nz - kbase, nw);
     if (last)
-      k_vd64<true><<<nt * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tl, tin,
-                                                   tout, h->fzs64, nw, nchunk, t0, kbase);
+      k_vd64<true><<<nt * nchunk, blk, smem, st>>>(
+          h->G, h->F, h->W, h->O, h->T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
+          h->W.vd_div, h->W.vd_ud, nw, nchunk, t0, kbase);
     else
-      k_vd64<false><<<nt * nchunk, blk, smem, st>>>(h->G, h->F, h->W, h->O, h->T, ss, tl, tin,
-                                                    tout, h->fzs64, nw, nchunk, t0, kbase);
+      k_vd64<false><<<nt * nchunk, blk, smem, st>>>(
+          h->G, h->F, h->W, h->O, h->T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
+          h->W.vd_div, h->W.vd_ud, nw, nchunk, t0, kbase);
     nl++;
   }
   if (ev) cudaEventRecord(ev[2], st);

@@ -67,6 +67,7 @@ struct Geo {
   const int *col_top, *col_bot;  // surface-layer and bottom cell per column
   const int *col_kb;             // layer index of the bottom cell per column
   const int *kof;                // layer index of every cell (s2k)
+  const int *colntr;             // tracers updated per column (numbers below it)
   const double *h1au1, *h2au2, *h1au2, *h2au1, *h1acell, *h2acell, *cellarea, *botz;
   const double *gridz;
   const Face2D *fx, *fy;         // [S2]

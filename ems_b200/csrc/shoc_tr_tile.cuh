@@ -167,8 +167,8 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
   }
   __syncthreads();
 
-  // this thread's cell and its column
-  int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0;
+  // this thread's cell and its column (ntc: tracers carried by the column)
+  int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0, ntc = 0;
   if (i < Tl.nwet) {
     c = Tl.wet[i];
     col = Tl.colof[c];
@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
       kb = tc.kb;
       ks = tc.ks;
       c2 = tc.c2;
+      ntc = G.colntr[col];
     } else {
       c = 0;
     }
@@ -268,6 +269,8 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
     const int idx[13] = {c,    n1.z, n2.z, n1.w, n2.w, vm1, vm2,
                          vp1,  vp2,  n1.x, n2.x, n1.y, n2.y};
     for (int s0 = 0; s0 < ntb; s0 += U) {
+      // tracers are ascending when columns carry different numbers of them
+      if (!__any_sync(FULL, on && sTr[s0] < ntc)) continue;
       float v[U][13];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -290,8 +293,8 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
         const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
         const float Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
         const float Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
-        if (!on) continue;
         const int n = sTr[s];
+        if (!on || n >= ntc) continue;
         // FP64 flux divergence (tracers.c:888-892)
         const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
         float val;
@@ -359,7 +362,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
         }
       }
       const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
-      if (!on) continue;
+      if (!on || nn[u] >= ntc) continue;
       if (sxp1) Fxe = Fnext;
       // FP64 flux divergence (tracers.c:888-892)
       const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
@@ -430,6 +433,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   if (!act || slot >= T.nslot) return;
 
   const int n = T.slot_tr[slot];
+  if (n >= G.colntr[col]) return;  // tracer not carried in this column
   const int tf = T.trf[n];
   const bool tbdy = (tf & TR_TBDY) != 0;
   const bool adv = tbdy && (tf & TR_ADV);

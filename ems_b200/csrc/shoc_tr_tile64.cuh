@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv64(Geo G, Flow F, Work W, T
   }
   __syncthreads();
 
-  int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0;
+  int c = 0, col = 0, kb = nz, ks = 0, k = 0, c2 = 0, ntc = 0;
   if (i < Tl.nwet) {
     c = Tl.wet[i];
     col = Tl.colof[c];
@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv64(Geo G, Flow F, Work W, T
       kb = tc.kb;
       ks = tc.ks;
       c2 = tc.c2;
+      ntc = G.colntr[col];
     } else {
       c = 0;
     }
@@ -170,6 +171,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv64(Geo G, Flow F, Work W, T
   for (int s = 0; s < ntb; ++s) {
     const int n = sTr[s];
     const int tf = sTf[s];
+    if (!__any_sync(FULL, on && n < ntc)) continue;  // no lane carries it
     const bool adv = MODE != 0 || (tf & TR_ADV);
     const bool hd = MODE == 2 || (MODE == 0 && (tf & TR_HDIFF));
     const double *__restrict__ tr = tri + (size_t)n * G.S;
@@ -196,7 +198,7 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv64(Geo G, Flow F, Work W, T
                                   h ? Px(xp, me.x) : 0.0, G.h1au1[me.x], txm1, t0, txp1, txp2);
     }
     const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
-    if (!on) continue;
+    if (!on || n >= ntc) continue;
     if (sxp1) Fxe = Fnext;
     // dtracer (tracers.c:888-892)
     const double dtr = (Fxe - Fxw + Fyn - Fys) * dtu;
@@ -229,7 +231,11 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
                                               SubStep ss, Tile Tl,
                                               const double *__restrict__ tri,
                                               double *__restrict__ tro,
-                                              const double *__restrict__ fzs, int nw,
+                                              const double *__restrict__ fzs,
+                                              const double *__restrict__ vdzdt,
+                                              const double *__restrict__ vcm1,
+                                              const double *__restrict__ vdiv,
+                                              const double *__restrict__ vud, int nw,
                                               int nchunk, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int nz = G.nz, nd = nz - kbase;
@@ -258,6 +264,7 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
   if (!act || slot >= T.nslot) return;
 
   const int n = T.slot_tr[slot];
+  if (n >= G.colntr[col]) return;  // tracer not carried in this column
   const int tf = T.trf[n];
   const bool tbdy = (tf & TR_TBDY) != 0;
   const bool adv = tbdy && (tf & TR_ADV);
@@ -296,16 +303,17 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
       const double v = A0[nk * sa];
       to[cs] = v + F.dt * (0.0 - 0.0) / h;
     } else if (solve) {
+#pragma unroll 4
       for (int j = 0; j <= nk; ++j) {
         const int cc = C0[j * 32];
-        double rhs = W.vd_dzdt[cc] * A0[j * sa];
+        double rhs = __ldg(&vdzdt[cc]) * A0[j * sa];
         double sl;
         if (j == 0) {
           rhs = rhs + 0.0;
-          sl = rhs / W.vd_div[cc];
+          sl = rhs / __ldg(&vdiv[cc]);
         } else {
           if (j == nk) rhs = rhs - 0.0;
-          sl = (rhs - W.vd_cm1[cc] * solp) / W.vd_div[cc];
+          sl = (rhs - __ldg(&vcm1[cc]) * solp) / __ldg(&vdiv[cc]);
         }
         S0[j * sa] = sl;
         solp = sl;
@@ -313,6 +321,7 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
     }
   } else {
     double a_below = 0.0;
+#pragma unroll 4
     for (int j = 0; j < nk; ++j) {
       const int cc = C0[j * 32];
       double a = A0[j * sa];
@@ -322,13 +331,13 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
       if (a < mn || a > mx) nwarn++;
       if (solve) {
         A0[j * sa] = a;
-        double rhs = W.vd_dzdt[cc] * a;
+        double rhs = __ldg(&vdzdt[cc]) * a;
         double sl;
         if (j == 0) {
           rhs = rhs + 0.0;
-          sl = rhs / W.vd_div[cc];
+          sl = rhs / __ldg(&vdiv[cc]);
         } else {
-          sl = (rhs - W.vd_cm1[cc] * solp) / W.vd_div[cc];
+          sl = (rhs - __ldg(&vcm1[cc]) * solp) / __ldg(&vdiv[cc]);
         }
         S0[j * sa] = sl;
         solp = sl;
@@ -367,14 +376,14 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
       to[cs] = vs + F.dt * (0.0 - 0.0) / h;
     } else if (solve) {
       A0[nk * sa] = vs;
-      double rhs = W.vd_dzdt[cs] * vs;
+      double rhs = __ldg(&vdzdt[cs]) * vs;
       double sl;
       if (nk == 0) {
         rhs = rhs + 0.0;
-        sl = rhs / W.vd_div[cs];
+        sl = rhs / __ldg(&vdiv[cs]);
       } else {
         rhs = rhs - 0.0;
-        sl = (rhs - W.vd_cm1[cs] * solp) / W.vd_div[cs];
+        sl = (rhs - __ldg(&vcm1[cs]) * solp) / __ldg(&vdiv[cs]);
       }
       S0[nk * sa] = sl;
     }
@@ -386,7 +395,8 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
     double fin = a + (x - a) * 1.0;
     to[cs] = fin;
     if (isnan(fin)) stat |= ST_NAN;
-    double udp = W.vd_ud[cs];
+    double udp = __ldg(&vud[cs]);
+#pragma unroll 4
     for (int j = nk - 1; j >= 0; --j) {
       const int cc = C0[j * 32];
       x = S0[j * sa] - udp * x;
@@ -394,7 +404,7 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
       fin = a + (x - a) * 1.0;
       to[cc] = fin;
       if (isnan(fin)) stat |= ST_NAN;
-      udp = W.vd_ud[cc];
+      udp = __ldg(&vud[cc]);
     }
   }
   if (nwarn) atomicAdd(W.nwarn, nwarn);

@@ -251,6 +251,8 @@ class Case:
         self.u1kh = np.zeros(S) if u1kh is None else u1kh
         self.u2kh = np.zeros(S) if u2kh is None else u2kh
         self.diffuse = np.zeros(ntr, np.int32) if diffuse is None else np.asarray(diffuse, np.int32)
+        # tracers per water column (None: all); see shoc_tr_opts.ntr2d
+        self.ntr2d = None
         self.sur_t, self.nsur_t = win.init_surface(oldeta)
 
     @property
@@ -273,7 +275,7 @@ class Case:
         return _abi.Opts(self.trasc, self.ultimate, self.stab, self.hmin,
                          self.ntr, iptr(a["tbdy"]), self.ntr, iptr(a["tdif_v"]),
                          iptr(a["advect"]), iptr(a["diffuse"]), dptr(a["mintr"]),
-                         dptr(a["maxtr"]))
+                         dptr(a["maxtr"]), iptr(self.ntr2d))
 
     def make_state(self, tr, sur_t, nsur_t, keep):
         """shoc_tr_state over caller-owned arrays (tr: (ntr, sgsiz) float64)."""
@@ -286,12 +288,19 @@ class Case:
                           dptr(self.u1kh), dptr(self.u2kh), dptr(self.eta), dptr(self.oldeta),
                           self.dt)
 
+    def cell_tracers(self):
+        """Tracer values a step updates: wet cells x tracers, or with per-
+        column tracer counts (ntr2d) the sum of each wet cell's count."""
+        if self.ntr2d is None:
+            return self.nwet * self.ntr
+        return int(self.ntr2d[self.win.m2d[self.win.wet_cells()]].sum())
+
     def bytes_per_step(self, fp64=True):
         """Algorithmic HBM bytes of one step: one read + one write of every
         tracer value and one read of five per-cell fields (u1flux3d, u2flux3d,
         w, Kz, dz) per wet cell."""
         s = 8 if fp64 else 4
-        return self.nwet * self.ntr * 2 * s + self.nwet * 5 * s
+        return self.cell_tracers() * 2 * s + self.nwet * 5 * s
 
 
 def _coast_taper(land, width):
@@ -321,18 +330,21 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
                land_frac=0.0, cell=(1000.0, 1000.0), curvilinear=False, umax=0.5,
                baroclinic=0.2, kz=("exp", 1e-2, 1e-5), tracers="gauss", nsteps=1,
                trasc=_abi.QUICKEST, ultimate=1, stab=_abi.SUB_STEP, hmin=0.07,
-               mintr=None, maxtr=None, eta_offset=None, hdiff=None):
+               mintr=None, maxtr=None, eta_offset=None, hdiff=None, bathy_land=None):
     rng = np.random.default_rng(seed)
     layers = np.asarray(layers, np.float64)
     nz = len(layers) - 1
-    f = _smooth(rng, ny, nx)
-    bathy = -(depth[0] + (depth[1] - depth[0]) * f)
-    bathy = np.maximum(bathy, layers[0])
-    bathy = _snap_bathy(bathy, layers)
-    land = np.zeros((ny, nx), np.uint8)
-    if land_frac > 0:
-        g = _smooth(rng, ny, nx, nmodes=10, kmax=6.0)
-        land = (g < np.quantile(g, land_frac)).astype(np.uint8)
+    if bathy_land is None:
+        f = _smooth(rng, ny, nx)
+        bathy = -(depth[0] + (depth[1] - depth[0]) * f)
+        bathy = np.maximum(bathy, layers[0])
+        bathy = _snap_bathy(bathy, layers)
+        land = np.zeros((ny, nx), np.uint8)
+        if land_frac > 0:
+            g = _smooth(rng, ny, nx, nmodes=10, kmax=6.0)
+            land = (g < np.quantile(g, land_frac)).astype(np.uint8)
+    else:
+        bathy, land = bathy_land
     if curvilinear:
         h1c = cell[0] + (cell[1] - cell[0]) * _smooth(rng, ny, nx, nmodes=6, kmax=2.0)
         h2c = cell[0] + (cell[1] - cell[0]) * _smooth(rng, ny, nx, nmodes=6, kmax=2.0)
@@ -408,6 +420,58 @@ def build_case(name, nx, ny, layers, *, seed, ntr, dt=60.0, depth=(10.0, 50.0),
                 u1kh=u1kh, u2kh=u2kh, diffuse=diffuse)
 
 
+# Uneven batch of independent basins (horizontal size, layers, tracers): the
+# sizes, layer counts and tracer counts of the multi-basin configuration.
+BATCH8 = ((128, 128, 20, 4), (256, 256, 26, 8), (384, 256, 31, 12), (512, 512, 37, 16),
+          (768, 512, 43, 20), (1024, 1024, 49, 24), (1536, 768, 54, 28),
+          (2048, 1024, 60, 32))
+
+
+def build_batch(name, basins, *, seed, scale=1.0, gap=3, nz=60, depth=250.0, **kw):
+    """One window holding independent basins side by side, separated by
+    `gap` land columns, each with its own seeded bathymetry (its own deepest
+    layer count and 30 % land) and tracer count (shoc_tr_opts.ntr2d).  The
+    streamfunction vanishes at every coast, so no water or tracer crosses
+    between basins and each steps as it would alone."""
+    rng = np.random.default_rng(seed)
+    layers = uniform_layers(nz, depth)
+    dims = [(max(8, int(round(bx * scale))), max(8, int(round(by * scale))), L, T)
+            for bx, by, L, T in basins]
+    nx = sum(d[0] for d in dims) + gap * (len(dims) + 1)
+    ny = max(d[1] for d in dims) + 2 * gap
+    bathy = np.full((ny, nx), layers[-2])
+    land = np.ones((ny, nx), np.uint8)
+    tr_of = np.zeros((ny, nx), np.int32)
+    x0 = gap
+    for bx, by, L, T in dims:
+        f = _smooth(rng, by, bx)
+        dmax = depth * L / nz
+        b = -(2.0 + (dmax - 2.0) * f)
+        b = np.maximum(b, layers[0])
+        g = _smooth(rng, by, bx, nmodes=10, kmax=6.0)
+        ld = (g < np.quantile(g, 0.3)).astype(np.uint8)
+        bathy[gap:gap + by, x0:x0 + bx] = _snap_bathy(b, layers)
+        land[gap:gap + by, x0:x0 + bx] = ld
+        tr_of[gap:gap + by, x0:x0 + bx] = T
+        x0 += bx + gap
+    ntr = max(d[3] for d in dims)
+    d = dict(layers=layers, seed=seed, ntr=ntr, cell=(150.0, 150.0), umax=1.5,
+             kz=("logu", 1e-6, 1e-1), tracers=("logn", 1.0, 1.0), nsteps=500)
+    d.update(kw)
+    case = build_case(name, nx, ny, bathy_land=(bathy, land), **d)
+    # tracers carried per water column: the basin's count
+    win = case.win
+    c2 = np.arange(1, win.sgsizS)
+    ntr2d = np.zeros(win.sgsizS, np.int32)
+    ok = c2 < len(win.s2i)
+    i, j = win.s2i[c2[ok]], win.s2j[c2[ok]]
+    inb = (i >= 0) & (i < nx) & (j >= 0) & (j < ny)
+    ntr2d[c2[ok][inb]] = tr_of[j[inb], i[inb]]
+    case.ntr2d = ntr2d
+    case.basins = dims
+    return case
+
+
 def uniform_layers(nz, depth):
     return np.linspace(-depth, 0.0, nz + 1)
 
@@ -418,7 +482,7 @@ def stiff_layers(nz, depth, nthin=10, thin=0.5):
     return np.concatenate([rest[:-1], top])
 
 
-WORKLOADS = ("small", "basin64", "drop512", "batch2048", "stiff2048")
+WORKLOADS = ("small", "basin64", "drop512", "batch2048", "stiff2048", "batch8", "batch8small")
 
 
 def make(name, seed=None, **kw):
@@ -439,6 +503,10 @@ def make(name, seed=None, **kw):
         d = dict(nx=2048, ny=1024, layers=uniform_layers(50, 250.0), seed=2048, ntr=24,
                  depth=(2.0, 250.0), land_frac=0.35, cell=(200.0, 2000.0), curvilinear=True,
                  umax=1.0, kz=("logu", 1e-6, 1e-1), tracers=("logn", 1e-3, 1e2), nsteps=1000)
+    elif name in ("batch8", "batch8small"):
+        kw = dict(kw)
+        sc = kw.pop("scale", 1.0 if name == "batch8" else 1.0 / 16)
+        return build_batch(name, BATCH8, seed=2048 if seed is None else seed, scale=sc, **kw)
     elif name == "stiff2048":
         d = dict(nx=2048, ny=1024, layers=stiff_layers(50, 250.0), seed=2048, ntr=24,
                  depth=(2.0, 250.0), land_frac=0.35, cell=(200.0, 2000.0), curvilinear=True,

@@ -114,6 +114,14 @@ typedef struct shoc_tr_opts {
   const int *advect;              /* [ntr] per-tracer advect flag */
   const int *diffuse;             /* [ntr] per-tracer horizontal diffusion flag */
   const double *mintr, *maxtr;    /* [ntr] valid range */
+  /* Optional (NULL: every tracer in every column).  Per 2D cell (SHOC 2D
+   * index, [sgsizS]): the number of leading tracers, tracer numbers
+   * 0..ntr2d[c2]-1, that the step updates in that water column; the others
+   * keep their values.  No reference counterpart: it lets one window hold
+   * several independent basins that carry different numbers of tracers, so
+   * that they step in one launch (the tbdy list must be ascending when it is
+   * given). */
+  const int *ntr2d;
 } shoc_tr_opts;
 
 /* What one step reports besides the status code. */

@@ -51,3 +51,23 @@ def test_workload_sizes():
     case = synth.make("basin64")
     assert case.win.nx == 64 and case.win.nz == 20 and case.ntr == 1
     assert case.win.ncol == 64 * 64  # no land
+
+
+def test_batch_window_basins_and_tracer_counts():
+    """batch8small: eight basins side by side; every wet column carries its
+    basin's tracer count (4, 8, ... 32) and no basin touches another."""
+    import numpy as np
+    from ems_b200 import synth
+    case = synth.make("batch8small")
+    w = case.win.wet_cells()
+    cols = np.unique(case.win.m2d[w])
+    counts = sorted(set(case.ntr2d[cols].tolist()))
+    assert counts == [4, 8, 12, 16, 20, 24, 28, 32]
+    # no wet column's x-neighbour column belongs to another basin
+    i = case.win.s2i[w]
+    nt = case.ntr2d[case.win.m2d[w]]
+    xp = case.win.xp1[w]
+    wet = np.zeros(case.win.sgsiz, bool)
+    wet[w] = True
+    nb = xp[wet[xp]]
+    assert np.all(case.ntr2d[case.win.m2d[nb]] == nt[wet[xp]])
