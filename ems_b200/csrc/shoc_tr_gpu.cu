@@ -172,83 +172,81 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
   atomicMin(p, (unsigned long long)__double_as_longlong(v));
 }
 
-// One thread per column.
-// list_all: put every column the staged kernels do not handle on the
+// One thread per column: the surface cells, set_dz (tracers.c:5731-5848), the
+// scheme work arrays w5/w9 (:561-567) and their 2/(w9+w9) factors, the
+// sub-step search (:591-668) as a min-reduction, the column flags and the
+// tracer-independent LU factors of vert_diffuse_3d / implicit_vdiff_tr
+// (:3841-3889, :4185-4195).  The column's cells come from the layer-by-column
+// table in one batch of independent loads (cl[j]: j = 0 the sediment cell,
+// j = 1..nk the wet layers from the bottom up) and its thicknesses and w9 are
+// kept in local arrays, so the walks below index layers instead of chasing
+// zm1 / zp1; every walk visits the cells the reference's walk visits, in the
+// same order, with the same arithmetic.
+// list_all: put every column the tile kernels do not handle on the
 // general-path list (else only the tracer-coupled thin-surface columns).
 // fp32: also write the FP32 thickness and LU factors.
-__global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *counts, int list_all,
-                         int fp32) {
+__global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Tile Tl,
+                                                int any_vdiff, int *counts, int list_all,
+                                                int fp32) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   double dtmin = __longlong_as_double(0x7ff0000000000000ll);
   if (col < G.ncol) {
-    const int *zm1 = G.zm1, *zp1 = G.zp1;
-    const int top = G.col_top[col], bot = G.col_bot[col];
-    // new and old surface cells (tracers.c:5739-5755)
-    const int lim = G.nz + 2;  // every column walk is bounded by the layer count
+    const int top = G.col_top[col], bot = G.col_bot[col], kb = G.col_kb[col];
+    const int nk = G.nz - kb;  // wet layers of the column
+    int cl[kSerialMaxLayers + 1];
+    double dzl[kSerialMaxLayers + 1], w9l[kSerialMaxLayers + 1];
+    cl[0] = G.zm1[bot];  // the sediment cell
+    for (int j = 1; j <= nk; ++j) cl[j] = Tl.cellk[(size_t)(kb + j - 1) * Tl.ncolp + col];
+    // layer position of a cell of this column (0: the sediment)
+    auto jof = [&](int c) { return c == cl[0] ? 0 : G.kof[c] - kb + 1; };
+
+    // new and old surface cells (tracers.c:5739-5755): down from the top
+    // while the cell's bottom is at or above eta, at most to the sediment
     int sur = W.nsur_t[col];
-    int c = top, m = zm1[c];
-    for (int it = 0; c != m && G.gridz[c] >= F.eta[top] && it < lim; ++it) {
-      c = m;
-      m = zm1[c];
-    }
-    int nsur = c;
+    int jn = nk;
+    const double etat = F.eta[top];
+    while (jn > 0 && G.gridz[cl[jn]] >= etat) --jn;
+    int nsur = cl[jn];
     W.sur_t[col] = sur;
     W.nsur_t[col] = nsur;
-    // cells-to-process membership (:5778-5800)
+    const int js0 = jof(sur);
+    // cells-to-process membership (:5778-5800): s is the lower of the two
     int s = sur > nsur ? sur : nsur;
+    const int js = js0 < jn ? js0 : jn;
     int c2 = G.m2d[s];
     double tz = F.eta[c2] < F.oldeta[c2] ? F.eta[c2] : F.oldeta[c2];
     double bz = SHOC_TR_DRY_FRAC * O.hmin + G.botz[c2];
-    bool wet = (tz > bz && s != zm1[s]);
-    // thicknesses (:5824-5846)
+    bool wet = (tz > bz && js > 0);
+    // thicknesses (:5824-5846): from the old surface down, then copied up
     {
-      int cc = sur, c3 = cc;
-      int t2 = G.m2d[c3];
+      dzl[0] = W.dz[cl[0]];
+      int t2 = G.m2d[sur];
       double tp = F.oldeta[t2];
-      int it = 0;
-      for (; c3 < bot && it < lim; ++it) {
-        double b = G.gridz[c3];
-        W.dz[c3] = tp - b;
+      for (int j = js0; j > 1; --j) {
+        double b = G.gridz[cl[j]];
+        dzl[j] = tp - b;
         tp = b;
-        c3 = zm1[c3];
       }
-      W.dz[bot] = tp - G.botz[t2];
-      c3 = cc;
-      for (int j = 0; cc > t2 && j < lim; ++j) {
-        cc = zp1[cc];
-        W.dz[cc] = W.dz[c3];
-      }
-      if (it >= lim) atomicOr(W.status, ST_GEOM);
-      if (fp32) {
-        int q = top;
-        for (int j = 0; j < lim; ++j) {
-          W.dz32[q] = (float)W.dz[q];
-          if (q == bot) break;
-          q = zm1[q];
-        }
-      }
+      dzl[1] = tp - G.botz[t2];
+      for (int j = js0 + 1; j <= nk; ++j) dzl[j] = dzl[js0];
+      for (int j = 1; j <= nk; ++j) W.dz[cl[j]] = dzl[j];
+      if (fp32)
+        for (int j = 1; j <= nk; ++j) W.dz32[cl[j]] = (float)dzl[j];
     }
     // scheme work arrays over every cell of the column (:530-567)
-    {
-      int cc = top;
-      for (int it = 0; it < lim; ++it) {
-        int zm = zm1[cc];
-        double dzm = W.dz[zm], dzc = W.dz[cc];
-        if (O.trasc == SHOC_TR_QUICKEST) W.w5[cc] = dzm / (dzm + dzc);
-        W.w9[cc] = 0.5 * (dzc + dzm);
-        if (cc == bot) break;
-        cc = zm;
-      }
-      cc = top;
-      for (int it = 0; it < lim; ++it) {
-        int zm = zm1[cc], zp = zp1[cc];
-        double w9c = W.w9[cc];
-        double w9m = (cc == bot) ? 0.0 : W.w9[zm];
-        W.dbz[cc] = 2.0 / (w9m + w9c);
-        W.dfz[cc] = 2.0 / (w9c + W.w9[zp]);
-        if (cc == bot) break;
-        cc = zm;
-      }
+    for (int j = nk; j >= 1; --j) {
+      const int cc = cl[j];
+      double dzm = dzl[j - 1], dzc = dzl[j];
+      if (O.trasc == SHOC_TR_QUICKEST) W.w5[cc] = dzm / (dzm + dzc);
+      w9l[j] = 0.5 * (dzc + dzm);
+      W.w9[cc] = w9l[j];
+    }
+    for (int j = nk; j >= 1; --j) {
+      const int cc = cl[j];
+      double w9c = w9l[j];
+      double w9m = (j == 1) ? 0.0 : w9l[j - 1];
+      W.dbz[cc] = 2.0 / (w9m + w9c);
+      W.dfz[cc] = 2.0 / (w9c + w9l[j < nk ? j + 1 : nk]);
     }
     int flags = 0;
     int cbs = 0;
@@ -257,12 +255,12 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
       atomicAdd(&counts[0], 1);
       // sub-step search over this column's cells to process (:591-661)
       int nc = 0;
-      int cc = s;
       bool first = true;
-      for (int it = 0; it < lim; ++it) {
+      for (int j = js; j >= 1; --j) {
+        const int cc = cl[j];
         nc++;
         if (O.substep) {
-          int xp = G.xp1[cc], yp = G.yp1[cc], zp = zp1[cc];
+          int xp = G.xp1[cc], yp = G.yp1[cc], zp = cl[j < nk ? j + 1 : nk];
           double d4 = 0.5 * (F.u1[cc] + F.u1[xp]);
           if (fabs(d4) < kMinVal) d4 = kMinVal;
           double d1 = kSF * fabs(G.h1acell[c2] / d4);
@@ -274,44 +272,38 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
           if (!first) {
             d4 = 0.5 * (F.w[cc] + F.w[zp]);
             if (fabs(d4) < kMinVal) d4 = kMinVal;
-            double d3 = kSF * fabs(W.dz[cc] * 1.0 / d4);
+            double d3 = kSF * fabs(dzl[j] * 1.0 / d4);
             if (d3 > 0.0 && d3 < dtmin) dtmin = d3;
           }
         }
         first = false;
-        int nx = zm1[cc];
-        if (nx == zm1[nx]) break;  // next is the sediment cell
-        cc = nx;
       }
       atomicAdd(&counts[1], nc);
       // tr_bounds thin-surface test (:3250-3252)
-      if (s < bot && W.dz[sur] < O.hmin) {
+      if (js > 1 && dzl[js0] < O.hmin) {
         flags |= COL_THIN;
         if (s != top) flags |= COL_SERIAL;
       }
       // implicit vertical diffusion set-up (:3841-3889) and LU (:4185-4195)
       int cs = nsur;
-      int zm = zm1[cs];
-      if (zm == zm1[zm] || !W.dz[zm]) {
+      if (jn <= 1 || !dzl[jn - 1]) {
         flags |= COL_SINGLE;
-      } else if (any_vdiff && !W.dz[cs]) {
+      } else if (any_vdiff && !dzl[jn]) {
         // zero-thickness surface cell: the reference solves over an empty
         // range and reads stale work memory; report instead of guessing
         flags |= COL_NOSOLVE;
         atomicOr(W.status, ST_GEOM);
       } else if (any_vdiff) {
-        int ca = cs, za = zm;
-        for (int it = 0; ca != za && W.dz[ca] && it < lim; ++it) {
-          ca = za;
-          za = zm1[ca];
-        }
-        cbs = zp1[ca];
+        int ja = jn;
+        while (ja > 0 && dzl[ja]) --ja;
+        const int jb = ja + 1;  // bottom of the solve
+        cbs = cl[jb];
         // dzface(c) = 0.5 (dz[zm1] + dz[c]) for c in [cbs, cs]
         double dt = F.dt;
         int cb = cbs;
-        int zpb = zp1[cb];
-        double dzf_p = 0.5 * (W.dz[cb] + W.dz[zpb]);
-        double dzdt = W.dz[cb] / dt;
+        int zpb = cl[jb + 1];
+        double dzf_p = 0.5 * (dzl[jb] + dzl[jb + 1]);
+        double dzdt = dzl[jb] / dt;
         double cp1 = -F.Kz[zpb] / dzf_p;
         double C = dzdt - cp1;
         double div = C;
@@ -321,12 +313,11 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
         W.vd_dzdt[cb] = dzdt;
         if (fp32) W.lu32[cb] = make_float4((float)dzdt, 0.f, (float)(1.0 / div), 0.f);
         double bp1 = cp1;
-        int cc2 = zpb;
-        for (int it = 0; cc2 != cs && it < lim; ++it) {
-          int zp = zp1[cc2];
+        for (int j = jb + 1; j < jn; ++j) {
+          const int cc2 = cl[j], zp = cl[j + 1];
           double dzf_c = dzf_p;
-          dzf_p = 0.5 * (W.dz[cc2] + W.dz[zp]);
-          dzdt = W.dz[cc2] / dt;
+          dzf_p = 0.5 * (dzl[j] + dzl[j + 1]);
+          dzdt = dzl[j] / dt;
           double cm1 = -F.Kz[cc2] / dzf_c;
           cp1 = -F.Kz[zp] / dzf_p;
           C = dzdt - cm1 - cp1;
@@ -340,11 +331,10 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
           if (fp32)
             W.lu32[cc2] = make_float4((float)dzdt, (float)cm1, (float)(1.0 / div), (float)ud);
           bp1 = cp1;
-          cc2 = zp;
         }
         {
           double dzf_c = dzf_p;
-          dzdt = W.dz[cs] / dt;
+          dzdt = dzl[jn] / dt;
           double cm1 = -F.Kz[cs] / dzf_c;
           C = dzdt - cm1;
           double ud = bp1 / div;
@@ -367,7 +357,7 @@ __global__ void k_set_dz(Geo G, Flow F, Work W, Opt O, int any_vdiff, int *count
     ci.cs = nsur;
     ci.cbs = cbs;
     ci.flags = flags;
-    ci.ks = G.kof[s];
+    ci.ks = kb + js - 1;
     if (staged_column(ci, bot)) ci.flags |= COL_STAGED;
     W.col[col] = ci;
     if ((flags & COL_SERIAL) || (list_all && !(ci.flags & COL_STAGED))) {
@@ -1037,7 +1027,7 @@ int launch_part_a(shoc_tr_gpu *h) {
     h->launches++;
   }
   int nb = (h->ncol + 127) / 128;
-  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->any_vdiff ? 1 : 0, h->d_counts,
+  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->tl, h->any_vdiff ? 1 : 0, h->d_counts,
                                h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0);
   h->launches++;
   CK(cudaGetLastError());
