@@ -8,15 +8,16 @@ namespace shoc {
 
 namespace {
 template <class K>
-cudaError_t attr(K k) {
-  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+cudaError_t attr(K k, int bytes = 227 * 1024) {
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <bool Q, bool U, int M>
 void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
          const float *tin, float *tout, float *fzs, int hd) {
-  k_adv32<Q, U, M><<<grid, kAdvBlock, 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+  k_adv32<Q, U, M><<<grid, kAdvBlock, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
+                                                                  tin, tout, fzs, hd);
 }
 template <bool Q, bool U>
 void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F3,
@@ -34,7 +35,13 @@ void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F
 
 cudaError_t tile32_set_smem_attr() {
   cudaError_t e = cudaSuccess;
-  const cudaError_t r[2] = {attr(k_vd32<true>), attr(k_vd32<false>)};
+  const int a = (int)kAdvSmem;
+  const cudaError_t r[10] = {
+      attr(k_vd32<true>),              attr(k_vd32<false>),
+      attr(k_adv32<true, true, 1>, a), attr(k_adv32<true, true, 2>, a),
+      attr(k_adv32<true, false, 1>, a), attr(k_adv32<true, false, 2>, a),
+      attr(k_adv32<false, true, 1>, a), attr(k_adv32<false, true, 2>, a),
+      attr(k_adv32<false, false, 1>, a), attr(k_adv32<false, false, 2>, a)};
   for (auto x : r)
     if (x != cudaSuccess) e = x;
   return e;

@@ -142,6 +142,9 @@ __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2,
 
 constexpr int kAdvBlock = 256;
 constexpr int kAdvGroup = 2;       // tracers whose loads a thread issues together
+// dynamic shared memory of k_adv32 with uniform flags: the double-buffered
+// stencil values of a group of tracers per thread
+constexpr size_t kAdvSmem = (size_t)2 * kAdvGroup * 13 * kAdvBlock * sizeof(float);
 constexpr int kMaxTracers = 256;   // tracers a handle of the FP32-mixed path may carry
 
 // MODE: 0 tracers with their own advect / diffuse flags, 1 every advected
@@ -266,27 +269,46 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
     // and neighbours a cell does not use, read valid cells) and the face
     // code has no per-tracer branches
     constexpr bool HD = MODE == 2;
-    const int idx[13] = {c,    n1.z, n2.z, n1.w, n2.w, vm1, vm2,
+    constexpr int NQ = 13;
+    const int idx[NQ] = {c,    n1.z, n2.z, n1.w, n2.w, vm1, vm2,
                          vp1,  vp2,  n1.x, n2.x, n1.y, n2.y};
-    for (int s0 = 0; s0 < ntb; s0 += U) {
-      // tracers are ascending when columns carry different numbers of them
-      if (!__any_sync(FULL, on && sTr[s0] < ntc)) continue;
-      float v[U][13];
+    // the stencil values of the next group of tracers are copied into this
+    // thread's slots of a double buffer while the current group is computed
+    extern __shared__ float pf[];  // [2][U][NQ][kAdvBlock]
+    auto issue = [&](int s0, int buf) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int s = s0 + u < ntb ? s0 + u : s0;
-        const float *__restrict__ tr = tri + (size_t)sTr[s] * G.S;
+        const float *tr = tri + (size_t)sTr[s] * G.S;
+        float *d = pf + (buf * U + u) * NQ * kAdvBlock + threadIdx.x;
 #pragma unroll
-        for (int q = 0; q < 13; ++q) v[u][q] = tr[idx[q]];
+        for (int q = 0; q < NQ; ++q) cp_async4(d + q * kAdvBlock, tr + idx[q]);
       }
+      cp_async_commit();
+    };
+    issue(0, 0);
+    for (int s0 = 0, g = 0; s0 < ntb; s0 += U, ++g) {
+      if (s0 + U < ntb) {
+        issue(s0 + U, (g + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      // tracers are ascending when columns carry different numbers of them
+      if (!__any_sync(FULL, on && sTr[s0] < ntc)) continue;
+      const float *P = pf + (g & 1) * U * NQ * kAdvBlock + threadIdx.x;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int s = s0 + u;
         if (s >= ntb) break;
-        const float t0 = v[u][0];
-        const float tym1 = v[u][1], tym2 = v[u][2], typ1 = v[u][3], typ2 = v[u][4];
-        const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7], tp2 = v[u][8];
-        const float txm1 = v[u][9], txm2 = v[u][10], txp1 = v[u][11], txp2 = v[u][12];
+        const float *v = P + u * NQ * kAdvBlock;
+        const float t0 = v[0];
+        const float tym1 = v[1 * kAdvBlock], tym2 = v[2 * kAdvBlock];
+        const float typ1 = v[3 * kAdvBlock], typ2 = v[4 * kAdvBlock];
+        const float tm1 = v[5 * kAdvBlock], tm2 = v[6 * kAdvBlock];
+        const float tp1 = v[7 * kAdvBlock], tp2 = v[8 * kAdvBlock];
+        const float txm1 = v[9 * kAdvBlock], txm2 = v[10 * kAdvBlock];
+        const float txp1 = v[11 * kAdvBlock], txp2 = v[12 * kAdvBlock];
         const float Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
         const float Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
         const float Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
