@@ -1010,7 +1010,7 @@ int make_schedule(shoc_tr_gpu *h, double dmin, Sched &s) {
   return SHOC_TR_OK;
 }
 
-int launch_part_a(shoc_tr_gpu *h) {
+int launch_part_a(shoc_tr_gpu *h, int cur) {
   cudaStream_t st = h->stream;
   k_reset<<<1, 32, 0, st>>>(h->W, h->d_counts);
   h->launches++;
@@ -1019,11 +1019,11 @@ int launch_part_a(shoc_tr_gpu *h) {
     int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
     if (h->esize == sizeof(float))
       k_lateral<float><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
-                                               (float *)h->tr[h->cur], (float *)h->tr[h->cur ^ 1]);
+                                               (float *)h->tr[cur], (float *)h->tr[cur ^ 1]);
     else
       k_lateral<double><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
-                                                (double *)h->tr[h->cur],
-                                                (double *)h->tr[h->cur ^ 1]);
+                                                (double *)h->tr[cur],
+                                                (double *)h->tr[cur ^ 1]);
     h->launches++;
   }
   int nb = (h->ncol + 127) / 128;
@@ -1196,7 +1196,7 @@ int read_status(shoc_tr_gpu *h) {
 // k_set_dz to read the sub-step minimum; afterwards steps replay a graph.
 int step_async(shoc_tr_gpu *h) {
   if (h->probe_left > 0 || !h->have_sched) {
-    int rc = launch_part_a(h);
+    int rc = launch_part_a(h, h->cur);
     if (rc) return rc;
     rc = read_status(h);
     if (rc) return rc;
@@ -1235,7 +1235,7 @@ int step_async(shoc_tr_gpu *h) {
   }
   if (h->profile) {
     // profiling launches directly so each transport launch is timed
-    int rc = launch_part_a(h);
+    int rc = launch_part_a(h, h->cur);
     if (rc) return rc;
     rc = launch_part_b(h, h->sched, h->cur);
     if (rc) return rc;
@@ -1244,18 +1244,27 @@ int step_async(shoc_tr_gpu *h) {
   }
   int gi = h->cur;
   if (!h->graph[gi]) {
-    cudaGraph_t graph;
-    long long l0 = h->launches;
-    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    int rc = launch_part_a(h);
-    if (!rc) rc = launch_part_b(h, h->sched, h->cur);
-    cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
-    if (rc) return rc;
-    CK(e);
-    CK(cudaGraphInstantiate(&h->graph[gi], graph, 0));
-    cudaGraphDestroy(graph);
-    h->graph_launches[gi] = h->launches - l0;  // kernels in the graph
-    h->launches = l0;
+    // An odd number of sub-steps alternates the buffers from step to step:
+    // both graphs are captured and uploaded together, so no later step pays
+    // for a capture or a first upload.
+    const int ng = (h->sched.sub.size() & 1) ? 2 : 1;
+    for (int k = 0; k < ng; ++k) {
+      const int g = gi ^ k;
+      if (h->graph[g]) continue;
+      cudaGraph_t graph;
+      long long l0 = h->launches;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = launch_part_a(h, g);
+      if (!rc) rc = launch_part_b(h, h->sched, g);
+      cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+      if (rc) return rc;
+      CK(e);
+      CK(cudaGraphInstantiate(&h->graph[g], graph, 0));
+      cudaGraphDestroy(graph);
+      CK(cudaGraphUpload(h->graph[g], h->stream));
+      h->graph_launches[g] = h->launches - l0;  // kernels in the graph
+      h->launches = l0;
+    }
   }
   CK(cudaGraphLaunch(h->graph[gi], h->stream));
   h->launches += h->graph_launches[gi];

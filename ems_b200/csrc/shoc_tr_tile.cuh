@@ -141,7 +141,7 @@ __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2,
 // k_adv32
 
 constexpr int kAdvBlock = 256;
-constexpr int kAdvGroup = 2;       // tracers whose loads a thread issues together
+constexpr int kAdvGroup = 1;       // tracers whose loads a thread issues together
 // dynamic shared memory of k_adv32 with uniform flags: the double-buffered
 // stencil values of a group of tracers per thread
 constexpr size_t kAdvSmem = (size_t)2 * kAdvGroup * 13 * kAdvBlock * sizeof(float);
