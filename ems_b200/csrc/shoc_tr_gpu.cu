@@ -107,6 +107,12 @@ struct shoc_tr_gpu {
   int *d_counts = nullptr;  // [0] vcs, [1] vc
   int last_status = 0;
   long long warn_total = 0;
+  // pipeline of the drop-in step on host arrays (made on its first use)
+  std::vector<int> slot_host;       // slot -> tracer, as T.slot_tr
+  cudaStream_t s_up = nullptr, s_dn = nullptr;  // host -> device, device -> host
+  std::vector<cudaEvent_t> pev;     // [0] flow sent, then per chunk: sent, stepped
+  double *xout = nullptr;           // FP32-mixed: one tracer of FP64 for the way back
+  uint8_t *c3s = nullptr;           // [kItermax + 2][ncol] k_serial cursors between chunks
 };
 
 namespace {
@@ -155,12 +161,12 @@ __global__ void k_reset(Work W, int *counts) {
 // both tracer buffers so the value read during every sub-step, and the value
 // left in the returned array, is the start-of-step one.
 template <class TR>
-__global__ void k_lateral(int nbpt, const int *bpt, const int *bin, int ntr, int S, TR *tra,
-                          TR *trb) {
-  long long tot = (long long)nbpt * ntr;
+__global__ void k_lateral(int nbpt, const int *bpt, const int *bin, const int *slot_tr,
+                          int nslot, int S, TR *tra, TR *trb) {
+  long long tot = (long long)nbpt * nslot;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
        i += (long long)gridDim.x * blockDim.x) {
-    int n = (int)(i / nbpt), b = (int)(i % nbpt);
+    int n = slot_tr[i / nbpt], b = (int)(i % nbpt);
     size_t off = (size_t)n * S;
     TR v = tra[off + bin[b]];
     tra[off + bpt[b]] = v;
@@ -388,14 +394,18 @@ __global__ void k_courant(Geo G, Flow F, Work W, double dtu, int only_listed) {
 
 // Columns where tr_bounds' thin-surface cursor can move between tracers:
 // one thread per column, tracers in tbdy order, as the reference loops.
+// When the tracers go through in chunks of slots (the drop-in step's
+// pipeline), c3s holds each listed column's cursor state between the chunks
+// of one sub-step: read when c3_load, written back always.
 template <bool LAST, class TR>
 __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
-                         const TR *__restrict__ tr_in, TR *__restrict__ tr_out) {
+                         const TR *__restrict__ tr_in, TR *__restrict__ tr_out,
+                         uint8_t *__restrict__ c3s, int c3_load) {
   int cnt = *W.serial_count;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     int col = W.serial_list[i];
     LocalSol sol;
-    bool c3 = false;
+    bool c3 = (c3s && c3_load) ? c3s[i] != 0 : false;
     unsigned long long warn = 0;
     int stat = 0;
     for (int sl = 0; sl < T.nslot; ++sl) {
@@ -404,6 +414,7 @@ __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
       column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S,
                         col, n, G.col_kb[col], true, sol, c3, warn, stat);
     }
+    if (c3s) c3s[i] = c3 ? 1 : 0;
     if (warn) atomicAdd(W.nwarn, warn);
     if (stat) atomicOr(W.status, stat);
   }
@@ -698,8 +709,13 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h) {
         if (std::find(done.begin(), done.end(), x) == done.end()) done.push_back(x);
     for (cudaEvent_t x : done) cudaEventDestroy(x);
   }
+  for (cudaStream_t x : {h->s_up, h->s_dn})
+    if (x) cudaStreamSynchronize(x);
+  for (cudaEvent_t x : h->pev) cudaEventDestroy(x);
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_dtm) cudaFreeHost(h->h_dtm);
+  for (cudaStream_t x : {h->s_up, h->s_dn})
+    if (x) cudaStreamDestroy(x);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -854,6 +870,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     h->adv_flags = !all_a ? 0 : (no_h ? 1 : (all_h ? 2 : 0));
   }
   h->nslot = (int)slot.size();
+  h->slot_host = slot;
   TrSet &T = h->T;
   T.ntr = ntr;
   T.nslot = h->nslot;
@@ -1010,22 +1027,30 @@ int make_schedule(shoc_tr_gpu *h, double dmin, Sched &s) {
   return SHOC_TR_OK;
 }
 
-int launch_part_a(shoc_tr_gpu *h, int cur) {
+// set_lateral_BC_tr for the tracers of T (every tracer, or one chunk of the
+// drop-in step's pipeline) into both buffers
+void launch_lateral(shoc_tr_gpu *h, int cur, const TrSet &T) {
+  if (h->nbpt <= 0 || T.nslot <= 0) return;
+  cudaStream_t st = h->stream;
+  long long tot = (long long)h->nbpt * T.nslot;
+  int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
+  if (h->esize == sizeof(float))
+    k_lateral<float><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, T.slot_tr, T.nslot, h->S,
+                                             (float *)h->tr[cur], (float *)h->tr[cur ^ 1]);
+  else
+    k_lateral<double><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, T.slot_tr, T.nslot,
+                                              h->S, (double *)h->tr[cur],
+                                              (double *)h->tr[cur ^ 1]);
+  h->launches++;
+}
+
+// Step set-up: counters, lateral boundaries (when `lateral`) and k_set_dz.
+// k_set_dz reads no tracer, so the lateral copies may follow it instead.
+int launch_part_a(shoc_tr_gpu *h, int cur, bool lateral = true) {
   cudaStream_t st = h->stream;
   k_reset<<<1, 32, 0, st>>>(h->W, h->d_counts);
   h->launches++;
-  if (h->nbpt > 0) {
-    long long tot = (long long)h->nbpt * h->ntr;
-    int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
-    if (h->esize == sizeof(float))
-      k_lateral<float><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
-                                               (float *)h->tr[cur], (float *)h->tr[cur ^ 1]);
-    else
-      k_lateral<double><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, h->ntr, h->S,
-                                                (double *)h->tr[cur],
-                                                (double *)h->tr[cur ^ 1]);
-    h->launches++;
-  }
+  if (lateral) launch_lateral(h, cur, h->T);
   int nb = (h->ncol + 127) / 128;
   k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->tl, h->any_vdiff ? 1 : 0, h->d_counts,
                                h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0);
@@ -1037,41 +1062,41 @@ int launch_part_a(shoc_tr_gpu *h, int cur) {
 // One FP64 transport sub-step over the staged columns: k_adv64, then one
 // k_vd64 launch per depth class.  Returns the kernels launched.
 template <bool Q, bool U, int M>
-void adv64(const shoc_tr_gpu *h, int grid, const SubStep &ss, const Tile &tl, const double *tin,
-           double *tout) {
-  k_adv64<Q, U, M><<<grid, kAdvBlock, 0, h->stream>>>(h->G, h->F, h->W, h->T, ss, tl, tin,
-                                                      tout, h->fzs64, h->any_hdiff ? 1 : 0);
+void adv64(const shoc_tr_gpu *h, int grid, const SubStep &ss, const Tile &tl, const TrSet &T,
+           const double *tin, double *tout) {
+  k_adv64<Q, U, M><<<grid, kAdvBlock, 0, h->stream>>>(h->G, h->F, h->W, T, ss, tl, tin, tout,
+                                                      h->fzs64, h->any_hdiff ? 1 : 0);
 }
 template <bool Q, bool U>
 void adv64_mode(const shoc_tr_gpu *h, int grid, const SubStep &ss, const Tile &tl,
-                const double *tin, double *tout) {
+                const TrSet &T, const double *tin, double *tout) {
   if (h->adv_flags == 1)
-    adv64<Q, U, 1>(h, grid, ss, tl, tin, tout);
+    adv64<Q, U, 1>(h, grid, ss, tl, T, tin, tout);
   else if (h->adv_flags == 2)
-    adv64<Q, U, 2>(h, grid, ss, tl, tin, tout);
+    adv64<Q, U, 2>(h, grid, ss, tl, T, tin, tout);
   else
-    adv64<Q, U, 0>(h, grid, ss, tl, tin, tout);
+    adv64<Q, U, 0>(h, grid, ss, tl, T, tin, tout);
 }
 int tile64_substep(const shoc_tr_gpu *h, bool last, const SubStep &ss, const Tile &tl,
-                   const double *tin, double *tout, int nw, cudaEvent_t *ev) {
+                   const TrSet &T, const double *tin, double *tout, int nw, cudaEvent_t *ev) {
   cudaStream_t st = h->stream;
   int nl = 0;
   if (ev) cudaEventRecord(ev[0], st);
-  if (h->T.ntb > 0 && tl.nwet > 0) {
+  if (T.ntb > 0 && tl.nwet > 0) {
     const int grid = (tl.nwet + kAdvBlock - 1) / kAdvBlock;
     const bool q = h->O.trasc == SHOC_TR_QUICKEST, u = h->O.ultimate != 0;
     if (q && u)
-      adv64_mode<true, true>(h, grid, ss, tl, tin, tout);
+      adv64_mode<true, true>(h, grid, ss, tl, T, tin, tout);
     else if (q)
-      adv64_mode<true, false>(h, grid, ss, tl, tin, tout);
+      adv64_mode<true, false>(h, grid, ss, tl, T, tin, tout);
     else if (u)
-      adv64_mode<false, true>(h, grid, ss, tl, tin, tout);
+      adv64_mode<false, true>(h, grid, ss, tl, T, tin, tout);
     else
-      adv64_mode<false, false>(h, grid, ss, tl, tin, tout);
+      adv64_mode<false, false>(h, grid, ss, tl, T, tin, tout);
     nl++;
   }
   if (ev) cudaEventRecord(ev[1], st);
-  const int nchunk = (h->T.nslot + nw - 1) / nw;
+  const int nchunk = (T.nslot + nw - 1) / nw;
   const dim3 blk(32, nw);
   for (int i = 0; i < tl.nclass; i++) {
     const int t0 = tl.ctile[i], nt = tl.ctile[i + 1] - t0, kbase = tl.cbase[i];
@@ -1079,11 +1104,11 @@ int tile64_substep(const shoc_tr_gpu *h, bool last, const SubStep &ss, const Til
     const size_t smem = vd64_smem(h->nz - kbase, nw);
     if (last)
       k_vd64<true><<<nt * nchunk, blk, smem, st>>>(
-          h->G, h->F, h->W, h->O, h->T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
+          h->G, h->F, h->W, h->O, T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
           h->W.vd_div, h->W.vd_ud, nw, nchunk, t0, kbase);
     else
       k_vd64<false><<<nt * nchunk, blk, smem, st>>>(
-          h->G, h->F, h->W, h->O, h->T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
+          h->G, h->F, h->W, h->O, T, ss, tl, tin, tout, h->fzs64, h->W.vd_dzdt, h->W.vd_cm1,
           h->W.vd_div, h->W.vd_ud, nw, nchunk, t0, kbase);
     nl++;
   }
@@ -1116,7 +1141,11 @@ Tile vd_classes(const shoc_tr_gpu *h, int nw) {
   return t;
 }
 
-int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
+// The transport sub-steps of one step for the tracers of T (every tracer, or
+// one chunk of the drop-in step's pipeline; c3s/c3_load as k_serial takes
+// them, one row of ncol bytes per sub-step).
+int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
+                  uint8_t *c3s = nullptr, bool c3_load = false) {
   cudaStream_t st = h->stream;
   int cur = cur0;
   const int nsub = (int)s.sub.size();
@@ -1125,9 +1154,10 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
   for (int i = 0; i < nsub; i++) {
     const SubStep &ss = s.sub[i];
     bool last = (i == nsub - 1);
+    uint8_t *c3row = c3s ? c3s + (size_t)i * h->ncol : nullptr;
     k_courant<<<cblocks, 256, 0, st>>>(h->G, h->F, h->W, ss.dtu, h->staged ? 1 : 0);
     h->launches++;
-    if (h->esize == sizeof(float) && h->nslot > 0) {  // FP32-mixed
+    if (h->esize == sizeof(float) && T.nslot > 0) {  // FP32-mixed
       const float *tin = (const float *)h->tr[cur];
       float *tout = (float *)h->tr[cur ^ 1];
       bool prof = h->profile && last;
@@ -1136,34 +1166,34 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
         for (auto &e : ev) cudaEventCreate(&e);
       const Tile tl = vd_classes(h, tw);
       tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
-                     h->F3, h->W, h->O, h->T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
+                     h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
                      h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
       if (prof) {  // pairs share events; sync destroys each event once
         h->ev.push_back({0, ev[0], ev[2]});
         h->ev.push_back({1, ev[0], ev[1]});
         h->ev.push_back({2, ev[1], ev[2]});
       }
-      h->launches += (h->T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
-      for (int i = 0; i < tl.nclass; i++) h->launches += tl.ctile[i + 1] > tl.ctile[i] ? 1 : 0;
+      h->launches += (T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
+      for (int k = 0; k < tl.nclass; k++) h->launches += tl.ctile[k + 1] > tl.ctile[k] ? 1 : 0;
       if (last)
-        k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                            tin, tout);
+        k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
+                                                            tin, tout, c3row, c3_load);
       else
-        k_serial<false, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                             tin, tout);
+        k_serial<false, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
+                                                             tin, tout, c3row, c3_load);
       h->launches++;
       cur ^= 1;
       continue;
     }
     const double *tin = (const double *)h->tr[cur];
     double *tout = (double *)h->tr[cur ^ 1];
-    if (h->nslot > 0) {
+    if (T.nslot > 0) {
       bool prof = h->profile && last;
       cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
       if (prof)
         for (auto &e : ev) cudaEventCreate(&e);
       const Tile tl = vd_classes(h, tw);
-      const int nl = tile64_substep(h, last, ss, tl, tin, tout, tw, prof ? ev : nullptr);
+      const int nl = tile64_substep(h, last, ss, tl, T, tin, tout, tw, prof ? ev : nullptr);
       if (prof) {
         h->ev.push_back({0, ev[0], ev[2]});
         h->ev.push_back({1, ev[0], ev[1]});
@@ -1171,11 +1201,11 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0) {
       }
       h->launches += nl;
       if (last)
-        k_serial<true, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                             tin, tout);
+        k_serial<true, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
+                                                             tin, tout, c3row, c3_load);
       else
-        k_serial<false, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, h->T, ss,
-                                                              tin, tout);
+        k_serial<false, double><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
+                                                              tin, tout, c3row, c3_load);
       h->launches++;
     }
     cur ^= 1;
@@ -1192,52 +1222,64 @@ int read_status(shoc_tr_gpu *h) {
   return 0;
 }
 
+// Part A of a step whose sub-step schedule is not known yet, then the
+// sub-step minimum read back and the schedule built from it (tracers.c:
+// 591-720).  lateral: whether part A fills every tracer's lateral boundary.
+int probe_schedule(shoc_tr_gpu *h, bool lateral, Sched &s) {
+  int rc = launch_part_a(h, h->cur, lateral);
+  if (rc) return rc;
+  rc = read_status(h);
+  if (rc) return rc;
+  int st = *h->h_status;
+  if (st & (ST_LASTDRY | ST_GEOM)) {
+    h->last_status = map_status(st);
+    return h->last_status;
+  }
+  double dmin;
+  unsigned long long b = *h->h_dtm;
+  memcpy(&dmin, &b, 8);
+  rc = make_schedule(h, dmin, s);
+  if (rc) h->last_status = rc;
+  return rc;
+}
+
+// Keep a probed schedule for the graph-replayed steps; graphs made for
+// another schedule are dropped.
+void adopt_schedule(shoc_tr_gpu *h, const Sched &s) {
+  bool same = h->have_sched && s.sub.size() == h->sched.sub.size();
+  if (same)
+    for (size_t i = 0; i < s.sub.size(); i++)
+      if (memcmp(&s.sub[i], &h->sched.sub[i], sizeof(SubStep)) != 0) same = false;
+  if (!same) {
+    for (int i = 0; i < 2; i++)
+      if (h->graph[i]) {
+        cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+      }
+  }
+  h->sched = s;
+  h->have_sched = true;
+  if (h->probe_left > 0) h->probe_left--;
+}
+
 // One step.  When the schedule is not yet known the step synchronises after
 // k_set_dz to read the sub-step minimum; afterwards steps replay a graph.
 int step_async(shoc_tr_gpu *h) {
   if (h->probe_left > 0 || !h->have_sched) {
-    int rc = launch_part_a(h, h->cur);
-    if (rc) return rc;
-    rc = read_status(h);
-    if (rc) return rc;
-    int st = *h->h_status;
-    if (st & (ST_LASTDRY | ST_GEOM)) {
-      h->last_status = map_status(st);
-      return h->last_status;
-    }
-    double dmin;
-    unsigned long long b = *h->h_dtm;
-    memcpy(&dmin, &b, 8);
     Sched s;
-    rc = make_schedule(h, dmin, s);
-    if (rc) {
-      h->last_status = rc;
-      return rc;
-    }
-    rc = launch_part_b(h, s, h->cur);
+    int rc = probe_schedule(h, true, s);
+    if (rc) return rc;
+    rc = launch_part_b(h, s, h->cur, h->T);
     if (rc) return rc;
     if (s.sub.size() & 1) h->cur ^= 1;
-    bool same = h->have_sched && s.sub.size() == h->sched.sub.size();
-    if (same)
-      for (size_t i = 0; i < s.sub.size(); i++)
-        if (memcmp(&s.sub[i], &h->sched.sub[i], sizeof(SubStep)) != 0) same = false;
-    if (!same) {
-      for (int i = 0; i < 2; i++)
-        if (h->graph[i]) {
-          cudaGraphExecDestroy(h->graph[i]);
-          h->graph[i] = nullptr;
-        }
-    }
-    h->sched = s;
-    h->have_sched = true;
-    if (h->probe_left > 0) h->probe_left--;
+    adopt_schedule(h, s);
     return 0;
   }
   if (h->profile) {
     // profiling launches directly so each transport launch is timed
     int rc = launch_part_a(h, h->cur);
     if (rc) return rc;
-    rc = launch_part_b(h, h->sched, h->cur);
+    rc = launch_part_b(h, h->sched, h->cur, h->T);
     if (rc) return rc;
     if (h->sched.sub.size() & 1) h->cur ^= 1;
     return 0;
@@ -1255,7 +1297,7 @@ int step_async(shoc_tr_gpu *h) {
       long long l0 = h->launches;
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       int rc = launch_part_a(h, g);
-      if (!rc) rc = launch_part_b(h, h->sched, g);
+      if (!rc) rc = launch_part_b(h, h->sched, g, h->T);
       cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
       if (rc) return rc;
       CK(e);
@@ -1269,6 +1311,142 @@ int step_async(shoc_tr_gpu *h) {
   CK(cudaGraphLaunch(h->graph[gi], h->stream));
   h->launches += h->graph_launches[gi];
   if (h->sched.sub.size() & 1) h->cur ^= 1;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The drop-in step on host arrays, pipelined.  The tracers cross the host
+// link in chunks of slots: chunk j goes up on one copy stream, is stepped on
+// the main stream and comes back on a second copy stream, so the way back of
+// chunk j overlaps the way up of the chunks after it (the link is full
+// duplex) and every chunk's transport overlaps both.  Per tracer the kernels
+// and their order are those of a whole step: the tracers of a step are
+// independent apart from the general path's thin-surface cursor, which
+// k_serial carries from chunk to chunk (c3s); set_dz reads no tracer, so the
+// lateral boundaries of a chunk may follow it.
+
+// slots per chunk: the column kernels' tracers per block (no idle tracer rows
+// in their blocks), widened to keep at most 12 chunks
+int pipe_chunk_slots(const shoc_tr_gpu *h) {
+  const int tw = std::max(h->tw, 1);
+  int c = tw;
+  while ((h->nslot + c - 1) / c > 12) c += tw;
+  return c;
+}
+
+int pipe_init(shoc_tr_gpu *h) {
+  if (h->s_up) return 0;
+  CK(cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h->s_dn, cudaStreamNonBlocking));
+  if (h->esize == sizeof(float)) {
+    int rc = dalloc(h, &h->xout, (size_t)h->S);
+    if (rc) return rc;
+  }
+  int rc = dalloc(h, &h->c3s, (size_t)(kItermax + 2) * h->ncol);
+  if (rc) return rc;
+  h->pev.assign(1 + 2 * (size_t)h->nslot, nullptr);
+  for (auto &e : h->pev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  return 0;
+}
+
+// wait for every copy that may still touch the caller's host arrays
+void pipe_drain(shoc_tr_gpu *h) {
+  cudaStreamSynchronize(h->s_up);
+  cudaStreamSynchronize(h->s_dn);
+  cudaStreamSynchronize(h->stream);
+}
+
+int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
+  cudaStream_t s = h->s_up;
+  const size_t S = (size_t)h->S;
+  if (h->esize == sizeof(double)) {
+    double *a = (double *)h->tr[cur] + n * S, *b = (double *)h->tr[cur ^ 1] + n * S;
+    CK(cudaMemcpyAsync(a, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b, a, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else {
+    float *a = (float *)h->tr[cur] + n * S, *b = (float *)h->tr[cur ^ 1] + n * S;
+    CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_to_f32<<<592, 256, 0, s>>>(h->xfer, a, S);
+    h->launches++;
+    CK(cudaMemcpyAsync(b, a, S * sizeof(float), cudaMemcpyDeviceToDevice, s));
+  }
+  return 0;
+}
+
+int down_tracer(shoc_tr_gpu *h, int buf, int n, double *dst) {
+  cudaStream_t s = h->s_dn;
+  const size_t S = (size_t)h->S;
+  if (h->esize == sizeof(double)) {
+    CK(cudaMemcpyAsync(dst, (double *)h->tr[buf] + n * S, S * sizeof(double),
+                       cudaMemcpyDeviceToHost, s));
+  } else {
+    k_to_f64<<<592, 256, 0, s>>>((float *)h->tr[buf] + n * S, h->xout, S);
+    h->launches++;
+    CK(cudaMemcpyAsync(dst, h->xout, S * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  return 0;
+}
+
+int step_pipelined(shoc_tr_gpu *h, shoc_tr_state *st) {
+  int rc = pipe_init(h);
+  if (rc) return rc;
+  rc = shoc_tr_gpu_set_flow(h, st);
+  if (rc) return rc;
+  const int cur = h->cur, csl = pipe_chunk_slots(h);
+  const int nch = (h->nslot + csl - 1) / csl;
+  cudaEvent_t *ev = h->pev.data();  // [0] flow sent, [1 + 2j] chunk j sent, [2 + 2j] stepped
+  // the tracers follow the flow fields up the link
+  CK(cudaEventRecord(ev[0], h->stream));
+  CK(cudaStreamWaitEvent(h->s_up, ev[0], 0));
+  for (int j = 0; j < nch; j++) {
+    for (int sl = j * csl; sl < std::min(h->nslot, (j + 1) * csl); sl++) {
+      const int n = h->slot_host[sl];
+      rc = up_tracer(h, cur, n, st->tr_wc[n]);
+      if (rc) {
+        pipe_drain(h);
+        return rc;
+      }
+    }
+    CK(cudaEventRecord(ev[1 + 2 * j], h->s_up));
+  }
+  // the schedule from this step's flow, while the tracers travel
+  Sched s;
+  rc = probe_schedule(h, false, s);
+  if (!rc && s.sub.size() > (size_t)kItermax + 2) rc = SHOC_TR_ESUBSTEP;
+  if (rc) {
+    pipe_drain(h);
+    return rc;
+  }
+  const int fin = cur ^ (int)(s.sub.size() & 1);  // the buffer the step ends in
+  for (int j = 0; j < nch; j++) {
+    const int s0 = j * csl, ns = std::min(h->nslot - s0, csl);
+    TrSet Tc = h->T;
+    Tc.slot_tr = h->T.slot_tr + s0;
+    Tc.nslot = ns;
+    Tc.ntb = std::max(0, std::min(h->T.ntb - s0, ns));
+    CK(cudaStreamWaitEvent(h->stream, ev[1 + 2 * j], 0));
+    launch_lateral(h, cur, Tc);
+    rc = launch_part_b(h, s, cur, Tc, h->c3s, j > 0);
+    if (rc) {
+      pipe_drain(h);
+      return rc;
+    }
+    CK(cudaEventRecord(ev[2 + 2 * j], h->stream));
+    CK(cudaStreamWaitEvent(h->s_dn, ev[2 + 2 * j], 0));
+    for (int sl = s0; sl < s0 + ns; sl++) {
+      const int n = h->slot_host[sl];
+      rc = down_tracer(h, fin, n, st->tr_wc[n]);
+      if (rc) {
+        pipe_drain(h);
+        return rc;
+      }
+    }
+  }
+  // the main stream (and so the status read after it) waits for the way back
+  CK(cudaEventRecord(ev[0], h->s_dn));
+  CK(cudaStreamWaitEvent(h->stream, ev[0], 0));
+  h->cur = fin;
+  adopt_schedule(h, s);
   return 0;
 }
 
@@ -1435,21 +1613,30 @@ int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag) {
 
 int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag) {
   if (!h || !st || !st->tr_wc || st->ntr != h->ntr) return SHOC_TR_EARG;
-  int rc = shoc_tr_gpu_set_flow(h, st);
-  if (rc) return rc;
-  rc = shoc_tr_gpu_upload_tracers(h, st->tr_wc);
-  if (rc) return rc;
-  rc = shoc_tr_gpu_run(h, 1);
+  for (int n = 0; n < h->ntr; n++)
+    if (!st->tr_wc[n]) return SHOC_TR_EARG;
+  cudaSetDevice(h->device);
+  int rc = step_pipelined(h, st);
   if (rc) {
     shoc_tr_gpu_sync(h, nullptr);
     return rc;
   }
   rc = shoc_tr_gpu_sync(h, diag);
-  int rc2 = shoc_tr_gpu_download_tracers(h, st->tr_wc);
-  if (!rc) rc = rc2;
-  rc2 = shoc_tr_gpu_get_surface(h, st->sur_t, st->nsur_t);
+  int rc2 = shoc_tr_gpu_get_surface(h, st->sur_t, st->nsur_t);
   if (!rc) rc = rc2;
   return rc;
+}
+
+int shoc_tr_gpu_host_register(void *ptr, size_t bytes) {
+  if (!ptr || !bytes) return SHOC_TR_EARG;
+  CK(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return 0;
+}
+
+int shoc_tr_gpu_host_unregister(void *ptr) {
+  if (!ptr) return SHOC_TR_EARG;
+  CK(cudaHostUnregister(ptr));
+  return 0;
 }
 
 int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {

@@ -22,7 +22,7 @@ EXPORTS = (
     "shoc_tr_gpu_create", "shoc_tr_gpu_destroy", "shoc_tr_gpu_step",
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
-    "shoc_tr_gpu_mass_noalloc",
+    "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
@@ -55,6 +55,8 @@ def lib(path=None):
     L.shoc_tr_gpu_sync.argtypes = [H, C.POINTER(_abi.Diag)]
     L.shoc_tr_gpu_mass.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
+    L.shoc_tr_gpu_host_unregister.argtypes = [C.c_void_p]
     L.shoc_tr_gpu_stream.argtypes = [H]
     L.shoc_tr_gpu_stream.restype = C.c_void_p
     L.shoc_tr_gpu_set_tiling.argtypes = [H, C.c_int, C.c_int]
@@ -79,6 +81,30 @@ def lib(path=None):
 def _check(where, rc):
     if rc != 0:
         raise _abi.StatusError(where, rc)
+
+
+class HostPinned:
+    """Page-locks numpy arrays the drop-in step copies every step
+    (shoc_tr_gpu_host_register) for as long as the context is open."""
+
+    def __init__(self, arrays):
+        self.L = lib()
+        self.arrays = []
+        for a in arrays:
+            assert a.flags.c_contiguous
+            _check("host_register", self.L.shoc_tr_gpu_host_register(a.ctypes.data, a.nbytes))
+            self.arrays.append(a)
+
+    def close(self):
+        while self.arrays:
+            a = self.arrays.pop()
+            _check("host_unregister", self.L.shoc_tr_gpu_host_unregister(a.ctypes.data))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 class TracerStep:

@@ -36,6 +36,8 @@
 #ifndef SHOC_TR_GPU_H
 #define SHOC_TR_GPU_H
 
+#include <stddef.h>
+
 #include "shoc_tr.h"
 
 #ifdef __cplusplus
@@ -60,8 +62,22 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h);
 /* One step on host arrays: copies st's tracers, surface vectors and flow
  * fields to the device, runs the step, copies tracers and surface vectors
  * back into st, and waits.  Drop-in for set_lateral_BC_tr + set_dz +
- * advect_diffuse + vert_diffuse_3d on one window. */
+ * advect_diffuse + vert_diffuse_3d on one window.  The tracers travel in
+ * chunks, so the copies back of the first chunks overlap the copies up of
+ * the later ones and the step of every chunk; the results are those of
+ * shoc_tr_gpu_upload_tracers + shoc_tr_gpu_run(h, 1) +
+ * shoc_tr_gpu_download_tracers, bit for bit.  Copies reach the host link's
+ * speed only from page-locked memory: see shoc_tr_gpu_host_register. */
 int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag);
+
+/* Page-locks (cudaHostRegister) / releases a host array the caller passes to
+ * shoc_tr_gpu_step every step (tracers, flow fields), so its copies run at
+ * the host link's full speed without a staging copy.  No counterpart in the
+ * reference: an addition of this library for a host model that keeps its
+ * window arrays for the whole run.  Register once after allocating the
+ * array and unregister before freeing it. */
+int shoc_tr_gpu_host_register(void *ptr, size_t bytes);
+int shoc_tr_gpu_host_unregister(void *ptr);
 
 /* Device-resident use. */
 int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc);

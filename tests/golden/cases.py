@@ -12,6 +12,10 @@ import numpy as np
 from ems_b200 import _abi
 
 MOVING = dict(layers=np.linspace(-30, 2.0, 8))
+# layer faces at -1.0 and 0.6 m, inside the range of eta and oldeta: the
+# surface cell of most columns changes during the step (general path; with a
+# thin surface layer, tr_bounds' thin-surface cursor)
+CROSS = dict(layers=np.array([-30.0, -22.0, -14.0, -8.0, -3.0, -1.0, 0.6, 2.5]))
 
 CASES = {
     "small_quickest_ultimate": ("small", {}, 10),
@@ -24,6 +28,10 @@ CASES = {
                                  maxtr=[1.0, 2.0, 2.5]), 20),
     "small_thin_surface": ("small", dict(eta_offset=(1.9, -1.7), hmin=1.5,
                                          maxtr=[0.5, 0.5, 0.5], **MOVING), 4),
+    "small_crossing": ("small", dict(eta_offset=(1.9, -1.7), **CROSS), 6),
+    "small_crossing_substeps": ("small", dict(eta_offset=(1.9, -1.7), dt=1500.0, **CROSS), 3),
+    "small_crossing_thin": ("small", dict(eta_offset=(1.9, -1.7), hmin=1.2,
+                                          maxtr=[0.5, 0.5, 0.5], **CROSS), 4),
     "small_hdiff": ("small", dict(hdiff=(40.0, [1, 1, 1])), 10),
     "small_hdiff_mixed": ("small", dict(hdiff=(40.0, [1, 0, 1])), 10),
     "small_vanleer_hdiff": ("small", dict(trasc=_abi.VANLEER, ultimate=0,

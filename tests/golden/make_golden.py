@@ -4,6 +4,7 @@ Runs model/hd/tracers/tracers.c, compiled unmodified into oracle/_ref by
 oracle/build.py, on each case of cases.py and stores the final tracer arrays,
 surface vectors and range-warning count.  Run from the repository root in a
 checkout that has the reference tree:  python tests/golden/make_golden.py
+[name ...]  (default: every case).
 """
 import os
 import sys
@@ -21,7 +22,7 @@ from cases import CASES, build, input_digest  # noqa: E402
 def main():
     if not oracle.ref_available():
         raise SystemExit("reference build oracle/_ref missing (run oracle/build.py)")
-    for name in CASES:
+    for name in sys.argv[1:] or CASES:
         case, nsteps = build(name)
         rc, tr, sur, nsur, d = oracle.run_ref(case, nsteps)
         path = os.path.join(HERE, name + ".npz")

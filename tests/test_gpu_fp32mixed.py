@@ -50,9 +50,13 @@ def test_small_windows_within_tolerance(kw):
     np.testing.assert_array_equal(nsur, ref[3])
 
 
-def test_moving_surface_general_path():
-    # surface crossing layer faces: those columns take the general path
-    case = synth.make("small", seed=62, layers=np.linspace(-30, 2.0, 8), eta_offset=(1.9, -1.7))
+@pytest.mark.parametrize("kw", [{}, dict(dt=1500.0), dict(hmin=1.2)])
+def test_surface_crossing_general_path(kw):
+    # layer faces at -1.0 and 0.6 m between eta and oldeta: the surface cell
+    # of most columns changes during the step, and those columns take the
+    # general path (with hmin=1.2 also tr_bounds' thin-surface cursor)
+    case = synth.make("small", seed=62, eta_offset=(1.9, -1.7),
+                      layers=np.array([-30.0, -22.0, -14.0, -8.0, -3.0, -1.0, 0.6, 2.5]), **kw)
     out, sur, nsur, d = run(case, 6)
     ref = oracle.run_oracle(case, 6)
     emax, _ = errors(case, out, ref[1])

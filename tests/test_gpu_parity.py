@@ -57,7 +57,7 @@ def test_resident_run_matches_reference_fixture(name):
 
 
 @pytest.mark.parametrize("name", ["small_quickest_ultimate", "small_moving_surface",
-                                  "small_clip", "small_thin_surface"])
+                                  "small_clip", "small_thin_surface", "small_crossing_thin"])
 def test_warning_count_matches(name):
     case, nsteps = build(name)
     g = np.load(os.path.join(HERE, "golden", name + ".npz"))

@@ -40,6 +40,21 @@ def test_oracle_matches_reference_fixture(name):
         assert oracle.max_rel_err(tr, g["tr"], cells).max() <= 1e-12
 
 
+@pytest.mark.parametrize("name", ["small_crossing", "small_crossing_substeps",
+                                  "small_crossing_thin"])
+def test_crossing_cases_move_the_surface_cell(name):
+    """In the crossing cases eta and oldeta of most columns lie in different
+    layers, so the surface cell changes during every step (the general path
+    of surf_conc, and with a thin surface layer tr_bounds' cursor)."""
+    case, _ = build(name)
+    w = case.win
+    c = w.wet_cells()
+    j = w.m2d[c]
+    n_new = np.bincount(j, weights=w.gridz[c] < case.eta[j], minlength=len(case.eta))
+    n_old = np.bincount(j, weights=w.gridz[c] < case.oldeta[j], minlength=len(case.eta))
+    assert np.sum(n_new != n_old) > 50
+
+
 needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference build not present")
 
 
