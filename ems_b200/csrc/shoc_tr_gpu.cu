@@ -435,6 +435,15 @@ __global__ void k_to_f32(const double *a, float *b, size_t n) {
        i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
 }
+// one uploaded tracer into both ping-pong buffers
+__global__ void k_to_f32x2(const double *a, float *b, float *c, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float v = (float)a[i];
+    b[i] = v;
+    c[i] = v;
+  }
+}
 __global__ void k_to_f64(const float *a, double *b, size_t n) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -1149,7 +1158,7 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
   cudaStream_t st = h->stream;
   int cur = cur0;
   const int nsub = (int)s.sub.size();
-  const int tw = h->tw;
+  const int tw = std::max(1, std::min(h->tw, T.nslot));  // no idle tracer rows
   int cblocks = std::min((h->S + 255) / 256, 148 * 32);
   for (int i = 0; i < nsub; i++) {
     const SubStep &ss = s.sub[i];
@@ -1325,14 +1334,10 @@ int step_async(shoc_tr_gpu *h) {
 // k_serial carries from chunk to chunk (c3s); set_dz reads no tracer, so the
 // lateral boundaries of a chunk may follow it.
 
-// slots per chunk: the column kernels' tracers per block (no idle tracer rows
-// in their blocks), widened to keep at most 12 chunks
-int pipe_chunk_slots(const shoc_tr_gpu *h) {
-  const int tw = std::max(h->tw, 1);
-  int c = tw;
-  while ((h->nslot + c - 1) / c > 12) c += tw;
-  return c;
-}
+// slots per chunk: about a twelfth of the tracers, so the first chunk is
+// back on its way while most are still going up and the last chunk's step
+// and copy back (the part nothing overlaps) are short
+int pipe_chunk_slots(const shoc_tr_gpu *h) { return std::max(1, (h->nslot + 11) / 12); }
 
 int pipe_init(shoc_tr_gpu *h) {
   if (h->s_up) return 0;
@@ -1366,9 +1371,8 @@ int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
   } else {
     float *a = (float *)h->tr[cur] + n * S, *b = (float *)h->tr[cur ^ 1] + n * S;
     CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
-    k_to_f32<<<592, 256, 0, s>>>(h->xfer, a, S);
+    k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S);
     h->launches++;
-    CK(cudaMemcpyAsync(b, a, S * sizeof(float), cudaMemcpyDeviceToDevice, s));
   }
   return 0;
 }
@@ -1467,9 +1471,8 @@ int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
       float *a = (float *)h->tr[h->cur] + n * S, *b = (float *)h->tr[h->cur ^ 1] + n * S;
       CK(cudaMemcpyAsync(h->xfer, tr_wc[n], S * sizeof(double), cudaMemcpyHostToDevice,
                          h->stream));
-      k_to_f32<<<592, 256, 0, h->stream>>>(h->xfer, a, S);
+      k_to_f32x2<<<592, 256, 0, h->stream>>>(h->xfer, a, b, S);
       h->launches++;
-      CK(cudaMemcpyAsync(b, a, S * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
     }
   }
   return 0;
