@@ -16,7 +16,7 @@ template <bool Q, bool U, int M>
 void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
          const float *tin, float *tout, float *fzs, int hd) {
-  k_adv32<Q, U, M><<<grid, kAdvBlock, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
+  k_adv32<Q, U, M><<<grid, kAdv32Block, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
                                                                   tin, tout, fzs, hd);
 }
 template <bool Q, bool U>
@@ -54,7 +54,7 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     int any_hd, int adv_flags, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {
-    const int grid = (Tl.nwet + kAdvBlock - 1) / kAdvBlock;
+    const int grid = (Tl.nwet + kAdv32Block - 1) / kAdv32Block;
     if (quick && ult)
       adv_mode<true, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
                            any_hd);

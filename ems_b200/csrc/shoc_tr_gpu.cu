@@ -182,12 +182,14 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
 // scheme work arrays w5/w9 (:561-567) and their 2/(w9+w9) factors, the
 // sub-step search (:591-668) as a min-reduction, the column flags and the
 // tracer-independent LU factors of vert_diffuse_3d / implicit_vdiff_tr
-// (:3841-3889, :4185-4195).  The column's cells come from the layer-by-column
-// table in one batch of independent loads (cl[j]: j = 0 the sediment cell,
-// j = 1..nk the wet layers from the bottom up) and its thicknesses and w9 are
-// kept in local arrays, so the walks below index layers instead of chasing
-// zm1 / zp1; every walk visits the cells the reference's walk visits, in the
-// same order, with the same arithmetic.
+// (:3841-3889, :4185-4195).  Layer j of the column (j = 0 the sediment cell,
+// j = 1..nk the wet layers from the bottom up) comes from the layer-by-column
+// table; the thickness of a layer is a function of the surface cells and two
+// layer faces, so the column is streamed twice without per-layer arrays: top
+// down for the thicknesses, work arrays and sub-step search (a window of the
+// layers around j in registers), bottom up for the LU recurrence.  Every
+// value is the reference's expression on the reference's operands, and the
+// sub-step minimum does not depend on the order the cells are visited in.
 // list_all: put every column the tile kernels do not handle on the
 // general-path list (else only the tracer-coupled thin-surface columns).
 // fp32: also write the FP32 thickness and LU factors.
@@ -199,20 +201,20 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
   if (col < G.ncol) {
     const int top = G.col_top[col], bot = G.col_bot[col], kb = G.col_kb[col];
     const int nk = G.nz - kb;  // wet layers of the column
-    int cl[kSerialMaxLayers + 1];
-    double dzl[kSerialMaxLayers + 1], w9l[kSerialMaxLayers + 1];
-    cl[0] = G.zm1[bot];  // the sediment cell
-    for (int j = 1; j <= nk; ++j) cl[j] = Tl.cellk[(size_t)(kb + j - 1) * Tl.ncolp + col];
-    // layer position of a cell of this column (0: the sediment)
-    auto jof = [&](int c) { return c == cl[0] ? 0 : G.kof[c] - kb + 1; };
+    const int sed = G.zm1[bot];
+    // cell of layer j and the layer of a cell of this column
+    auto cell = [&](int j) {
+      return j == 0 ? sed : Tl.cellk[(size_t)(kb + j - 1) * Tl.ncolp + col];
+    };
+    auto jof = [&](int c) { return c == sed ? 0 : G.kof[c] - kb + 1; };
 
     // new and old surface cells (tracers.c:5739-5755): down from the top
     // while the cell's bottom is at or above eta, at most to the sediment
     int sur = W.nsur_t[col];
     int jn = nk;
     const double etat = F.eta[top];
-    while (jn > 0 && G.gridz[cl[jn]] >= etat) --jn;
-    int nsur = cl[jn];
+    while (jn > 0 && G.gridz[cell(jn)] >= etat) --jn;
+    int nsur = cell(jn);
     W.sur_t[col] = sur;
     W.nsur_t[col] = nsur;
     const int js0 = jof(sur);
@@ -223,50 +225,45 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     double tz = F.eta[c2] < F.oldeta[c2] ? F.eta[c2] : F.oldeta[c2];
     double bz = SHOC_TR_DRY_FRAC * O.hmin + G.botz[c2];
     bool wet = (tz > bz && js > 0);
-    // thicknesses (:5824-5846): from the old surface down, then copied up
-    {
-      dzl[0] = W.dz[cl[0]];
-      int t2 = G.m2d[sur];
-      double tp = F.oldeta[t2];
-      for (int j = js0; j > 1; --j) {
-        double b = G.gridz[cl[j]];
-        dzl[j] = tp - b;
-        tp = b;
-      }
-      dzl[1] = tp - G.botz[t2];
-      for (int j = js0 + 1; j <= nk; ++j) dzl[j] = dzl[js0];
-      for (int j = 1; j <= nk; ++j) W.dz[cl[j]] = dzl[j];
-      if (fp32)
-        for (int j = 1; j <= nk; ++j) W.dz32[cl[j]] = (float)dzl[j];
-    }
-    // scheme work arrays over every cell of the column (:530-567)
+    // thickness of layer j (:5824-5846): from the old surface down to the
+    // bottom, the layers above the old surface copy the old surface cell's
+    // (with the old surface in the sediment, every layer copies the
+    // sediment's)
+    const int t2 = G.m2d[sur];
+    const double oet = F.oldeta[t2], bott = G.botz[t2], dzsed = W.dz[sed];
+    auto dzof = [&](int j) -> double {
+      const int jj = j < js0 ? j : js0;
+      if (jj == 0) return dzsed;
+      const double tp = (jj == js0) ? oet : G.gridz[cell(jj + 1)];
+      return tp - ((jj > 1) ? G.gridz[cell(jj)] : bott);
+    };
+    // top-down pass: dz, dz32, w5, w9, dbz, dfz (:530-567), the sub-step
+    // search over the cells to process (:591-661) and what the flags need
+    const bool substep = O.substep != 0, quick = O.trasc == SHOC_TR_QUICKEST;
+    int nc = 0;
+    int ja = -1;             // highest layer <= jn of zero thickness
+    double dz_js0 = dzsed, dz_jn = 0.0, dz_jn1 = 0.0;
+    double dzc = dzof(nk);                         // dz(j)
+    double dzm = nk >= 1 ? dzof(nk - 1) : dzsed;   // dz(j - 1)
+    double w9c = 0.5 * (dzc + dzm), w9p = w9c;     // w9(j), w9(j + 1)
     for (int j = nk; j >= 1; --j) {
-      const int cc = cl[j];
-      double dzm = dzl[j - 1], dzc = dzl[j];
-      if (O.trasc == SHOC_TR_QUICKEST) W.w5[cc] = dzm / (dzm + dzc);
-      w9l[j] = 0.5 * (dzc + dzm);
-      W.w9[cc] = w9l[j];
-    }
-    for (int j = nk; j >= 1; --j) {
-      const int cc = cl[j];
-      double w9c = w9l[j];
-      double w9m = (j == 1) ? 0.0 : w9l[j - 1];
+      const int cc = cell(j);
+      const double dzmm = j >= 2 ? dzof(j - 2) : 0.0;
+      const double w9m = j >= 2 ? 0.5 * (dzm + dzmm) : 0.0;  // w9(j - 1)
+      W.dz[cc] = dzc;
+      if (fp32) W.dz32[cc] = (float)dzc;
+      if (quick) W.w5[cc] = dzm / (dzm + dzc);
+      W.w9[cc] = w9c;
       W.dbz[cc] = 2.0 / (w9m + w9c);
-      W.dfz[cc] = 2.0 / (w9c + w9l[j < nk ? j + 1 : nk]);
-    }
-    int flags = 0;
-    int cbs = 0;
-    if (wet) {
-      flags |= COL_WET;
-      atomicAdd(&counts[0], 1);
-      // sub-step search over this column's cells to process (:591-661)
-      int nc = 0;
-      bool first = true;
-      for (int j = js; j >= 1; --j) {
-        const int cc = cl[j];
+      W.dfz[cc] = 2.0 / (w9c + w9p);
+      if (j == js0) dz_js0 = dzc;
+      if (j == jn) dz_jn = dzc;
+      if (j == jn - 1) dz_jn1 = dzc;
+      if (j <= jn && ja < 0 && !dzc) ja = j;
+      if (wet && j <= js) {
         nc++;
-        if (O.substep) {
-          int xp = G.xp1[cc], yp = G.yp1[cc], zp = cl[j < nk ? j + 1 : nk];
+        if (substep) {
+          const int xp = G.xp1[cc], yp = G.yp1[cc], zp = cell(j < nk ? j + 1 : nk);
           double d4 = 0.5 * (F.u1[cc] + F.u1[xp]);
           if (fabs(d4) < kMinVal) d4 = kMinVal;
           double d1 = kSF * fabs(G.h1acell[c2] / d4);
@@ -275,41 +272,52 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
           if (fabs(d4) < kMinVal) d4 = kMinVal;
           double d2 = kSF * fabs(G.h2acell[c2] / d4);
           if (d2 < dtmin) dtmin = d2;
-          if (!first) {
+          if (j != js) {
             d4 = 0.5 * (F.w[cc] + F.w[zp]);
             if (fabs(d4) < kMinVal) d4 = kMinVal;
-            double d3 = kSF * fabs(dzl[j] * 1.0 / d4);
+            double d3 = kSF * fabs(dzc * 1.0 / d4);
             if (d3 > 0.0 && d3 < dtmin) dtmin = d3;
           }
         }
-        first = false;
       }
+      w9p = w9c;
+      w9c = w9m;
+      dzc = dzm;
+      dzm = dzmm;
+    }
+    if (jn == 0) dz_jn = dzsed;
+    if (ja < 0) ja = 0;
+    int flags = 0;
+    int cbs = 0;
+    if (wet) {
+      flags |= COL_WET;
+      atomicAdd(&counts[0], 1);
       atomicAdd(&counts[1], nc);
       // tr_bounds thin-surface test (:3250-3252)
-      if (js > 1 && dzl[js0] < O.hmin) {
+      if (js > 1 && dz_js0 < O.hmin) {
         flags |= COL_THIN;
         if (s != top) flags |= COL_SERIAL;
       }
-      // implicit vertical diffusion set-up (:3841-3889) and LU (:4185-4195)
+      // implicit vertical diffusion set-up (:3841-3889) and LU (:4185-4195),
+      // bottom up from the lowest layer of the solve
       int cs = nsur;
-      if (jn <= 1 || !dzl[jn - 1]) {
+      if (jn <= 1 || !dz_jn1) {
         flags |= COL_SINGLE;
-      } else if (any_vdiff && !dzl[jn]) {
+      } else if (any_vdiff && !dz_jn) {
         // zero-thickness surface cell: the reference solves over an empty
         // range and reads stale work memory; report instead of guessing
         flags |= COL_NOSOLVE;
         atomicOr(W.status, ST_GEOM);
       } else if (any_vdiff) {
-        int ja = jn;
-        while (ja > 0 && dzl[ja]) --ja;
         const int jb = ja + 1;  // bottom of the solve
-        cbs = cl[jb];
+        cbs = cell(jb);
         // dzface(c) = 0.5 (dz[zm1] + dz[c]) for c in [cbs, cs]
         double dt = F.dt;
         int cb = cbs;
-        int zpb = cl[jb + 1];
-        double dzf_p = 0.5 * (dzl[jb] + dzl[jb + 1]);
-        double dzdt = dzl[jb] / dt;
+        int zpb = cell(jb + 1);
+        double dzj = W.dz[cb], dzj1 = W.dz[zpb];
+        double dzf_p = 0.5 * (dzj + dzj1);
+        double dzdt = dzj / dt;
         double cp1 = -F.Kz[zpb] / dzf_p;
         double C = dzdt - cp1;
         double div = C;
@@ -319,11 +327,13 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
         W.vd_dzdt[cb] = dzdt;
         if (fp32) W.lu32[cb] = make_float4((float)dzdt, 0.f, (float)(1.0 / div), 0.f);
         double bp1 = cp1;
+        int cc2 = zpb;
         for (int j = jb + 1; j < jn; ++j) {
-          const int cc2 = cl[j], zp = cl[j + 1];
+          const int zp = cell(j + 1);
+          const double dzn = W.dz[zp];
           double dzf_c = dzf_p;
-          dzf_p = 0.5 * (dzl[j] + dzl[j + 1]);
-          dzdt = dzl[j] / dt;
+          dzf_p = 0.5 * (dzj1 + dzn);
+          dzdt = dzj1 / dt;
           double cm1 = -F.Kz[cc2] / dzf_c;
           cp1 = -F.Kz[zp] / dzf_p;
           C = dzdt - cm1 - cp1;
@@ -337,10 +347,12 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
           if (fp32)
             W.lu32[cc2] = make_float4((float)dzdt, (float)cm1, (float)(1.0 / div), (float)ud);
           bp1 = cp1;
+          cc2 = zp;
+          dzj1 = dzn;
         }
         {
           double dzf_c = dzf_p;
-          dzdt = dzl[jn] / dt;
+          dzdt = dz_jn / dt;
           double cm1 = -F.Kz[cs] / dzf_c;
           C = dzdt - cm1;
           double ud = bp1 / div;

@@ -140,17 +140,21 @@ __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2,
 // ---------------------------------------------------------------------------
 // k_adv32
 
-constexpr int kAdvBlock = 256;
+constexpr int kAdvBlock = 256;     // k_adv64
+// k_adv32: 128 threads, 5 blocks per SM (at most 102 registers a thread: 20
+// warps per SM where 256-thread blocks fit 16; measured 13.0 ms against 14.3
+// on stiff2048)
+constexpr int kAdv32Block = 128, kAdv32MinBlocks = 5;
 constexpr int kAdvGroup = 1;       // tracers whose loads a thread issues together
 // dynamic shared memory of k_adv32 with uniform flags: the double-buffered
 // stencil values of a group of tracers per thread
-constexpr size_t kAdvSmem = (size_t)2 * kAdvGroup * 13 * kAdvBlock * sizeof(float);
+constexpr size_t kAdvSmem = (size_t)2 * kAdvGroup * 13 * kAdv32Block * sizeof(float);
 constexpr int kMaxTracers = 256;   // tracers a handle of the FP32-mixed path may carry
 
 // MODE: 0 tracers with their own advect / diffuse flags, 1 every advected
 // tracer advected without horizontal diffusion, 2 advected with it.
 template <bool QUICK, bool ULT, int MODE>
-__global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
+__global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
                                                      SubStep ss, Tile Tl,
                                                      const f32::Face2 *__restrict__ fx2,
                                                      const f32::Face2 *__restrict__ fy2,
@@ -160,10 +164,10 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
   using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ int sTr[kMaxTracers], sTf[kMaxTracers];
-  const int i = blockIdx.x * kAdvBlock + threadIdx.x;
+  const int i = blockIdx.x * kAdv32Block + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const int nz = G.nz;
-  for (int s = threadIdx.x; s < T.ntb; s += kAdvBlock) {
+  for (int s = threadIdx.x; s < T.ntb; s += kAdv32Block) {
     const int n = T.slot_tr[s];
     sTr[s] = n;
     sTf[s] = T.trf[n];
@@ -274,15 +278,15 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
                          vp1,  vp2,  n1.x, n2.x, n1.y, n2.y};
     // the stencil values of the next group of tracers are copied into this
     // thread's slots of a double buffer while the current group is computed
-    extern __shared__ float pf[];  // [2][U][NQ][kAdvBlock]
+    extern __shared__ float pf[];  // [2][U][NQ][kAdv32Block]
     auto issue = [&](int s0, int buf) {
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int s = s0 + u < ntb ? s0 + u : s0;
         const float *tr = tri + (size_t)sTr[s] * G.S;
-        float *d = pf + (buf * U + u) * NQ * kAdvBlock + threadIdx.x;
+        float *d = pf + (buf * U + u) * NQ * kAdv32Block + threadIdx.x;
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) cp_async4(d + q * kAdvBlock, tr + idx[q]);
+        for (int q = 0; q < NQ; ++q) cp_async4(d + q * kAdv32Block, tr + idx[q]);
       }
       cp_async_commit();
     };
@@ -296,19 +300,19 @@ __global__ void __launch_bounds__(kAdvBlock, 2) k_adv32(Geo G, Flow32 F3, Work W
       }
       // tracers are ascending when columns carry different numbers of them
       if (!__any_sync(FULL, on && sTr[s0] < ntc)) continue;
-      const float *P = pf + (g & 1) * U * NQ * kAdvBlock + threadIdx.x;
+      const float *P = pf + (g & 1) * U * NQ * kAdv32Block + threadIdx.x;
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int s = s0 + u;
         if (s >= ntb) break;
-        const float *v = P + u * NQ * kAdvBlock;
+        const float *v = P + u * NQ * kAdv32Block;
         const float t0 = v[0];
-        const float tym1 = v[1 * kAdvBlock], tym2 = v[2 * kAdvBlock];
-        const float typ1 = v[3 * kAdvBlock], typ2 = v[4 * kAdvBlock];
-        const float tm1 = v[5 * kAdvBlock], tm2 = v[6 * kAdvBlock];
-        const float tp1 = v[7 * kAdvBlock], tp2 = v[8 * kAdvBlock];
-        const float txm1 = v[9 * kAdvBlock], txm2 = v[10 * kAdvBlock];
-        const float txp1 = v[11 * kAdvBlock], txp2 = v[12 * kAdvBlock];
+        const float tym1 = v[1 * kAdv32Block], tym2 = v[2 * kAdv32Block];
+        const float typ1 = v[3 * kAdv32Block], typ2 = v[4 * kAdv32Block];
+        const float tm1 = v[5 * kAdv32Block], tm2 = v[6 * kAdv32Block];
+        const float tp1 = v[7 * kAdv32Block], tp2 = v[8 * kAdv32Block];
+        const float txm1 = v[9 * kAdv32Block], txm2 = v[10 * kAdv32Block];
+        const float txp1 = v[11 * kAdv32Block], txp2 = v[12 * kAdv32Block];
         const float Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
         const float Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
         const float Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
