@@ -103,7 +103,7 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       const float df = pq > 0.f ? 2.f * __fdividef(pq, den) : 0.f;
       F = pos ? tm1 + f.wa * df : (neg ? t0 - f.wa * df : 0.f);
     }
-    if (ULT && (f.bits & FB_ULT)) {
+    if (ULT) {
       // ulimate_filter (tracers.c:3526-3554) without its divisions: with
       // s = sign(td - tu) and the normalised variables scaled back by
       // |td - tu|, nc in [0, 1] is 0 <= c <= d, nu > 1 is a > d, nu < nc is
@@ -122,7 +122,9 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       if (a < c) G = tc;
       if (a > d) G = td;
       if (!(c >= 0.f && c <= d)) G = tc;
-      F = G;
+      // computed for every face and selected, so the faces of a cell stay
+      // one straight-line block the compiler can interleave
+      F = (f.bits & FB_ULT) ? G : F;
     }
     F *= f.U;
   }
