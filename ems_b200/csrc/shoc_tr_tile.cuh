@@ -569,31 +569,36 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
     }
   }
   if (solve) {
-    // back substitution (FP32); x(k) replaces s(k).  Then the FP64 residual
+    // back substitution (FP32), x(j) replacing s(j), and in the same pass
+    // down the column the FP64 residual of the row above,
     //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
     // (the difference form of b - A x for A = dzdt I + the diffusion
-    // operator, cp1(j) = cm1(j+1)) replaces a(j), the correction solve runs
-    // on it in FP32 and the update x + d is added in FP64.
-    float x = S0[nk * sa];
+    // operator, cp1(j) = cm1(j+1)), which replaces a(j); the bottom row has
+    // no cm1 term (x(-1) = x(0)), the top row no cp1 term.  The correction
+    // solve runs on r in FP32 and the update x + d is added in FP64.  The
+    // FP64 copies of x and of the factors are carried from row to row, so
+    // each value is converted once.
+    float x1 = S0[nk * sa];      // x(j + 1)
+    float4 l1 = L0[nk * 32];     // factors of row j + 1
+    double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;  // x(j + 1), x(j + 2), cm1(j + 2)
     for (int j = nk - 1; j >= 0; --j) {
-      x = S0[j * sa] - L0[(j + 1) * 32].w * x;
+      const float x = S0[j * sa] - l1.w * x1;
       S0[j * sa] = x;
+      const double xd = (double)x, l1y = (double)l1.y;
+      double r = (double)l1.x * ((double)A0[(j + 1) * sa] - xd1) - l1y * (xd - xd1);
+      if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
+      A0[(j + 1) * sa] = (float)r;
+      x1 = x;
+      xd2 = xd1;
+      xd1 = xd;
+      l2y = l1y;
+      l1 = L0[j * 32];
     }
-    float xm = S0[0], x0 = xm;  // the bottom row has no cm1 term
-    float4 lj = L0[0];
-    for (int j = 0; j < nk; ++j) {
-      const float xp = S0[(j + 1) * sa];
-      const float4 lp = L0[(j + 1) * 32];
-      const double r = (double)lj.x * ((double)A0[j * sa] - (double)x0) -
-                       (double)lj.y * ((double)xm - (double)x0) -
-                       (double)lp.y * ((double)xp - (double)x0);
-      A0[j * sa] = (float)r;
-      xm = x0;
-      x0 = xp;
-      lj = lp;
+    {
+      double r = (double)l1.x * ((double)A0[0] - xd1) - (double)l1.y * (xd1 - xd1);
+      if (nk > 0) r = r - l2y * (xd2 - xd1);
+      A0[0] = (float)r;
     }
-    A0[nk * sa] = (float)((double)lj.x * ((double)A0[nk * sa] - (double)x0) -
-                          (double)lj.y * ((double)xm - (double)x0));
     // correction solve (FP32 forward and back) and update in FP64
     float u = 0.f;
     for (int j = 0; j <= nk; ++j) {
