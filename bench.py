@@ -139,6 +139,33 @@ def max_over_ranks(pg, x, device):
     return float(t.item())
 
 
+def mass_over_ranks(pg, mass, device):
+    """Whole-job mass per tracer: every rank's per-tracer masses are gathered
+    and summed in rank order with Neumaier compensation, so every rank holds
+    the same bits.  The one collective of the multi-GPU path (outside the
+    timed steps); each rank's basin needs no exchange while it steps."""
+    m = np.asarray(mass, np.float64)
+    if pg is None:
+        return m
+    import torch
+    t = torch.tensor(m, dtype=torch.float64, device=device)
+    parts = [torch.empty_like(t) for _ in range(pg.get_world_size())]
+    pg.all_gather(parts, t)
+    return compensated_sum([p.cpu().numpy() for p in parts])
+
+
+def compensated_sum(rows):
+    """Element-wise Neumaier sum of equal-length rows, in row order."""
+    s = np.zeros_like(np.asarray(rows[0], np.float64))
+    c = np.zeros_like(s)
+    for v in rows:
+        v = np.asarray(v, np.float64)
+        u = s + v
+        c += np.where(np.abs(s) >= np.abs(v), (s - u) + v, (v - u) + s)
+        s = u
+    return s + c
+
+
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -209,7 +236,7 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     from ems_b200 import gpu
     step = gpu.TracerStep(case, precision=prec, device=local)
     step.start()
-    m0 = step.mass()
+    m0 = mass_over_ranks(pg, step.mass(), dev)
     stream = torch.cuda.ExternalStream(step.stream(), device=dev)
     step.run(max(args.warmup, 3))
     step.sync()
@@ -235,7 +262,7 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     step.sync()
     parts = [step.kernel_time(p)[0] for p in range(3)]
     step.profile(False)
-    m1 = step.mass()
+    m1 = mass_over_ranks(pg, step.mass(), dev)
     drift = float(np.max(np.abs(m1 - m0) / np.maximum(np.abs(m0), 1e-300)))
     return dict(step=step, ms_step=ms_step, launches=launches, clocks=clk, diag=diag,
                 parts=parts, mass_drift=drift, nsteps=max(args.warmup, 3) + 2 * args.steps)

@@ -38,7 +38,9 @@ def _worker(rank, world, port, q):
     # the reference arm: rank 0 alone times the reference, the others exit
     ref = bench.run_reference(argparse.Namespace(workload="small", cpu_sample="20x14",
                                                  steps=1, warmup=0), r, w)
-    q.put((r, w, t, case.nwet, float(case.tr.sum()), ref is None))
+    # whole-job mass: per-rank masses gathered and summed in rank order
+    m = bench.mass_over_ranks(pg, [0.1 * (r + 1), 2.0 * (r + 1)], "cpu")
+    q.put((r, w, t, case.nwet, float(case.tr.sum()), ref is None, m.tolist()))
     pg.barrier()
     pg.destroy_process_group()
 
@@ -54,8 +56,18 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, w0, t0, n0, s0, none0), (r1, w1, t1, n1, s1, none1) = out
+    (r0, w0, t0, n0, s0, none0, m0), (r1, w1, t1, n1, s1, none1, m1) = out
     assert (r0, r1, w0, w1) == (0, 1, 2, 2)
     assert t0 == t1 == 11.0            # max over ranks
     assert s0 != s1                    # each rank its own seeded basin
     assert none1 and (none0 is False)  # only rank 0 runs the reference arm
+    assert m0 == m1 == [0.1 + 0.2, 6.0]   # the same bits on every rank
+
+
+def test_compensated_sum_of_rank_masses():
+    """The rank-order sum is compensated: 1e16 + 1 - 1e16 keeps the 1 that a
+    plain sum loses."""
+    sys.path.insert(0, ROOT)
+    import bench
+    got = bench.compensated_sum([[1e16, 3.0], [1.0, 4.0], [-1e16, 5.0]])
+    assert got.tolist() == [1.0, 12.0]
