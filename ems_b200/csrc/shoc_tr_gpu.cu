@@ -126,6 +126,21 @@ namespace {
     }                                               \
   } while (0)
 
+// Makes a device current for the scope of one entry point and gives the
+// caller's current device back on the way out, so a host model that drives
+// several devices from one thread keeps its own choice.
+struct DeviceScope {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceScope(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    ok = cudaSetDevice(dev) == cudaSuccess;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 template <class T>
 int dalloc(shoc_tr_gpu *h, T **p, size_t n) {
   void *q = nullptr;
@@ -719,7 +734,7 @@ const char *shoc_tr_gpu_strerror(int st) {
 
 void shoc_tr_gpu_destroy(shoc_tr_gpu *h) {
   if (!h) return;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (int i = 0; i < 2; i++)
     if (h->graph[i]) cudaGraphExecDestroy(h->graph[i]);
@@ -769,7 +784,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
       return r_;              \
     }                         \
   } while (0)
-  if (cudaSetDevice(device) != cudaSuccess) TRY(SHOC_TR_ECUDA);
+  DeviceScope dev_(device);
+  if (!dev_.ok) TRY(SHOC_TR_ECUDA);
   if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     TRY(SHOC_TR_ECUDA);
   const int S = h->S, S2 = h->S2, ncol = h->ncol;
@@ -1472,7 +1488,7 @@ extern "C" {
 
 int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
   if (!h || !tr_wc) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   const size_t S = (size_t)h->S;
   for (int n = 0; n < h->ntr; n++) {
     if (h->esize == sizeof(double)) {
@@ -1492,7 +1508,7 @@ int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
 
 int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc) {
   if (!h || !tr_wc) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   const size_t S = (size_t)h->S;
   for (int n = 0; n < h->ntr; n++) {
     if (h->esize == sizeof(double)) {
@@ -1511,7 +1527,7 @@ int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc) {
 
 int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
   if (!h || !st) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   const size_t S = (size_t)h->S * sizeof(double), S2 = (size_t)h->S2 * sizeof(double);
   cudaStream_t s = h->stream;
   const struct {
@@ -1569,7 +1585,7 @@ int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
 
 int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
   if (!h) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   if (sur_t)
     CK(cudaMemcpyAsync(sur_t + 1, h->W.sur_t, (size_t)h->ncol * sizeof(int),
                        cudaMemcpyDeviceToHost, h->stream));
@@ -1583,7 +1599,7 @@ int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
 int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps) {
   if (!h || nsteps < 0) return SHOC_TR_EARG;
   if (h->dt <= 0.0) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   for (int i = 0; i < nsteps; i++) {
     int rc = step_async(h);
     if (rc) return rc;
@@ -1593,7 +1609,7 @@ int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps) {
 
 int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag) {
   if (!h) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   CK(cudaMemcpyAsync(h->h_status, h->W.status, 4, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(h->h_nwarn, h->W.nwarn, 8, cudaMemcpyDeviceToHost, h->stream));
   CK(cudaMemcpyAsync(h->h_counts, h->d_counts, 8, cudaMemcpyDeviceToHost, h->stream));
@@ -1630,7 +1646,7 @@ int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag) {
   if (!h || !st || !st->tr_wc || st->ntr != h->ntr) return SHOC_TR_EARG;
   for (int n = 0; n < h->ntr; n++)
     if (!st->tr_wc[n]) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   int rc = step_pipelined(h, st);
   if (rc) {
     shoc_tr_gpu_sync(h, nullptr);
@@ -1656,7 +1672,7 @@ int shoc_tr_gpu_host_unregister(void *ptr) {
 
 int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
   if (!h || !mass) return SHOC_TR_EARG;
-  cudaSetDevice(h->device);
+  DeviceScope dev_(h->device);
   const int nb = 148 * 2;
   double *part = nullptr;
   CK(cudaMallocAsync(&part, (size_t)nb * std::max(h->ntr, 1) * sizeof(double), h->stream));
@@ -1691,13 +1707,12 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
 // ---------------------------------------------------------------------------
 // Mass reduction that allocates nothing.
 //
-// For callers that may not allocate device memory while they step: code that
-// runs while a stream is being captured into a CUDA graph (an allocation there
-// would become part of the graph, or fail), and host frameworks that hand all
-// device memory out of their own fixed pool and forbid allocations once the
-// run is going.  The block partials live in the fixed device array below
-// instead of a stream-ordered allocation; the caller passes the (already
-// allocated) handle and a host array for the result.
+// For host frameworks that hand all device memory out of a pool reserved at
+// start-up and forbid any other allocation once the run is going (a coupled
+// model sharing the GPU with other components): shoc_tr_gpu_mass allocates a
+// stream-ordered buffer per call, this one does not.  The block partials live
+// in the fixed device array below; the caller passes the (already allocated)
+// handle and a host array for the result.
 namespace {
 
 constexpr int kNoAllocBlocks = 148 * 2;     // partial sums per tracer
@@ -1725,7 +1740,9 @@ std::mutex g_noalloc_mu;
 double *g_noalloc_ptr[64] = {nullptr};
 
 // Device address of the scratch array for the current device, looked up once
-// per device (the symbol's host-side name is not a device address).
+// per device and kept (the symbol's host-side name is not a device address).
+// A reset of the device (cudaDeviceReset) invalidates the kept address, as it
+// invalidates every handle's device memory.
 int noalloc_scratch(int device, double **out) {
   if (device < 0 || device >= 64) return SHOC_TR_EARG;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1749,7 +1766,8 @@ extern "C" {
 int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass) {
   if (!h || !mass) return SHOC_TR_EARG;
   if (h->ntr > kNoAllocMaxTracers) return SHOC_TR_ESCRATCH;
-  if (cudaSetDevice(h->device) != cudaSuccess) return SHOC_TR_ECUDA;
+  DeviceScope dev_(h->device);
+  if (!dev_.ok) return SHOC_TR_ECUDA;
   double *scr = nullptr;
   int rc = noalloc_scratch(h->device, &scr);
   if (rc) return rc;
@@ -1776,6 +1794,7 @@ void *shoc_tr_gpu_stream(shoc_tr_gpu *h) { return h ? (void *)h->stream : nullpt
 
 int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block) {
   if (!h) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
   if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
   if (tracers_per_block > 0) {
     if (tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;

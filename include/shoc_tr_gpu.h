@@ -101,16 +101,21 @@ int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag);
 int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
 
 /* The same mass reduction, allocating nothing (no counterpart in the
- * reference: an addition of this library).  For callers that must not
- * allocate device memory while they run -- code inside a stream capture, and
- * host frameworks that serve all device memory from their own fixed pool.
- * The per-block partial sums go to a fixed device array of about 152 KB
- * (room for 64 tracers); with more tracers it returns SHOC_TR_ESCRATCH.
- * The first call on a device looks the array's device address up once
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the one array: calls whose GPU work overlaps in time (two
- * handles on different streams, say) race and must be serialised by the
- * caller.  mass[ntr] is host memory; the call waits for the result. */
+ * reference: an addition of this library).  For host frameworks that hand
+ * out all device memory from a pool they reserved at start-up and forbid
+ * any other cudaMalloc once the run is going (a coupled model sharing the
+ * GPU with other components, say): shoc_tr_gpu_mass allocates a small
+ * stream-ordered buffer on every call, this entry point does not.  The
+ * per-block partial sums go to a fixed device array of about 152 KB (room
+ * for 64 tracers) that every device loading the library holds until the
+ * process exits; with more tracers it returns SHOC_TR_ESCRATCH.  The first
+ * call on a device looks the array's device address up once
+ * (cudaGetSymbolAddress) and keeps it, so make that first call before any
+ * stream capture, and do not keep using the library across a reset of the
+ * device (cudaDeviceReset).  All calls share the one array: calls whose GPU
+ * work overlaps in time (two handles on different streams, say) race and
+ * must be serialised by the caller.  mass[ntr] is host memory; the call
+ * copies the sums into it and waits for its stream before returning. */
 int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass);
 
 /* cudaStream_t of the handle, for event timing by the caller. */

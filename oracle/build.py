@@ -7,7 +7,9 @@
                                     reference's OpenMP tracer loop)
 
 The reference libraries are built only where the reference source tree is
-present (REF_ROOT, default /root/reference); elsewhere the prebuilt files
+present: the directory named by the REF_ROOT environment variable or the
+--ref-root argument, else a tree named `reference` beside this repository's
+directory; elsewhere (a machine without the reference) the prebuilt files
 are used as they are.  The reference build uses three stub headers
 (oracle/ref/stub) for netcdf.h / ems_conf.h / svn_rev.h and the no-op link
 stubs in oracle/ref/ref_harness.c.  Flags: -O3 -march=x86-64-v3
@@ -20,7 +22,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("REF_ROOT") or os.path.join(os.path.dirname(ROOT), "reference")
 LIB = os.path.join(HERE, "_lib")
 REF_OUT = os.path.join(HERE, "_ref")
 
@@ -83,5 +85,7 @@ def build_all(force=False):
 
 
 if __name__ == "__main__":
+    if "--ref-root" in sys.argv:
+        REF_ROOT = sys.argv[sys.argv.index("--ref-root") + 1]
     for p in build_all(force="--force" in sys.argv):
         print(p)

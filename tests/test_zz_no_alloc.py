@@ -1,11 +1,13 @@
 """The mass reduction entry point that allocates no device memory.
 
-Some callers cannot allocate device memory while they step: code inside a
-stream capture, and host frameworks that serve all device memory from their
-own fixed pool.  shoc_tr_gpu_mass_noalloc keeps its partial sums in a fixed
-device array instead; it must give what shoc_tr_gpu_mass gives, on repeated
-calls (the array keeps the previous call's contents), and refuse tracer counts
-beyond its fixed capacity.  This file is collected last on purpose.
+Some callers cannot allocate device memory while they step: host frameworks
+that hand out all device memory from a pool reserved at start-up and forbid
+any other allocation during the run.  shoc_tr_gpu_mass_noalloc keeps its
+partial sums in a fixed device array instead; it must give what
+shoc_tr_gpu_mass gives -- bit for bit, since both sum the same block partials
+in the same compensated order -- on repeated calls (the array keeps the
+previous call's contents), and refuse tracer counts beyond its fixed
+capacity.  This file is collected last on purpose.
 """
 import numpy as np
 import pytest
@@ -13,8 +15,6 @@ import pytest
 from ems_b200 import _abi, gpu, synth
 
 pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("need_gpu")]
-
-REL = 1e-12  # the mass tolerance the other tests use
 
 
 @pytest.mark.parametrize("precision", [gpu.FP64, gpu.FP32_MIXED])
@@ -27,7 +27,7 @@ def test_noalloc_mass_matches_allocating_entry_point(precision):
     for _ in range(2):  # two calls in a row: the second reuses the fixed array
         want = t.mass()
         got = t.mass_noalloc()
-        np.testing.assert_allclose(got, want, rtol=REL, atol=0.0)
+        np.testing.assert_array_equal(got, want)
         t.run(1)
         t.sync()
     t.close()
