@@ -19,7 +19,12 @@ ranks.  Rank 0 prints one JSON line.
 
 The reference arm (--impl reference) times the reference's own
 model/hd/tracers/tracers.c (compiled unmodified into oracle/_ref, OpenMP
-tracer loop over all host cores) on a bounded sample of the same workload.
+tracer loop over all host cores) on the same workload window: one untimed
+step, then --steps steps in one call, timed around the step loop alone.  It
+builds the window with the oracle's own build of the window builder
+(oracle/_lib), so that process loads no library of this package.  The
+cpu_baseline of the GPU arm's line is the same reference build on a bounded
+sample (a 512x256 window of the workload, one step).
 """
 import argparse
 import json
@@ -173,49 +178,78 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_sample_case(args, seed):
+def workload_case(args, seed, sample=False):
+    """The arm's window (sample: the bounded CPU sample of it)."""
     from ems_b200 import synth
-    if args.workload in ("batch8", "batch8small"):
-        # the eight basins at 1/16 of their horizontal size
-        return synth.make(args.workload, seed=seed, scale=1.0 / 16)
-    nx, ny = (int(v) for v in args.cpu_sample.split("x"))
-    return synth.make(args.workload, seed=seed, nx=nx, ny=ny)
+    kw = {}
+    if sample:
+        if args.workload in ("batch8", "batch8small"):
+            # the eight basins at 1/16 of their horizontal size
+            return synth.make(args.workload, seed=seed, scale=1.0 / 16)
+        kw["nx"], kw["ny"] = (int(v) for v in args.cpu_sample.split("x"))
+    elif args.size:
+        kw["nx"], kw["ny"] = (int(v) for v in args.size.split("x"))
+    return synth.make(args.workload, seed=seed, **kw)
 
 
-def run_reference(args, rank, world):
-    """The reference's tracers.c (oracle/_ref) on a bounded sample."""
+def reference_time(case, steps, warmup, nthr):
+    """(status, seconds per step) of the reference's tracers.c: `warmup`
+    untimed steps, then `steps` steps in one call timed around its step
+    loop."""
+    import oracle
+    tr, sur, nsur = case.copy_state()
+    if warmup > 0:
+        rc = oracle.run_ref(case, warmup, tr, sur, nsur, nthreads=nthr)[0]
+        if rc:
+            return rc, None
+    rc = oracle.run_ref(case, steps, tr, sur, nsur, nthreads=nthr)[0]
+    return rc, oracle.ref_loop_seconds(nthr) / max(steps, 1)
+
+
+def run_reference(args, rank, world, sample=False):
+    """The reference's tracers.c (oracle/_ref) on the workload window, or on
+    its bounded sample for the cpu_baseline of the GPU arm."""
     import oracle
     if rank != 0:
         return None
     if not oracle.ref_available(omp=True):
         return {"impl": "reference",
                 "unavailable": "reference build oracle/_ref/libshoc_ref_omp.so not present"}
-    case = cpu_sample_case(args, seed=2048)
+    if not sample:
+        # this process builds its window with the oracle's copy of the
+        # window builder and loads nothing of the package's native code
+        from ems_b200 import synth
+        from oracle import build as obuild
+        synth.use_grid_lib(obuild.grid_lib())
+    case = workload_case(args, seed=2048, sample=sample)
     nthr = cpu_threads()
-    tr, sur, nsur = case.copy_state()
-    for _ in range(max(args.warmup, 0) and 1):
-        oracle.run_ref(case, 1, tr, sur, nsur, nthreads=nthr)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        rc = oracle.run_ref(case, 1, tr, sur, nsur, nthreads=nthr)[0]
-        times.append(time.perf_counter() - t0)
-        if rc:
-            return {"impl": "reference", "unavailable": "reference step failed: status %d" % rc}
-    ms = 1000.0 * sum(times) / len(times)
-    value = case.nwet * case.ntr / (ms / 1000.0)
-    size = ("basins at 1/16 size" if args.workload.startswith("batch8") else
-            "%s cells" % args.cpu_sample)
-    sample = ("%s window, %s x %d layers, %d wet cells x %d tracers (every tracer in every "
-              "column), 1 step per measured step" % (args.workload, size, case.win.nz, case.nwet,
-                                                      case.ntr))
+    warm = 1 if args.warmup > 0 else 0  # the CPU path has no caches or clocks to warm
+    rc, sec = reference_time(case, args.steps, warm, nthr)
+    if rc:
+        return {"impl": "reference", "unavailable": "reference step failed: status %d" % rc}
+    ms = 1000.0 * sec
+    units = case.cell_tracers()
+    value = units / sec
+    if sample:
+        size = ("basins at 1/16 size" if args.workload.startswith("batch8") else
+                "%s cells" % args.cpu_sample)
+        desc = ("%s window, %s x %d layers, %d wet cells x %d tracers, %d step(s) timed" %
+                (args.workload, size, case.win.nz, case.nwet, case.ntr, args.steps))
+    else:
+        desc = ("the full %s window (%dx%dx%d, %d wet cells x %d tracers), %d untimed + %d "
+                "timed steps in one call, step loop timed" %
+                (args.workload, case.win.nx, case.win.ny, case.win.nz, case.nwet, case.ntr,
+                 warm, args.steps))
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.workload, "sample": args.cpu_sample},
+            "config": {"workload": args.workload + ("@" + args.size if args.size else ""),
+                       "nx": case.win.nx, "ny": case.win.ny, "nz": case.win.nz,
+                       "tracers": case.ntr, "wet_cells": case.nwet, "cell_tracers": units,
+                       "seed": case.seed, "sample": args.cpu_sample if sample else None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthr, "kind": "reference",
-                             "sample": sample},
+                             "sample": desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
 
@@ -286,10 +320,7 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     mixed = args.precision == "fp32mixed"
-    kw = {}
-    if args.size:
-        kw["nx"], kw["ny"] = (int(v) for v in args.size.split("x"))
-    case = synth.make(args.workload, seed=2048 + rank, **kw)
+    case = workload_case(args, seed=2048 + rank)
     units = case.cell_tracers()
     host_gb = case.ntr * case.win.sgsiz * 8 / 1e9  # one FP64 copy of all tracers
 
@@ -372,7 +403,8 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu:
-        rr = run_reference(argparse.Namespace(**dict(vars(args), steps=1, warmup=0)), 0, 1)
+        rr = run_reference(argparse.Namespace(**dict(vars(args), steps=1, warmup=0)), 0, 1,
+                           sample=True)
         if rr and "value" in rr:
             cpu = rr["cpu_baseline"]
 

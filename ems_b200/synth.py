@@ -60,13 +60,29 @@ class _Grid(C.Structure):
             "botz", "gridz")]
 
 
+_lib_path = None
+
+
+def use_grid_lib(path):
+    """Build windows with the window-builder library at `path` (another build
+    of csrc/shoc_grid.c) instead of the package's own; call before the first
+    window is built."""
+    global _lib_path
+    if _lib is not None and path != _lib_path:
+        raise RuntimeError("the window builder is already loaded from %s" % _lib_path)
+    _lib_path = path
+
+
 def lib():
-    global _lib
+    global _lib, _lib_path
     if _lib is None:
-        from . import _build
-        path = os.path.join(_HERE, "_lib", "libshoc_grid.so")
-        if not os.path.exists(path):
-            _build.grid_lib()
+        path = _lib_path
+        if path is None:
+            from . import _build
+            path = os.path.join(_HERE, "_lib", "libshoc_grid.so")
+            if not os.path.exists(path):
+                _build.grid_lib()
+            _lib_path = path
         L = C.CDLL(path)
         L.shoc_grid_build.argtypes = [C.POINTER(_GridSpec), C.POINTER(_Grid)]
         L.shoc_grid_build.restype = C.c_int

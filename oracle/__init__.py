@@ -42,6 +42,7 @@ def _load(name):
                               C.POINTER(_abi.Opts), C.c_int, C.c_int, C.POINTER(_abi.Diag)]
         L.ref_run.restype = C.c_int
         L.ref_last_message.restype = C.c_char_p
+        L.ref_last_loop_seconds.restype = C.c_double
     _libs[name] = L
     return L
 
@@ -72,6 +73,13 @@ def run_ref(case, nsteps, tr=None, sur=None, nsur=None, nthreads=1):
     if L is None:
         raise FileNotFoundError("reference build oracle/_ref not available")
     return _call(L.ref_run, case, nsteps, tr, sur, nsur, C.c_int(int(nthreads)))
+
+
+def ref_loop_seconds(nthreads=1):
+    """Wall time of the step loop of the last run_ref (its window set-up,
+    the copy of the caller's arrays into SHOC's structs, excluded)."""
+    L = _load("ref_omp" if nthreads > 1 else "ref")
+    return float(L.ref_last_loop_seconds())
 
 
 def max_rel_err(a, b, cells, floor=1e-300):

@@ -1,6 +1,9 @@
 """Builds the CPU checkers (TEST INFRASTRUCTURE ONLY).
 
   oracle/_lib/liboracle.so          the C restatement in oracle/shoc_oracle.c
+  oracle/_lib/libshoc_grid.so       the window builder (ems_b200/csrc/shoc_grid.c)
+                                    compiled for the reference arm of bench.py,
+                                    so that arm loads no library of the product
   oracle/_ref/libshoc_ref.so        the reference's own model/hd/tracers/tracers.c,
                                     compiled unmodified, single thread
   oracle/_ref/libshoc_ref_omp.so    the same with -fopenmp -DHAVE_OMP (the
@@ -54,6 +57,19 @@ def oracle_lib(force=False):
     return out
 
 
+def grid_lib(force=False):
+    """The synthetic-window builder for the CPU checkers' own use."""
+    os.makedirs(LIB, exist_ok=True)
+    out = os.path.join(LIB, "libshoc_grid.so")
+    csrc = os.path.join(ROOT, "ems_b200", "csrc")
+    src = os.path.join(csrc, "shoc_grid.c")
+    deps = [src, os.path.join(csrc, "shoc_grid.h"), os.path.join(ROOT, "include", "shoc_tr.h")]
+    if force or _stale(out, deps):
+        _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-fopenmp", "-I",
+              os.path.join(ROOT, "include"), "-I", csrc, "-o", out, src])
+    return out
+
+
 def ref_available():
     return os.path.exists(os.path.join(REF_ROOT, "model", "hd", "tracers", "tracers.c"))
 
@@ -79,7 +95,7 @@ def ref_libs(force=False):
 
 
 def build_all(force=False):
-    out = [oracle_lib(force)]
+    out = [oracle_lib(force), grid_lib(force)]
     out += ref_libs(force)
     return out
 

@@ -19,7 +19,11 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 #include "hd.h"
+#if defined(HAVE_OMP)
+#include <omp.h>
+#endif
 #include "shoc_tr.h"
 
 /* ---- globals the reference file expects (globals.h:71-76) ---- */
@@ -58,6 +62,15 @@ void hd_warn(const char *s, ...) {
   }
 }
 const char *ref_last_message(void) { return ref_msg; }
+
+/* wall time of the last ref_run's step loop (window set-up excluded) */
+static double ref_loop_seconds = 0.0;
+double ref_last_loop_seconds(void) { return ref_loop_seconds; }
+static double ref_now(void) {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
 
 /* ---- allocation (emsalloc.h) ---- */
 double *d_alloc_1d(int n1) { return (double *)calloc((size_t)(n1 > 0 ? n1 : 1), sizeof(double)); }
@@ -160,6 +173,9 @@ static ref_window *ref_make(const shoc_tr_geom *g, shoc_tr_state *st,
   if (!master) master = (master_t *)calloc(1, sizeof(master_t));
 #if defined(HAVE_OMP)
   master->trans_num_omp = nthreads;
+  /* the tracer loop's work arrays exist for nthreads threads: run that many,
+   * as SHOC's driver does (model/hd/control/dp.c:155) */
+  omp_set_num_threads(nthreads > 1 ? nthreads : 1);
 #endif
 
   /* geometry_t */
@@ -287,6 +303,7 @@ int ref_run(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
     return rc;
   }
   ref_jmp_armed = 1;
+  const double t0 = ref_now();
   for (int s = 0; s < nsteps; s++) {
     set_lateral_BC_tr(d->tr_wc, d->ntr, w->nbpt, w->bpt, w->bin);
     set_dz(w, d, c);
@@ -298,6 +315,7 @@ int ref_run(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
     d->nstep++;
     d->t += d->dt;
   }
+  ref_loop_seconds = ref_now() - t0;
   ref_jmp_armed = 0;
   if (diag) {
     diag->nwarn = ref_nwarn;

@@ -1,9 +1,11 @@
 """bench.py's reference arm on CPU: the JSON line the driver reads.
 
 `bench.py --impl reference` times the reference's own tracers.c (compiled
-unmodified into oracle/_ref) on a bounded sample of the workload and prints
-one JSON line with the contract's keys; these tests run it as the driver
-does, in a subprocess, on small samples.
+unmodified into oracle/_ref) on the workload window and prints one JSON line
+with the contract's keys; these tests run it as the driver does, in a
+subprocess, on small windows of the workloads (--size, and the multi-basin
+batch at 1/16 size).  The process builds its window with the oracle's build
+of the window builder and loads no library of the package.
 """
 import json
 import os
@@ -42,14 +44,26 @@ def check_line(d, workload):
 
 
 def test_reference_arm_line():
-    d = run_bench("--workload", "stiff2048", "--cpu-sample", "64x32", "--steps", "2",
-                  "--warmup", "1")
-    check_line(d, "stiff2048")
-    assert d["steps"] == 2 and "64x32" in d["cpu_baseline"]["sample"]
+    d = run_bench("--workload", "stiff2048", "--size", "96x64", "--steps", "2", "--warmup", "1")
+    check_line(d, "stiff2048@96x64")
+    assert d["steps"] == 2 and "full stiff2048 window (96x64x50" in d["cpu_baseline"]["sample"]
+    assert d["config"]["wet_cells"] > 0 and d["config"]["tracers"] == 24
 
 
-def test_reference_arm_multi_basin_sample():
-    """The multi-basin workload's sample is the eight basins at 1/16 size."""
-    d = run_bench("--workload", "batch8", "--steps", "1", "--warmup", "0")
-    check_line(d, "batch8")
-    assert "1/16" in d["cpu_baseline"]["sample"]
+def test_reference_arm_multi_basin():
+    d = run_bench("--workload", "batch8small", "--steps", "1", "--warmup", "0")
+    check_line(d, "batch8small")
+    assert d["config"]["cell_tracers"] < d["config"]["wet_cells"] * d["config"]["tracers"]
+
+
+def test_reference_arm_loads_no_package_library():
+    """The reference arm's process maps only oracle/ libraries of this
+    repository (the window builder included)."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', "
+            "'small', '--steps', '1', '--warmup', '0']; runpy.run_path('bench.py', "
+            "run_name='__main__'); print(open('/proc/self/maps').read())")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    libs = {l.split()[-1] for l in r.stdout.splitlines() if l.endswith(".so") and ROOT in l}
+    assert libs and all(os.sep + "oracle" + os.sep in p for p in libs), libs
