@@ -270,7 +270,8 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     from ems_b200 import gpu
     step = gpu.TracerStep(case, precision=prec, device=local)
     step.start()
-    m0 = mass_over_ranks(pg, step.mass(), dev)
+    own0 = step.mass()
+    m0 = mass_over_ranks(pg, own0, dev)
     stream = torch.cuda.ExternalStream(step.stream(), device=dev)
     step.run(max(args.warmup, 3))
     step.sync()
@@ -296,10 +297,15 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     step.sync()
     parts = [step.kernel_time(p)[0] for p in range(3)]
     step.profile(False)
-    m1 = mass_over_ranks(pg, step.mass(), dev)
+    own1 = step.mass()
+    m1 = mass_over_ranks(pg, own1, dev)
     drift = float(np.max(np.abs(m1 - m0) / np.maximum(np.abs(m0), 1e-300)))
+    # the largest drift of any one rank's basin (a gain on one rank and a
+    # loss on another could cancel in the whole-job figure)
+    own = float(np.max(np.abs(own1 - own0) / np.maximum(np.abs(own0), 1e-300)))
     return dict(step=step, ms_step=ms_step, launches=launches, clocks=clk, diag=diag,
-                parts=parts, mass_drift=drift, nsteps=max(args.warmup, 3) + 2 * args.steps)
+                parts=parts, mass_drift=drift, mass_drift_rank_max=max_over_ranks(pg, own, dev),
+                nsteps=max(args.warmup, 3) + 2 * args.steps)
 
 
 def main():
@@ -332,25 +338,29 @@ def main():
     fp64 = None
     if mixed and not args.no_fp64:
         ref = time_arm(case, gpu.FP64, local, args, pg, dev)
-        err = [None]
-        if host_gb <= 16.0:  # the comparison holds both results on the host
-            t32, t64 = step.download(), ref["step"].download()
-            wet = case.win.wet_cells()
-            if case.ntr2d is None:
-                sel = [wet] * case.ntr
-            else:
-                nt = case.ntr2d[case.win.m2d[wet]]
-                sel = [wet[nt > n] for n in range(case.ntr)]
-            err = [float(np.max(np.abs(t32[n, c] - t64[n, c])) /
-                         max(float(np.max(np.abs(t64[n, c]))), 1e-300))
-                   for n, c in enumerate(sel) if len(c)]
-            del t32, t64
+        # both precisions have stepped the same inputs the same number of
+        # steps: per tracer (and basin) max |x32 - x64| / max |x64|, on the device
+        basins = getattr(case, "basins", None)
+        if basins:
+            d = step.compare(ref["step"], region=case.basin2d, nregion=len(basins))
+            per = [[float(v) for v in d["max_rel"][b, :T]] for b, (_, _, _, T) in
+                   enumerate(basins)]
+            err = max(max(r) for r in per)
+            rms = max(float(v) for b, (_, _, _, T) in enumerate(basins)
+                      for v in d["rms_rel"][b, :T])
+        else:
+            d = step.compare(ref["step"])
+            per = [float(v) for v in d["max_rel"][0]]
+            err = max(per)
+            rms = float(np.nanmax(d["rms_rel"][0]))
+        err = max_over_ranks(pg, err, dev)
         fp64 = {"value": units * world / (ref["ms_step"] / 1000.0),
                 "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
                 "kernels_ms": {"k_adv64": ref["parts"][1], "k_vd64": ref["parts"][2]},
                 "mass_rel_drift": ref["mass_drift"],
                 "speedup_fp32mixed": ref["ms_step"] / arm["ms_step"],
-                "max_rel_err_fp32mixed": max(err) if err[0] is not None else None,
+                "max_rel_err_fp32mixed": err, "max_rms_rel_err_fp32mixed": rms,
+                ("max_rel_err_per_basin" if basins else "max_rel_err_per_tracer"): per,
                 "steps_compared": arm["nsteps"]}
         ref["step"].close()
 
@@ -426,6 +436,7 @@ def main():
         },
         "fp64": fp64,
         "mass_rel_drift": arm["mass_drift"],
+        "mass_rel_drift_rank_max": arm["mass_drift_rank_max"],
         "clocks": arm["clocks"],
         "e2e": {"value": units / e2e_s if e2e_s == e2e_s else None, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -23,8 +23,8 @@ from . import gpu, synth
 
 
 def compare(case, steps, every, device=0, log=None):
-    """Per-tracer errors of FP32-mixed vs FP64 after every `every` steps."""
-    wet = case.win.wet_cells()
+    """Per-tracer errors of FP32-mixed vs FP64 after every `every` steps
+    (compared on the device, shoc_tr_gpu_compare: no tracer leaves HBM)."""
     s64 = gpu.TracerStep(case, precision=gpu.FP64, device=device)
     s32 = gpu.TracerStep(case, precision=gpu.FP32_MIXED, device=device)
     s64.start()
@@ -39,11 +39,9 @@ def compare(case, steps, every, device=0, log=None):
         s64.sync()
         s32.sync()
         done += k
-        a = s64.download()[:, wet]
-        b = s32.download()[:, wet]
-        d = b - a
-        mx = np.max(np.abs(d), axis=1) / np.maximum(np.max(np.abs(a), axis=1), 1e-300)
-        rms = np.sqrt(np.sum(d * d, axis=1) / np.maximum(np.sum(a * a, axis=1), 1e-300))
+        d = s32.compare(s64)
+        mx = d["max_abs"][0] / np.maximum(d["max_ref"][0], 1e-300)
+        rms = np.sqrt(d["sumsq_diff"][0] / np.maximum(d["sumsq_ref"][0], 1e-300))
         m64, m32 = s64.mass(), s32.mass()
         row = {"step": done,
                "max_rel": mx.tolist(), "rms_rel": rms.tolist(),

@@ -521,6 +521,40 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
   }
 }
 
+// Differences between the tracers of two handles of one window: one thread
+// per (column, tracer) over the column's wet cells (bottom to top layer), for
+// the tracers both handles carry in the column.  Per (region, tracer): the
+// largest |a - b| and |b| (atomicMax on the bits of a non-negative double,
+// which order as unsigned integers) and the sums of (a - b)^2 and b^2.
+template <class TA, class TB>
+__global__ void k_compare(Geo G, Tile Tl, const int *colntr_b, const TA *ta, const TB *tb,
+                          const int *region, int nreg, unsigned long long *maxabs,
+                          unsigned long long *maxref, double *ssd, double *ssr) {
+  const int n = blockIdx.y;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
+       col += gridDim.x * blockDim.x) {
+    if (n >= G.colntr[col] || n >= colntr_b[col]) continue;
+    const int r = region ? region[col] : 0;
+    if (r < 0 || r >= nreg) continue;
+    double ma = 0.0, mr = 0.0, sd = 0.0, sr = 0.0;
+    for (int k = G.col_kb[col]; k < G.nz; ++k) {
+      const int c = Tl.cellk[(size_t)k * Tl.ncolp + col];
+      if (!c) continue;
+      const double a = (double)ta[(size_t)n * G.S + c], b = (double)tb[(size_t)n * G.S + c];
+      const double d = a - b;
+      ma = fmax(ma, fabs(d));
+      mr = fmax(mr, fabs(b));
+      sd += d * d;
+      sr += b * b;
+    }
+    const size_t o = (size_t)r * gridDim.y + n;
+    atomicMax(&maxabs[o], (unsigned long long)__double_as_longlong(ma));
+    atomicMax(&maxref[o], (unsigned long long)__double_as_longlong(mr));
+    atomicAdd(&ssd[o], sd);
+    atomicAdd(&ssr[o], sr);
+  }
+}
+
 // shared memory of the column kernel of the handle's precision
 size_t vd_smem(const shoc_tr_gpu *h, int nd, int nw) {
   return h->esize == sizeof(float) ? vd32_smem(nd, nw) : vd64_smem(nd, nw);
@@ -1787,6 +1821,76 @@ int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass) {
   CK(cudaMemcpyAsync(mass, sums, (size_t)h->ntr * sizeof(double), cudaMemcpyDeviceToHost,
                      h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_compare(shoc_tr_gpu *a, shoc_tr_gpu *b, const int *region, int nregion,
+                        double *maxabs, double *maxref, double *sumsq_diff, double *sumsq_ref) {
+  if (!a || !b || !maxabs || !maxref || !sumsq_diff || !sumsq_ref) return SHOC_TR_EARG;
+  if (nregion < 1 || (!region && nregion != 1)) return SHOC_TR_EARG;
+  if (a->device != b->device || a->S != b->S || a->S2 != b->S2 || a->ncol != b->ncol ||
+      a->ntr != b->ntr || a->nz != b->nz)
+    return SHOC_TR_EARG;
+  DeviceScope dev_(a->device);
+  const int ntr = a->ntr;
+  const size_t nout = (size_t)nregion * ntr;
+  if (nout == 0) return SHOC_TR_OK;
+  // both handles' work so far, then the comparison on a's stream
+  cudaEvent_t ev;
+  CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(ev, b->stream));
+  CK(cudaStreamWaitEvent(a->stream, ev, 0));
+  cudaEventDestroy(ev);
+  cudaStream_t st = a->stream;
+  // per column region ids (region is indexed by 2D cell, as SHOC's 2D arrays)
+  char *buf = nullptr;
+  const size_t bytes = nout * 4 * sizeof(double) + (region ? (size_t)a->ncol * sizeof(int) : 0);
+  CK(cudaMallocAsync((void **)&buf, bytes, st));
+  unsigned long long *dmax = (unsigned long long *)buf, *dref = dmax + nout;
+  double *dsd = (double *)(dref + nout), *dsr = dsd + nout;
+  int *dreg = nullptr;
+  CK(cudaMemsetAsync(buf, 0, nout * 4 * sizeof(double), st));
+  std::vector<int> hcol;
+  if (region) {
+    std::vector<int> top(a->ncol);
+    CK(cudaMemcpyAsync(top.data(), a->G.col_top, (size_t)a->ncol * sizeof(int),
+                       cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    hcol.resize(a->ncol);
+    for (int c = 0; c < a->ncol; c++) hcol[c] = region[top[c]];
+    dreg = (int *)(dsr + nout);
+    CK(cudaMemcpyAsync(dreg, hcol.data(), (size_t)a->ncol * sizeof(int),
+                       cudaMemcpyHostToDevice, st));
+  }
+  const dim3 grid(148 * 2, ntr);
+  const bool fa = a->esize == sizeof(float), fb = b->esize == sizeof(float);
+  const void *ta = a->tr[a->cur], *tb = b->tr[b->cur];
+  if (fa && fb)
+    k_compare<float, float><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const float *)ta,
+                                                 (const float *)tb, dreg, nregion, dmax, dref,
+                                                 dsd, dsr);
+  else if (fa)
+    k_compare<float, double><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const float *)ta,
+                                                  (const double *)tb, dreg, nregion, dmax,
+                                                  dref, dsd, dsr);
+  else if (fb)
+    k_compare<double, float><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const double *)ta,
+                                                  (const float *)tb, dreg, nregion, dmax, dref,
+                                                  dsd, dsr);
+  else
+    k_compare<double, double><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr,
+                                                   (const double *)ta, (const double *)tb, dreg,
+                                                   nregion, dmax, dref, dsd, dsr);
+  a->launches++;
+  CK(cudaGetLastError());
+  std::vector<double> out(nout * 4);
+  CK(cudaMemcpyAsync(out.data(), buf, nout * 4 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaFreeAsync(buf, st));
+  CK(cudaStreamSynchronize(st));
+  memcpy(maxabs, out.data(), nout * sizeof(double));
+  memcpy(maxref, out.data() + nout, nout * sizeof(double));
+  memcpy(sumsq_diff, out.data() + 2 * nout, nout * sizeof(double));
+  memcpy(sumsq_ref, out.data() + 3 * nout, nout * sizeof(double));
   return SHOC_TR_OK;
 }
 

@@ -22,7 +22,7 @@ EXPORTS = (
     "shoc_tr_gpu_create", "shoc_tr_gpu_destroy", "shoc_tr_gpu_step",
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
-    "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
+    "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_compare", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
@@ -55,6 +55,7 @@ def lib(path=None):
     L.shoc_tr_gpu_sync.argtypes = [H, C.POINTER(_abi.Diag)]
     L.shoc_tr_gpu_mass.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_compare.argtypes = [H, H, _abi.IP, C.c_int] + [_abi.DP] * 4
     L.shoc_tr_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
     L.shoc_tr_gpu_host_unregister.argtypes = [C.c_void_p]
     L.shoc_tr_gpu_stream.argtypes = [H]
@@ -204,6 +205,25 @@ class TracerStep:
         m = np.zeros(self.case.ntr)
         _check("mass_noalloc", self.L.shoc_tr_gpu_mass_noalloc(self.h, _abi.dptr(m)))
         return m
+
+    def compare(self, ref, region=None, nregion=1):
+        """Differences to another handle of the same window (on the device):
+        dict of per-(region, tracer) arrays max_abs, max_ref, sumsq_diff,
+        sumsq_ref, and the derived max_rel = max_abs / max_ref and rms_rel =
+        sqrt(sumsq_diff / sumsq_ref).  region: int32 [sgsizS] 2D cell ->
+        region id (None: the whole window)."""
+        if region is not None:
+            region = np.ascontiguousarray(region, np.int32)
+        shape = (nregion, self.case.ntr)
+        out = [np.zeros(shape) for _ in range(4)]
+        _check("compare", self.L.shoc_tr_gpu_compare(self.h, ref.h, _abi.iptr(region), nregion,
+                                                     *[_abi.dptr(o) for o in out]))
+        d = dict(zip(("max_abs", "max_ref", "sumsq_diff", "sumsq_ref"), out))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            d["max_rel"] = np.where(d["max_ref"] > 0, d["max_abs"] / d["max_ref"], np.nan)
+            d["rms_rel"] = np.where(d["sumsq_ref"] > 0, np.sqrt(d["sumsq_diff"] / d["sumsq_ref"]),
+                                    np.nan)
+        return d
 
     def stream(self):
         return self.L.shoc_tr_gpu_stream(self.h)

@@ -485,6 +485,15 @@ def build_batch(name, basins, *, seed, scale=1.0, gap=3, nz=60, depth=250.0, **k
     ntr2d[c2[ok][inb]] = tr_of[j[inb], i[inb]]
     case.ntr2d = ntr2d
     case.basins = dims
+    # basin of every 2D cell (-1: land between the basins)
+    bid = np.full((ny, nx), -1, np.int32)
+    x0 = gap
+    for b, (bx, by, L, T) in enumerate(dims):
+        bid[gap:gap + by, x0:x0 + bx] = b
+        x0 += bx + gap
+    basin2d = np.full(win.sgsizS, -1, np.int32)
+    basin2d[c2[ok][inb]] = bid[j[inb], i[inb]]
+    case.basin2d = basin2d
     return case
 
 

@@ -118,6 +118,18 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
  * copies the sums into it and waits for its stream before returning. */
 int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass);
 
+/* Differences between the current tracers of two handles of the same window
+ * on the same device, in either precision (the FP32-mixed path against the
+ * plain FP64 one, say), computed on the device.  Over the wet cells of every
+ * column that carries the tracer in both handles: the largest |a - b|, the
+ * largest |b|, sum (a - b)^2 and sum b^2 per tracer -- per region when
+ * region[sgsizS] (SHOC 2D cell -> region 0..nregion-1, < 0: left out) is
+ * given, else over the whole window (nregion 1).  Outputs [nregion][ntr].
+ * Waits for both handles' streams.  No reference counterpart: the accuracy
+ * measurement of this library. */
+int shoc_tr_gpu_compare(shoc_tr_gpu *a, shoc_tr_gpu *b, const int *region, int nregion,
+                        double *maxabs, double *maxref, double *sumsq_diff, double *sumsq_ref);
+
 /* cudaStream_t of the handle, for event timing by the caller. */
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
 
