@@ -215,10 +215,11 @@ def run_reference(args, rank, world, sample=False):
     if not oracle.ref_available(omp=True):
         return {"impl": "reference",
                 "unavailable": "reference build oracle/_ref/libshoc_ref_omp.so not present"}
-    if not sample:
-        # this process builds its window with the oracle's copy of the
-        # window builder and loads nothing of the package's native code
-        from ems_b200 import synth
+    from ems_b200 import synth
+    if not sample and synth._lib is None:
+        # this process (the reference arm) builds its window with the
+        # oracle's copy of the window builder and loads nothing of the
+        # package's native code
         from oracle import build as obuild
         synth.use_grid_lib(obuild.grid_lib())
     case = workload_case(args, seed=2048, sample=sample)
