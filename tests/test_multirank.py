@@ -37,7 +37,7 @@ def _worker(rank, world, port, q):
     case = synth.make("small", seed=2048 + r)
     # the reference arm: rank 0 alone times the reference, the others exit
     ref = bench.run_reference(argparse.Namespace(workload="small", cpu_sample="20x14",
-                                                 steps=1, warmup=0), r, w)
+                                                 size="", steps=1, warmup=0), r, w)
     # whole-job mass: per-rank masses gathered and summed in rank order
     m = bench.mass_over_ranks(pg, [0.1 * (r + 1), 2.0 * (r + 1)], "cpu")
     q.put((r, w, t, case.nwet, float(case.tr.sum()), ref is None, m.tolist()))
