@@ -19,7 +19,7 @@ GRID_SRC = ["shoc_grid.c"]
 # (source, FMA contraction): the FP64 reference path must not contract
 GPU_SRC = [("shoc_tr_gpu.cu", False), ("shoc_tr_f32.cu", True)]
 GPU_HDR = ["shoc_tr_kernels.cuh", "shoc_tr_stage.cuh", "shoc_tr_tile.cuh", "shoc_tr_tile64.cuh",
-           "shoc_tr_launch.h"]
+           "shoc_tr_fused.cuh", "shoc_tr_launch.h"]
 
 NVCC_ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -85,4 +85,58 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
   if (ev) cudaEventRecord(ev[2], st);
 }
 
+namespace {
+template <bool Q, bool U, bool L>
+void step32(int grid, cudaStream_t st, size_t smem, const Geo &G, const Flow &F, const Flow32 &F3,
+            const Work &W, const Opt &O, const TrSet &T, const SubStep &ss, const Tile &Tl,
+            const Fused &Fu, const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin,
+            float *tout, int hd) {
+  k_step32<Q, U, L><<<grid, kFusedThreads, smem, st>>>(G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2,
+                                                        tin, tout, hd, 0);
+}
+template <bool Q, bool U>
+void step32_last(bool last, int grid, cudaStream_t st, size_t smem, const Geo &G, const Flow &F,
+                 const Flow32 &F3, const Work &W, const Opt &O, const TrSet &T,
+                 const SubStep &ss, const Tile &Tl, const Fused &Fu, const f32::Face2 *fx2,
+                 const f32::Face2 *fy2, const float *tin, float *tout, int hd) {
+  if (last)
+    step32<Q, U, true>(grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin, tout, hd);
+  else
+    step32<Q, U, false>(grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin, tout, hd);
+}
+}  // namespace
+
+cudaError_t fused32_set_smem_attr(int bytes) {
+  cudaError_t e = cudaSuccess;
+  const cudaError_t r[8] = {
+      attr(k_step32<true, true, true>, bytes),   attr(k_step32<true, true, false>, bytes),
+      attr(k_step32<true, false, true>, bytes),  attr(k_step32<true, false, false>, bytes),
+      attr(k_step32<false, true, true>, bytes),  attr(k_step32<false, true, false>, bytes),
+      attr(k_step32<false, false, true>, bytes), attr(k_step32<false, false, false>, bytes)};
+  for (auto x : r)
+    if (x != cudaSuccess) e = x;
+  return e;
+}
+
+void fused32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo &G,
+                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
+                     const TrSet &T, const SubStep &ss, const Tile &Tl, const Fused &Fu,
+                     const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin, float *tout,
+                     int any_hd, size_t smem) {
+  const int grid = Fu.ntile;
+  if (grid <= 0) return;
+  if (quick && ult)
+    step32_last<true, true>(last, grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin,
+                            tout, any_hd);
+  else if (quick)
+    step32_last<true, false>(last, grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin,
+                             tout, any_hd);
+  else if (ult)
+    step32_last<false, true>(last, grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin,
+                             tout, any_hd);
+  else
+    step32_last<false, false>(last, grid, st, smem, G, F, F3, W, O, T, ss, Tl, Fu, fx2, fy2, tin,
+                              tout, any_hd);
+}
+
 }  // namespace shoc

@@ -1,0 +1,598 @@
+// shoc_tr_fused.cuh -- the FP32-mixed transport sub-step as ONE kernel per
+// sub-step: advection and horizontal diffusion (advect_diffuse, tracers.c:
+// 849-925), tr_bounds (:3217-3324), surf_conc (:3047-3207) and, on the last
+// sub-step, the implicit vertical diffusion (vert_diffuse_3d /
+// implicit_vdiff_tr, :3893-3953, :4067-4214) of a tile of 8 x 4 water columns
+// over all its layers and tracers, with an FP64 per-column mass carry.
+//
+// A block owns one tile (lane = column: lane = 8 * iy + ix for the columns at
+// (i0 + ix, j0 + iy)) and runs two phases:
+//
+//  A  advection, layer chunk by layer chunk from the top down: warp w holds
+//     layer k0 - w of the chunk, so a thread holds one cell and folds its
+//     tracer-independent face coefficients once, then loops over the
+//     advected tracers two at a time.  Of a cell's six face fluxes it
+//     computes the west, south and bottom ones; the east and north fluxes are
+//     the west / south fluxes of the lanes at ix + 1 / iy + 1 (shuffles) and
+//     the top flux is the bottom flux of the warp above (shared memory) --
+//     each computed by the cell itself where that neighbour is not in the
+//     tile.  The flux divergence and the interior update are FP64; the new
+//     value of every cell below the surface goes to the output array (FP32),
+//     while per (column, tracer) the exact FP64 mass of those values (the sum
+//     of a * dz), the FP64 divergence of the surface cell and the cells above
+//     it, and the surface cell's bottom-face flux are accumulated in shared
+//     memory in a fixed order (results do not depend on the schedule).
+//  B  one thread per (column, tracer): tr_bounds, surf_conc's column-mass
+//     balance (FP64), the copy above the surface and, on the last sub-step,
+//     the FP32 Thomas sweep with an FP64 residual and one FP32 correction
+//     solve, as k_vd32 (shoc_tr_tile.cuh) does.  The column's values come back
+//     from the output array, written a few microseconds earlier by phase A of
+//     the same block (an L2 round trip, not an HBM one); the LU factors were
+//     copied into shared memory while phase A ran.
+//
+// Mass carry.  Storing FP32 values loses mass at every rounding (and the
+// FP32 solve conserves the column mass only to its residual).  Per (tracer,
+// column) the kernel keeps, in FP64, the mass the stored values owe the
+// column: carry' = carry + M_exact - M_stored, where M_exact is the FP64 mass
+// the step computed (the exact advected values, the surf_conc surface value,
+// tr_bounds' clipping) and M_stored the mass of what was stored.  The carry
+// goes back into the column at the next sub-step (into the surface row of
+// the solve's FP64 residual, or into the surface value when nothing is
+// solved), so the stored values plus the carry conserve mass to FP64
+// round-off and the carry stays within a few FP32 ulps of the column mass.
+// The mass diagnostic adds it.  Columns whose surface moves during the step
+// (eta != oldeta) keep their carry as it is.
+#pragma once
+#include "shoc_tr_tile.cuh"
+
+namespace shoc {
+
+constexpr int kFusedThreads = 256;  // 8 warps: one layer of the chunk per warp in phase A
+constexpr int kFusedWarps = kFusedThreads / 32;
+constexpr int kFusedMaxTracers = 64;  // advected tracers the fused kernel's accumulators hold
+
+struct Fused {
+  const int *tcol;    // [ntile][32] column of each lane of each tile (-1: none)
+  const int *tkmin;   // [ntile] lowest layer of the tile's columns
+  int ntile;
+  double *carry;      // [ntr][ncol] FP64 mass the stored values owe each column
+  int nwb;            // warps of phase B (tracers in flight per tile)
+};
+
+// shared memory of k_step32 (bytes) for columns of at most nd layers, nwb
+// phase-B warps and ntb advected tracers
+inline size_t fused_smem(int nd, int nwb, int ntb) {
+  return (size_t)nd * 32 * 16                   // LU factors float4 [nd][32]
+         + (size_t)nd * 32 * 4                  // cells int [nd][32]
+         + (size_t)2 * nwb * nd * 32 * 4        // A, S float [nwb][nd][32]
+         + (size_t)kFusedWarps * 32 * 8         // bottom fluxes float2 [8][32]
+         + (size_t)kFusedWarps * 4 * 32 * 8     // reduction double [8][2][2][32]
+         + (size_t)ntb * 32 * (8 + 8 + 4);      // accumulators per (tracer, lane)
+}
+
+namespace f32x {
+
+using f32::Face;
+using f32::Face2;
+using f32::FB_NEG;
+using f32::FB_POS;
+using f32::FB_ULT;
+
+// Face weights (as f32::set_face) with every rounding explicit, so two
+// threads folding the same face from the same inputs get the same bits: a
+// cell's east (north) face, computed where the neighbour is not in the tile,
+// equals the neighbour's own west (south) face, and no mass is created
+// between them.
+__device__ __forceinline__ void fold_face(Face &f, bool quick, float cr, float d, float Ap,
+                                          float Bp, float Am, float Bm, float U, bool ult,
+                                          float K) {
+  f.bits = (cr > 0.f ? FB_POS : 0) | (cr < 0.f ? FB_NEG : 0) | ((ult && cr != 0.f) ? FB_ULT : 0);
+  if (quick) {
+    const float a = __fmaf_rn(-0.5f, cr, d);
+    const float b = __fmul_rn(__fmaf_rn(-cr, cr, 1.f), 1.f / 6.f);
+    if (cr > 0.f) {
+      f.wa = __fmul_rn(-b, Bp);
+      f.w1 = __fmaf_rn(2.f, b, __fsub_rn(1.f, a));
+      f.w2 = __fmaf_rn(-b, Ap, a);
+    } else if (cr < 0.f) {
+      f.wa = __fmul_rn(-b, Am);
+      f.w1 = __fmaf_rn(-b, Bm, __fsub_rn(1.f, a));
+      f.w2 = __fmaf_rn(2.f, b, a);
+    } else {
+      f.wa = 0.f;
+      f.w1 = __fsub_rn(1.f, d);
+      f.w2 = d;
+    }
+  } else {
+    f.wa = cr > 0.f ? __fmul_rn(0.5f, __fsub_rn(1.f, cr)) : __fmul_rn(0.5f, __fadd_rn(1.f, cr));
+    f.w1 = f.w2 = 0.f;
+  }
+  f.ircr = cr != 0.f ? __frcp_rn(fabsf(cr)) : 0.f;
+  f.U = U;
+  f.K = K;
+}
+
+__device__ __forceinline__ void fold_hface(Face &f, bool wet, bool eb, bool quick, bool ult,
+                                           float cr, float U, float K, const Face2 &m) {
+  if (!wet) {
+    f32::face_zero(f);
+    return;
+  }
+  if (!quick && !eb) {  // Van Leer advects interior faces only
+    f32::face_zero(f);
+    f.K = K;
+    return;
+  }
+  fold_face(f, quick, cr, m.d, m.Ap, m.Bp, m.Am, m.Bm, U, ult && eb, K);
+}
+
+__device__ __forceinline__ void fold_zface(Face &f, bool quick, bool ult, float dzm2, float dzm1,
+                                           float dz0, float dzp1, bool top, float wv) {
+  const float w9m = __fmul_rn(0.5f, __fadd_rn(dzm1, dzm2));
+  const float w90 = __fmul_rn(0.5f, __fadd_rn(dz0, dzm1));
+  const float w9p = top ? w90 : __fmul_rn(0.5f, __fadd_rn(dzp1, dz0));
+  const float cz = __fdiv_rn(wv, w90);
+  const float db = __fdiv_rn(2.f, __fadd_rn(w9m, w90)), df = __fdiv_rn(2.f, __fadd_rn(w90, w9p));
+  fold_face(f, quick, cz, __fdiv_rn(dzm1, __fadd_rn(dzm1, dz0)), __fmul_rn(db, w9m),
+            __fmul_rn(db, w90), __fmul_rn(df, w90), __fmul_rn(df, w9p), wv, ult, 0.f);
+}
+
+// One face flux (f32::face with every rounding explicit): QUICKEST or Van
+// Leer, then ULTIMATE (tracers.c:3526-3554 without its divisions), times the
+// volume flux, minus the horizontal-diffusion term.
+template <bool QUICK, bool ULT>
+__device__ __forceinline__ float face_flux(const Face &f, bool adv, bool hd, float tm2, float tm1,
+                                          float t0, float tp1) {
+  float F = 0.f;
+  if (adv) {
+    const bool pos = (f.bits & FB_POS) != 0;
+    const float tu = pos ? tm2 : tp1;
+    if (QUICK) {
+      F = __fmaf_rn(f.wa, tu, __fmaf_rn(f.w1, tm1, __fmul_rn(f.w2, t0)));
+    } else {
+      const bool neg = (f.bits & FB_NEG) != 0;
+      const float p = pos ? __fsub_rn(tm1, tm2) : __fsub_rn(t0, tm1);
+      const float q = pos ? __fsub_rn(t0, tm1) : __fsub_rn(tp1, t0);
+      const float den = pos ? __fsub_rn(t0, tm2) : __fsub_rn(tp1, tm1);
+      const float pq = __fmul_rn(p, q);
+      const float df = pq > 0.f ? __fmul_rn(2.f, __fdiv_rn(pq, den)) : 0.f;
+      F = pos ? __fmaf_rn(f.wa, df, tm1) : (neg ? __fmaf_rn(-f.wa, df, t0) : 0.f);
+    }
+    if (ULT) {
+      // with s = sign(td - tu) and the normalised variables scaled back by
+      // |td - tu|: nc in [0, 1] is 0 <= c <= d, nu > 1 is a > d, nu < nc is
+      // a < c and nu > nc / |cr| is a > c / |cr|; tu + nc (td - tu) is tc.
+      // Upwind and downwind equal in FP32 (d = 0) limit to tc (in FP64 they
+      // almost always differ by a few ulps and the limiter falls back to
+      // upwind).
+      const float tc = pos ? tm1 : t0, td = pos ? t0 : tm1;
+      const float diff = __fsub_rn(td, tu);
+      const float sg = diff < 0.f ? -1.f : 1.f;
+      const float d = fabsf(diff);
+      const float c = __fmul_rn(__fsub_rn(tc, tu), sg), a = __fmul_rn(__fsub_rn(F, tu), sg);
+      const float q = __fmul_rn(c, f.ircr);
+      float G = F;
+      if (a > q) G = __fmaf_rn(sg, q, tu);
+      if (a < c) G = tc;
+      if (a > d) G = td;
+      if (!(c >= 0.f && c <= d)) G = tc;
+      F = (f.bits & FB_ULT) ? G : F;
+    }
+    F = __fmul_rn(F, f.U);
+  }
+  if (hd) F = __fmaf_rn(-f.K, __fsub_rn(t0, tm1), F);
+  return F;
+}
+
+}  // namespace f32x
+
+// ---------------------------------------------------------------------------
+
+template <bool QUICK, bool ULT, bool LAST>
+__global__ void __launch_bounds__(kFusedThreads, 2)
+    k_step32(Geo G, Flow F, Flow32 F3, Work W, Opt O, TrSet T, SubStep ss, Tile Tl, Fused Fu,
+             const f32::Face2 *__restrict__ fx2, const f32::Face2 *__restrict__ fy2,
+             const float *__restrict__ tri, float *__restrict__ tro, int any_hd, int kbase) {
+  using namespace f32x;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb;
+  float4 *LU = reinterpret_cast<float4 *>(smem);                 // [nd][32]
+  int *colC = reinterpret_cast<int *>(LU + nd * 32);             // [nd][32]
+  float *A = reinterpret_cast<float *>(colC + nd * 32);          // [nwb][nd][32]
+  float *Sv = A + nwb * nd * 32;                                 // [nwb][nd][32]
+  float2 *fzx = reinterpret_cast<float2 *>(Sv + nwb * nd * 32);  // [8][32]
+  double *red = reinterpret_cast<double *>(fzx + kFusedWarps * 32);  // [8][2][2][32]
+  double *accM = red + kFusedWarps * 4 * 32;                     // [ntb][32]
+  double *accD = accM + ntb * 32;                                // [ntb][32]
+  float *accF = reinterpret_cast<float *>(accD + ntb * 32);      // [ntb][32]
+
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int tile = blockIdx.x;
+  const int col = Fu.tcol[tile * 32 + lane];
+  const TileCol tc = tile_column(G, W, Tl, col);
+  const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
+  const ColInfo ci = tc.ci;
+  const int ntc = tc.act ? G.colntr[col] : 0;
+  const int kmin = Fu.tkmin[tile];
+
+  // the cells of the tile's columns and, on the last sub-step, their LU
+  // factors, copied while phase A runs
+  for (int k = kmin + w; k < nz; k += kFusedWarps) {
+    const int c = (tc.act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
+    const int r = k - kbase;
+    colC[r * 32 + lane] = c;
+    if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &W.lu32[c]);
+  }
+  cp_async_commit();
+  for (int i = threadIdx.x; i < ntb * 32; i += kFusedThreads) {
+    accM[i] = 0.0;
+    accD[i] = 0.0;
+    accF[i] = 0.f;
+  }
+  __syncthreads();
+
+  // ---------------- phase A: advection, one layer of the chunk per warp
+  const double dtu = ss.dtu;
+  const float fdtu = (float)dtu;
+  const bool hdf = any_hd != 0;
+  const double area = tc.act ? G.cellarea[c2] : 1.0;
+  const double ia = 1.0 / area;
+  int nstat = 0;
+  for (int k0 = nz - 1; k0 >= kmin; k0 -= kFusedWarps) {
+    const int k = k0 - w;
+    const int c = k >= kmin ? colC[(k - kbase) * 32 + lane] : 0;
+    const bool on = c != 0;
+    int4 n1 = make_int4(0, 0, 0, 0), n2 = n1, nzv = n1;
+    int2 me = make_int2(0, 0);
+    int fl = 0;
+    if (on) {
+      n1 = Tl.nb1[c];
+      n2 = Tl.nb2[c];
+      nzv = Tl.nbz[c];
+      me = Tl.m2e[c];
+      fl = Tl.fl[c];
+    }
+    // east / north neighbours that are the cells of the lanes at ix + 1 / iy + 1
+    const int cE = __shfl_down_sync(FULL, c, 1), cN = __shfl_down_sync(FULL, c, 8);
+    const bool sxp1 = on && (lane & 7) != 7 && cE != 0 && n1.y == cE;
+    const bool syp1 = on && lane < 24 && cN != 0 && n1.w == cN;
+    const bool zf = on && k <= ks, zt = on && k < ks;
+    // the top face comes from the warp above, except in the chunk's first warp
+    const bool top_self = zt && w == 0;
+    Face fw, fs, fn, fe, fzb, fzt;
+    f32::face_zero(fw);
+    f32::face_zero(fs);
+    f32::face_zero(fn);
+    f32::face_zero(fe);
+    f32::face_zero(fzb);
+    f32::face_zero(fzt);
+    double dz0d = 1.0, idz = 0.0;
+    if (on) {
+      const Face2 mx = fx2[c2], my = fy2[c2];
+      fold_hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT,
+                 __fmul_rn(__fmul_rn(F3.u1[c], fdtu), mx.ih), F3.u1flux3d[c],
+                 hdf ? F3.khx[c] : 0.f, mx);
+      fold_hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT,
+                 __fmul_rn(__fmul_rn(F3.u2[c], fdtu), my.ih), F3.u2flux3d[c],
+                 hdf ? F3.khy[c] : 0.f, my);
+      if (!syp1 && (fl & FL_YP_WET)) {
+        const int yp = n1.w;
+        const Face2 mn = fy2[me.y];
+        fold_hface(fn, true, fl & FL_YP_E2, QUICK, ULT,
+                   __fmul_rn(__fmul_rn(F3.u2[yp], fdtu), mn.ih), F3.u2flux3d[yp],
+                   hdf ? F3.khy[yp] : 0.f, mn);
+      }
+      if (!sxp1 && (fl & FL_XP_WET)) {
+        const int xp = n1.y;
+        const Face2 mxe = fx2[me.x];
+        fold_hface(fe, true, fl & FL_XP_E1, QUICK, ULT,
+                   __fmul_rn(__fmul_rn(F3.u1[xp], fdtu), mxe.ih), F3.u1flux3d[xp],
+                   hdf ? F3.khx[xp] : 0.f, mxe);
+      }
+      const float dz0 = W.dz32[c];
+      if (zf) {
+        const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
+        const bool top = (nzv.z == c);
+        const float dzp1 = W.dz32[nzv.z];
+        fold_zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
+        if (top_self) {
+          const bool top1 = (nzv.w == nzv.z);
+          const float dzp2 = W.dz32[nzv.w];
+          fold_zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1,
+                     __fmul_rn(F3.w[nzv.z], fdtu));
+        }
+      }
+      dz0d = W.dz[c];
+      idz = 1.0 / dz0d;
+    }
+    // vertical neighbours (below the bottom: the sediment ghost holds the
+    // bottom value, tracers.c:827-830)
+    const int vm1 = (k - 1 >= kb) ? nzv.x : c;
+    const int vm2 = (k - 2 >= kb) ? nzv.y : vm1;
+    const int vp1 = nzv.z, vp2 = nzv.w;
+    const bool needE = on && !sxp1, needN = on && !syp1;
+
+    for (int s0 = 0; s0 < ntb; s0 += 2) {
+      float Fb[2], Fw[2], Fs[2], Fe[2], Fn[2], Ftop[2], t0v[2];
+      int nn[2];
+      bool adv[2];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int s = s0 + u < ntb ? s0 + u : s0;
+        const int n = T.slot_tr[s];
+        const int tf = T.trf[n];
+        nn[u] = n;
+        adv[u] = (tf & TR_ADV) != 0;
+        const bool hd = (tf & TR_HDIFF) != 0;
+        const float *__restrict__ tr = tri + (size_t)n * G.S;
+        const bool hor = on && (adv[u] || hd);
+        const bool vz = on && adv[u] && zf;
+        const float t0 = on ? tr[c] : 0.f;
+        const float tym1 = hor ? tr[n1.z] : 0.f, tym2 = hor ? tr[n2.z] : 0.f;
+        const float typ1 = hor ? tr[n1.w] : 0.f, typ2 = (hor && needN) ? tr[n2.w] : 0.f;
+        const float txm1 = hor ? tr[n1.x] : 0.f, txm2 = hor ? tr[n2.x] : 0.f;
+        const float txp1 = hor ? tr[n1.y] : 0.f, txp2 = (hor && needE) ? tr[n2.y] : 0.f;
+        const float tm1 = vz ? tr[vm1] : 0.f, tm2 = vz ? tr[vm2] : 0.f;
+        const float tp1 = vz ? tr[vp1] : 0.f, tp2 = (vz && top_self) ? tr[vp2] : 0.f;
+        t0v[u] = t0;
+        Fw[u] = hor ? face_flux<QUICK, ULT>(fw, adv[u], hd, txm2, txm1, t0, txp1) : 0.f;
+        Fs[u] = hor ? face_flux<QUICK, ULT>(fs, adv[u], hd, tym2, tym1, t0, typ1) : 0.f;
+        Fe[u] = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv[u], hd, txm1, t0, txp1, txp2)
+                               : 0.f;
+        Fn[u] = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv[u], hd, tym1, t0, typ1, typ2)
+                               : 0.f;
+        Fb[u] = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+        Ftop[u] =
+            (vz && top_self) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const float e = __shfl_down_sync(FULL, Fw[u], 1), nb = __shfl_down_sync(FULL, Fs[u], 8);
+        if (sxp1) Fe[u] = e;
+        if (syp1) Fn[u] = nb;
+      }
+      fzx[w * 32 + lane] = make_float2(Fb[0], Fb[1]);
+      __syncthreads();
+      if (w > 0) {
+        const float2 up = fzx[(w - 1) * 32 + lane];
+        Ftop[0] = up.x;
+        Ftop[1] = up.y;
+      }
+      double cm[2] = {0.0, 0.0}, cd[2] = {0.0, 0.0};
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int s = s0 + u;
+        if (s >= ntb || !on || nn[u] >= ntc) continue;
+        // FP64 flux divergence (tracers.c:888-892)
+        const double dtr =
+            (((double)Fe[u] - (double)Fw[u]) + ((double)Fn[u] - (double)Fs[u])) * dtu;
+        if (zt) {
+          const double Fzt = adv[u] ? (double)Ftop[u] : 0.0;
+          const double a = (double)t0v[u] - (dtr * ia + (Fzt - (double)Fb[u])) * idz;
+          const float a32 = (float)a;
+          tro[(size_t)nn[u] * G.S + c] = a32;
+          nstat |= isnan(a32) ? ST_NAN : 0;
+          cm[u] = a * dz0d;
+        } else {
+          cd[u] = dtr;
+          if (k == ks) accF[s * 32 + lane] = Fb[u];
+        }
+      }
+      // per (column, tracer) sums over the chunk's layers, in warp order
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        red[((w * 2 + u) * 2 + 0) * 32 + lane] = cm[u];
+        red[((w * 2 + u) * 2 + 1) * 32 + lane] = cd[u];
+      }
+      __syncthreads();
+      if (w < 4) {
+        const int u = w >> 1, q = w & 1, s = s0 + u;
+        if (s < ntb) {
+          double sum = 0.0;
+          for (int ww = 0; ww < kFusedWarps; ++ww) sum += red[((ww * 2 + u) * 2 + q) * 32 + lane];
+          double *acc = q ? accD : accM;
+          acc[s * 32 + lane] += sum;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // ---------------- phase B: one thread per (column, tracer)
+  if (w < nwb && tc.act) {
+    float *Aj = A + w * nd * 32 + lane;
+    float *Sj = Sv + w * nd * 32 + lane;
+    const bool steady = F.eta[c2] == F.oldeta[c2];
+    long long nwarn = 0;
+    for (int slot = w; slot < T.nslot; slot += nwb) {
+      const int n = T.slot_tr[slot];
+      if (n >= ntc) continue;  // tracer not carried in this column
+      const int tf = T.trf[n];
+      const bool tbdy = slot < ntb;
+      const bool adv = tbdy && (tf & TR_ADV);
+      const bool vdf = LAST && (tf & TR_VDIFF);
+      const bool single = (ci.flags & COL_SINGLE) != 0;
+      const bool solve = vdf && !single;
+      const float *tr = tri + (size_t)n * G.S;
+      float *to = tro + (size_t)n * G.S;
+      float *const A0 = Aj + (kb - kbase) * 32;
+      float *const S0 = Sj + (kb - kbase) * 32;
+      const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
+      const int *const C0 = colC + (kb - kbase) * 32 + lane;
+      const int nk = ks - kb;  // cells below the surface cell
+      // the column's values: advection results below the surface (advected
+      // tracers) or the old values (the rest, every layer)
+      if (tbdy) {
+        for (int j = 0; j < nk; ++j) A0[j * 32] = to[C0[j * 32]];
+      } else {
+        for (int j = 0; j < nz - kb; ++j) A0[j * 32] = tr[C0[j * 32]];
+      }
+      const double mn = T.mintr[n], mx = T.maxtr[n];
+      {  // sediment ghost (tracers.c:827-830)
+        const int sed = G.zm1[cbot];
+        to[sed] = tbdy ? tr[cbot] : tr[sed];
+      }
+      const double dzs_old = (double)W.dz32[ci.s];
+      const double ts_old = (double)tr[ci.s];
+      const double dzs = W.dz[ci.s];
+      double carry_in = 0.0;
+      if (Fu.carry && steady) carry_in = Fu.carry[(size_t)n * G.ncol + col];
+      // FP64 mass bookkeeping per unit area: what the step computed (mx*) and
+      // what is stored (ms*), compensated sums
+      double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
+      f32::neumaier_add(mxs, mxc, carry_in * ia);
+      long long nw = 0;
+      float fwd = 0.f;
+      double as64;  // the surface row's value in FP64 (with the carry put back)
+      bool bad = false;
+      if (!tbdy) {
+        for (int j = 0; j < nk; ++j)
+          f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
+        const double vs = (double)A0[nk * 32];
+        f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+        as64 = dzs > 0.0 ? vs + carry_in * ia / dzs : vs;
+        for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = A0[j * 32];
+        if (solve) {
+          for (int j = 0; j < nk; ++j) {
+            const float4 lu = L0[j * 32];
+            fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
+            S0[j * 32] = fwd;
+          }
+          A0[nk * 32] = (float)as64;
+          const float4 lu = L0[nk * 32];
+          S0[nk * 32] = (lu.x * A0[nk * 32] - lu.y * fwd) * lu.z;
+        } else {
+          for (int j = 0; j < nk; ++j) {
+            to[C0[j * 32]] = A0[j * 32];
+            f32::neumaier_add(mss, msc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
+          }
+        }
+      } else {
+        // tr_bounds clip and range check (:3278-3293) of the cells below the
+        // surface; a < mn and a > mx of a float a, exactly, as float compares
+        const double a_below = nk > 0 ? (double)A0[(nk - 1) * 32] : 0.0;
+        const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
+        const bool clip = mn <= kClipEps;
+        f32::neumaier_add(mxs, mxc, accM[slot * 32 + lane]);
+        for (int j = 0; j < nk; ++j) {
+          float a = A0[j * 32];
+          if (clip && a < mn_up) {
+            f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, W.dz[C0[j * 32]]));
+            a = mnf;
+          }
+          nw += (a < mn_up || a > mx_dn);
+          if (solve) {
+            A0[j * 32] = a;
+            const float4 lu = L0[j * 32];
+            fwd = (lu.x * a - lu.y * fwd) * lu.z;
+            S0[j * 32] = fwd;
+          } else {
+            to[C0[j * 32]] = a;
+            bad |= isnan(a);
+            f32::neumaier_add(mss, msc, __dmul_rn((double)a, W.dz[C0[j * 32]]));
+          }
+        }
+        // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
+        double vs = ts_old;
+        if (adv) {
+          const double Fzb_s = (double)accF[slot * 32 + lane];
+          const double wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
+          const double eta = F.eta[c2], oe = F.oldeta[c2];
+          const double osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
+          const double sub = oe + ss.subeta_f * (eta - oe);
+          double ssum = 0.0, scomp = 0.0;
+          f32::neumaier_add(ssum, scomp, __dmul_rn(Fzb_s, area));
+          f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
+          f32::neumaier_add(ssum, scomp, -accD[slot * 32 + lane]);
+          const double dzn = sub - wb;
+          const double svol = dzn * area;
+          const double st = ssum + scomp;
+          const double sv = (svol == 0.0 || (st < 0.0 && dzn <= O.hmin)) ? 0.0 : st / svol;
+          vs = (G.botz[c2] > 0.0 && dzs_old < O.hmin) ? ts_old : sv;
+        }
+        if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
+        if (mn <= kClipEps && vs < mn) vs = mn;
+        if (vs < mn || vs > mx) ++nw;
+        f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+        as64 = dzs > 0.0 ? vs + carry_in * ia / dzs : vs;
+        const float vs32 = (float)vs;
+        for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
+        if (solve) {
+          const float4 lu = L0[nk * 32];
+          A0[nk * 32] = (float)as64;
+          S0[nk * 32] = (lu.x * A0[nk * 32] - lu.y * fwd) * lu.z;
+        }
+      }
+      if (vdf && single) {
+        const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
+        const float fin = (float)(as64 + F.dt * (0.0 - 0.0) / h);
+        to[ci.s] = fin;
+        bad |= isnan(fin);
+        f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+      } else if (!solve) {
+        const float fin = (float)as64;
+        to[ci.s] = fin;
+        bad |= isnan(fin);
+        f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+      } else {
+        // back substitution (FP32) and, one row behind, the FP64 residual
+        //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
+        // (cp1(j) = cm1(j+1)); the surface row's value is the FP64 one
+        float x1 = S0[nk * 32];
+        float4 l1 = L0[nk * 32];
+        double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
+        for (int j = nk - 1; j >= 0; --j) {
+          const float x = S0[j * 32] - l1.w * x1;
+          S0[j * 32] = x;
+          const double xd = (double)x, l1y = (double)l1.y;
+          const double aj1 = (j + 1 == nk) ? as64 : (double)A0[(j + 1) * 32];
+          double r = (double)l1.x * (aj1 - xd1) - l1y * (xd - xd1);
+          if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
+          A0[(j + 1) * 32] = (float)r;
+          x1 = x;
+          xd2 = xd1;
+          xd1 = xd;
+          l2y = l1y;
+          l1 = L0[j * 32];
+        }
+        {
+          const double a0 = (nk == 0) ? as64 : (double)A0[0];
+          double r = (double)l1.x * (a0 - xd1) - (double)l1.y * (xd1 - xd1);
+          if (nk > 0) r = r - l2y * (xd2 - xd1);
+          A0[0] = (float)r;
+        }
+        // correction solve (FP32 forward and back) and the update in FP64
+        float u = 0.f;
+        for (int j = 0; j <= nk; ++j) {
+          const float4 lu = L0[j * 32];
+          u = (A0[j * 32] - lu.y * u) * lu.z;
+          A0[j * 32] = u;
+        }
+        float d = A0[nk * 32];
+        {
+          const float fin = (float)((double)S0[nk * 32] + (double)d);
+          to[C0[nk * 32]] = fin;
+          bad |= isnan(fin);
+          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+        }
+        for (int j = nk - 1; j >= 0; --j) {
+          d = A0[j * 32] - L0[(j + 1) * 32].w * d;
+          const float fin = (float)((double)S0[j * 32] + (double)d);
+          to[C0[j * 32]] = fin;
+          bad |= isnan(fin);
+          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, W.dz[C0[j * 32]]));
+        }
+      }
+      if (Fu.carry && steady)
+        Fu.carry[(size_t)n * G.ncol + col] = ((mxs + mxc) - (mss + msc)) * area;
+      if (bad) nstat |= ST_NAN;
+      nwarn += nw;
+    }
+    if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
+  }
+  if (nstat) atomicOr(W.status, nstat);
+}
+
+}  // namespace shoc

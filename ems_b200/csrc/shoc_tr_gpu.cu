@@ -74,6 +74,9 @@ struct shoc_tr_gpu {
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
   double *fzs64 = nullptr;            // the same, FP64 path
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
+  Fused fu{};                         // fused FP32-mixed sub-step (k_step32): tiles, carry
+  bool fused = false;                 // FP32-mixed sub-steps run k_step32
+  size_t fused_bytes = 0;             // its dynamic shared memory
   std::vector<int> vd_depth;          // layers of the k_vd32 tiles, in their (sorted) order
   bool staged = false;                // column-tile fast path
   int cur = 0;
@@ -487,8 +490,10 @@ __global__ void k_khfac(Geo G, Flow F, float *khx, float *khy) {
   }
 }
 
+// carry (FP32-mixed fused path, else null): [ntr][ncol] mass the stored
+// values owe each column, part of the state's mass.
 template <class TR>
-__global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
+__global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry, double *out) {
   const int n = blockIdx.y;
   const TR *t = tr + (size_t)n * G.S;
   double s = 0.0, comp = 0.0;
@@ -496,8 +501,9 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, double *out) {
        col += gridDim.x * blockDim.x) {
     const int top = G.col_top[col], bot = G.col_bot[col];
     int c = W.nsur_t[col];
-    if (c == G.zm1[c]) continue;  // surface below the bottom: dry
     if (n >= G.colntr[col]) continue;  // tracer not carried in this column
+    if (carry) neumaier(s, comp, carry[(size_t)n * G.ncol + col]);
+    if (c == G.zm1[c]) continue;  // surface below the bottom: dry
     const double area = G.cellarea[top];
     double tz = F.eta[top];
     for (int it = 0; it <= G.nz; ++it) {
@@ -678,6 +684,53 @@ int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<u
   T.wet = ip;
   if ((rc = dupload(h, &ip, vdcol.data(), vdcol.size()))) return rc;
   T.vdcol = ip;
+  return 0;
+}
+
+// Tiles of the fused FP32-mixed kernel: 8 x 4 water columns (lane = 8 * iy
+// + ix for the column at (8 * ti + ix, 4 * tj + iy)), in row-major tile order
+// so that blocks running at the same time hold neighbouring tiles; a tile's
+// lowest layer bounds its layer loop.
+int build_fused_tiles(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<int> &col_kb) {
+  const int ncol = h->ncol;
+  int imax = 0, jmax = 0;
+  for (int col = 0; col < ncol; col++) {
+    const int top = g->w2_t[col + 1];
+    if (g->s2i[top] < 0 || g->s2j[top] < 0) return SHOC_TR_EGEOM;
+    imax = std::max(imax, g->s2i[top]);
+    jmax = std::max(jmax, g->s2j[top]);
+  }
+  const long long nti = imax / 8 + 1, ntj = jmax / 4 + 1;
+  std::vector<int> tid((size_t)(nti * ntj), -1);
+  std::vector<int> tcol, tkmin;
+  std::vector<int> order(ncol);
+  for (int col = 0; col < ncol; col++) order[col] = col;
+  auto key = [&](int col) {
+    const int top = g->w2_t[col + 1];
+    return (long long)(g->s2j[top] / 4) * nti + g->s2i[top] / 8;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
+  for (int col : order) {
+    const int top = g->w2_t[col + 1];
+    const int i = g->s2i[top], j = g->s2j[top];
+    int &t = tid[(size_t)key(col)];
+    if (t < 0) {
+      t = (int)tkmin.size();
+      tkmin.push_back(h->nz);
+      tcol.insert(tcol.end(), 32, -1);
+    }
+    const int lane = (j % 4) * 8 + i % 8;
+    if (tcol[(size_t)t * 32 + lane] >= 0) return SHOC_TR_EGEOM;  // two columns at one (i, j)
+    tcol[(size_t)t * 32 + lane] = col;
+    tkmin[t] = std::min(tkmin[t], col_kb[col]);
+  }
+  h->fu.ntile = (int)tkmin.size();
+  int *ip;
+  int rc;
+  if ((rc = dupload(h, &ip, tcol.data(), tcol.size()))) return rc;
+  h->fu.tcol = ip;
+  if ((rc = dupload(h, &ip, tkmin.data(), tkmin.size()))) return rc;
+  h->fu.tkmin = ip;
   return 0;
 }
 
@@ -1018,6 +1071,25 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   }
   TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
+  if (f32p) {
+    // the fused sub-step kernel: every advected tracer's accumulators and the
+    // column arrays of as many phase-B warps as keep two blocks per SM
+    const char *env = getenv("SHOC_TR_GPU_KERNELS");
+    const bool want = !(env && strcmp(env, "split") == 0);
+    const int ntb = o->ntbdy;
+    int nwb = 0;
+    for (int c = 4; c >= 1 && !nwb; c--)
+      if (fused_smem(g->nz, c, ntb) <= 113 * 1024) nwb = c;
+    if (!nwb && fused_smem(g->nz, 1, ntb) <= 227 * 1024) nwb = 1;
+    if (want && nwb && ntb <= kFusedMaxTracers) {
+      TRY(build_fused_tiles(h, g, col_kb));
+      h->fu.nwb = nwb;
+      TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
+      h->fused_bytes = fused_smem(g->nz, nwb, ntb);
+      h->fused = true;
+      if (fused32_set_smem_attr((int)h->fused_bytes) != cudaSuccess) TRY(SHOC_TR_ECUDA);
+    }
+  }
   // flow fields
   Flow &F = h->F;
   TRY(dupload<double>(h, (double **)&F.u1, nullptr, S));
@@ -1235,17 +1307,31 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
       cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
       if (prof)
         for (auto &e : ev) cudaEventCreate(&e);
-      const Tile tl = vd_classes(h, tw);
-      tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
-                     h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
-                     h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
-      if (prof) {  // pairs share events; sync destroys each event once
-        h->ev.push_back({0, ev[0], ev[2]});
-        h->ev.push_back({1, ev[0], ev[1]});
-        h->ev.push_back({2, ev[1], ev[2]});
+      if (h->fused) {
+        if (prof) cudaEventRecord(ev[0], st);
+        fused32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
+                        h->F3, h->W, h->O, T, ss, h->tl, h->fu, h->fx2, h->fy2, tin, tout,
+                        h->any_hdiff ? 1 : 0, h->fused_bytes);
+        if (prof) {
+          cudaEventRecord(ev[1], st);
+          h->ev.push_back({0, ev[0], ev[1]});
+          h->ev.push_back({1, ev[0], ev[1]});
+          cudaEventDestroy(ev[2]);
+        }
+        h->launches += h->fu.ntile > 0 ? 1 : 0;
+      } else {
+        const Tile tl = vd_classes(h, tw);
+        tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
+                       h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
+                       h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
+        if (prof) {  // pairs share events; sync destroys each event once
+          h->ev.push_back({0, ev[0], ev[2]});
+          h->ev.push_back({1, ev[0], ev[1]});
+          h->ev.push_back({2, ev[1], ev[2]});
+        }
+        h->launches += (T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
+        for (int k = 0; k < tl.nclass; k++) h->launches += tl.ctile[k + 1] > tl.ctile[k] ? 1 : 0;
       }
-      h->launches += (T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
-      for (int k = 0; k < tl.nclass; k++) h->launches += tl.ctile[k + 1] > tl.ctile[k] ? 1 : 0;
       if (last)
         k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
                                                             tin, tout, c3row, c3_load);
@@ -1435,6 +1521,9 @@ int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
     CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
     k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S);
     h->launches++;
+    if (h->fu.carry)
+      CK(cudaMemsetAsync(h->fu.carry + (size_t)n * h->ncol, 0, (size_t)h->ncol * sizeof(double),
+                         s));
   }
   return 0;
 }
@@ -1524,6 +1613,9 @@ int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
   if (!h || !tr_wc) return SHOC_TR_EARG;
   DeviceScope dev_(h->device);
   const size_t S = (size_t)h->S;
+  // new values: nothing is owed to any column
+  if (h->fu.carry)
+    CK(cudaMemsetAsync(h->fu.carry, 0, (size_t)h->ntr * h->ncol * sizeof(double), h->stream));
   for (int n = 0; n < h->ntr; n++) {
     if (h->esize == sizeof(double)) {
       double *a = (double *)h->tr[h->cur] + n * S, *b = (double *)h->tr[h->cur ^ 1] + n * S;
@@ -1712,11 +1804,11 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
   CK(cudaMallocAsync(&part, (size_t)nb * std::max(h->ntr, 1) * sizeof(double), h->stream));
   if (h->ntr > 0) {
     if (h->esize == sizeof(float))
-      k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W,
-                                                             (const float *)h->tr[h->cur], part);
+      k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
+          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part);
     else
-      k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(h->G, h->F, h->W,
-                                                              (const double *)h->tr[h->cur], part);
+      k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
+          h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part);
     h->launches++;
   }
   std::vector<double> hp((size_t)nb * h->ntr);
@@ -1811,10 +1903,10 @@ int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass) {
   double *part = scr, *sums = scr + (size_t)kNoAllocMaxTracers * kNoAllocBlocks;
   if (h->esize == sizeof(float))
     k_mass<float><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
-        h->G, h->F, h->W, (const float *)h->tr[h->cur], part);
+        h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part);
   else
     k_mass<double><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
-        h->G, h->F, h->W, (const double *)h->tr[h->cur], part);
+        h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part);
   k_mass_finish<<<(h->ntr + 63) / 64, 64, 0, h->stream>>>(part, kNoAllocBlocks, h->ntr, sums);
   h->launches += 2;
   CK(cudaGetLastError());

@@ -4,7 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
-#include "shoc_tr_tile.cuh"
+#include "shoc_tr_fused.cuh"
 
 namespace shoc {
 
@@ -21,5 +21,16 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *fzs, int vd_nw,
                     int any_hd, int adv_flags, cudaEvent_t *ev);
+
+// allow every k_step32 instance `bytes` of dynamic shared memory
+cudaError_t fused32_set_smem_attr(int bytes);
+
+// one FP32-mixed transport sub-step over the staged columns as one fused
+// launch (k_step32: one block per tile of 8 x 4 columns, `smem` bytes)
+void fused32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo &G,
+                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
+                     const TrSet &T, const SubStep &ss, const Tile &Tl, const Fused &Fu,
+                     const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin, float *tout,
+                     int any_hd, size_t smem);
 
 }  // namespace shoc
