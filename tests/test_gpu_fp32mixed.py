@@ -99,3 +99,53 @@ def test_accuracy_report_small():
     assert max(rows[-1]["max_rel"]) <= TOL
     assert max(rows[-1]["rms_rel"]) <= TOL
     assert max(rows[-1]["mass_drift_fp64"]) <= 1e-12
+
+
+def run_kernels(case, nsteps, kernels):
+    """FP32-mixed run with the fused sub-step kernel or the two-kernel split
+    (SHOC_TR_GPU_KERNELS, read when a handle is created)."""
+    import os
+    old = os.environ.get("SHOC_TR_GPU_KERNELS")
+    os.environ["SHOC_TR_GPU_KERNELS"] = kernels
+    try:
+        t = gpu.TracerStep(case, precision=gpu.FP32_MIXED)
+    finally:
+        if old is None:
+            del os.environ["SHOC_TR_GPU_KERNELS"]
+        else:
+            os.environ["SHOC_TR_GPU_KERNELS"] = old
+    t.start()
+    m0 = t.mass()
+    t.run(nsteps)
+    t.sync()
+    out = t.download()
+    m1 = t.mass()
+    t.close()
+    return out, m0, m1
+
+
+@pytest.mark.parametrize("kw", [{}, dict(dt=2000.0), dict(trasc=_abi.VANLEER, ultimate=1),
+                                dict(hdiff=(40.0, [1, 0, 1]))])
+def test_fused_and_split_kernels_agree(kw):
+    """The fused sub-step kernel and the advection + column kernel pair give
+    the same tracers to FP32 rounding (the fused one keeps the advected
+    values in FP64 until tr_bounds and carries the rounded-off mass)."""
+    case = synth.make("small", seed=63, **kw)
+    a = run_kernels(case, 10, "fused")[0]
+    b = run_kernels(case, 10, "split")[0]
+    ref = oracle.run_oracle(case, 10)[1]
+    ea, _ = errors(case, a, ref)
+    eb, _ = errors(case, b, ref)
+    assert np.all(ea <= TOL) and np.all(eb <= TOL), (ea, eb)
+    c = case.win.wet_cells()
+    assert np.all(np.abs(a[:, c] - b[:, c]).max(axis=1) <= TOL * np.abs(ref[:, c]).max(axis=1))
+
+
+@pytest.mark.parametrize("name,steps", [("basin64", 100), ("small", 50)])
+def test_fp32mixed_conserves_mass(name, steps):
+    """FP32 storage loses mass at every rounding; the per-column FP64 carry
+    of the fused kernel gives it back, so the stored values plus the carry
+    conserve each tracer's mass to 1e-12 relative, as the FP64 path does."""
+    case = synth.make(name)
+    _, m0, m1 = run_kernels(case, steps, "fused")
+    assert np.all(np.abs(m1 - m0) <= 1e-12 * np.abs(m0)), np.abs(m1 - m0) / np.abs(m0)
