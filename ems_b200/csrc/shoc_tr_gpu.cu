@@ -1722,6 +1722,87 @@ int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
   return 0;
 }
 
+// ---- checkpoint / resume: a versioned raw image of the resident state ----
+// [header 8 x int64][tracers: ntr x S values of the handle's precision]
+// [carry: ntr x ncol doubles, FP32-mixed fused path only][sur_t, nsur_t: ncol ints each]
+namespace {
+constexpr long long kStateMagic = 0x53484f4354524731ll;  // "SHOCTRG1"
+void state_layout(const shoc_tr_gpu *h, long long hd[8]) {
+  hd[0] = kStateMagic;
+  hd[1] = 1;  // version
+  hd[2] = h->precision;
+  hd[3] = h->ntr;
+  hd[4] = h->S;
+  hd[5] = h->ncol;
+  hd[6] = h->fu.carry ? 1 : 0;
+  hd[7] = 0;
+}
+size_t state_bytes(const shoc_tr_gpu *h) {
+  return 8 * sizeof(long long) + (size_t)h->ntr * h->S * h->esize +
+         (h->fu.carry ? (size_t)h->ntr * h->ncol * sizeof(double) : 0) +
+         2 * (size_t)h->ncol * sizeof(int);
+}
+}  // namespace
+
+int shoc_tr_gpu_state_size(shoc_tr_gpu *h, size_t *bytes) {
+  if (!h || !bytes) return SHOC_TR_EARG;
+  *bytes = state_bytes(h);
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_save_state(shoc_tr_gpu *h, void *buf, size_t bytes) {
+  if (!h || !buf || bytes < state_bytes(h)) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  char *p = (char *)buf;
+  long long hd[8];
+  state_layout(h, hd);
+  memcpy(p, hd, sizeof(hd));
+  p += sizeof(hd);
+  const size_t tb = (size_t)h->ntr * h->S * h->esize;
+  CK(cudaMemcpyAsync(p, h->tr[h->cur], tb, cudaMemcpyDeviceToHost, h->stream));
+  p += tb;
+  if (h->fu.carry) {
+    const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
+    CK(cudaMemcpyAsync(p, h->fu.carry, cb, cudaMemcpyDeviceToHost, h->stream));
+    p += cb;
+  }
+  CK(cudaMemcpyAsync(p, h->W.sur_t, (size_t)h->ncol * sizeof(int), cudaMemcpyDeviceToHost,
+                     h->stream));
+  p += (size_t)h->ncol * sizeof(int);
+  CK(cudaMemcpyAsync(p, h->W.nsur_t, (size_t)h->ncol * sizeof(int), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_load_state(shoc_tr_gpu *h, const void *buf, size_t bytes) {
+  if (!h || !buf || bytes < state_bytes(h)) return SHOC_TR_EARG;
+  long long hd[8], want[8];
+  memcpy(hd, buf, sizeof(hd));
+  state_layout(h, want);
+  if (memcmp(hd, want, sizeof(hd)) != 0) return SHOC_TR_EARG;  // another window or precision
+  DeviceScope dev_(h->device);
+  const char *p = (const char *)buf + sizeof(hd);
+  const size_t tb = (size_t)h->ntr * h->S * h->esize;
+  // both ping-pong buffers hold the state (the values a step does not write
+  // are read back from either)
+  CK(cudaMemcpyAsync(h->tr[h->cur], p, tb, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->tr[h->cur ^ 1], h->tr[h->cur], tb, cudaMemcpyDeviceToDevice, h->stream));
+  p += tb;
+  if (h->fu.carry) {
+    const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
+    CK(cudaMemcpyAsync(h->fu.carry, p, cb, cudaMemcpyHostToDevice, h->stream));
+    p += cb;
+  }
+  CK(cudaMemcpyAsync(h->W.sur_t, p, (size_t)h->ncol * sizeof(int), cudaMemcpyHostToDevice,
+                     h->stream));
+  p += (size_t)h->ncol * sizeof(int);
+  CK(cudaMemcpyAsync(h->W.nsur_t, p, (size_t)h->ncol * sizeof(int), cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
+}
+
 int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps) {
   if (!h || nsteps < 0) return SHOC_TR_EARG;
   if (h->dt <= 0.0) return SHOC_TR_EARG;

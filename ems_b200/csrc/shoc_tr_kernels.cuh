@@ -377,6 +377,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
     if (c == cs) k_cs = k;
     if (!upd) {
       tro[c] = (TR)(t0);
+      if (isnan(t0)) stat |= ST_NAN;
       if (vd && c <= cbs && c >= cs) {
         double dzdt = W.vd_dzdt[c];
         double rhs = dzdt * t0;
@@ -422,6 +423,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       if (mn <= kClipEps && a < mn) a = mn;
       if (a < mn || a > mx) warn++;
       tro[c] = (TR)(a);
+      if (isnan(a)) stat |= ST_NAN;
       if (vd && c <= cbs && c >= cs) {
         double dzdt = W.vd_dzdt[c];
         double rhs = dzdt * a;
@@ -469,6 +471,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       double h = W.dz[cs] > O.hmin ? W.dz[cs] : O.hmin;
       double v = tro[cs];
       tro[cs] = (TR)(v + F.dt * (0.0 - 0.0) / h);
+      if (isnan(v)) stat |= ST_NAN;
     } else if (act && vd) {
       double x = sol.at(k_cs);
       double a = tro[cs];
@@ -507,6 +510,7 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
   }
   if (mn <= kClipEps && vs < mn) vs = mn;
   if (vs < mn || vs > mx) warn++;
+  if (isnan(vs)) stat |= ST_NAN;
   // surface and the cells above it (:3309-3323)
   {
     int cc = s;

@@ -504,9 +504,13 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const int nk = ks - kb;  // cells below the surface cell
   long long nwarn = 0;
+  bool bad = false;  // a NaN among the values this thread stores
   float fwd = 0.f;  // Thomas forward carry (the bottom row's cm1 is 0)
   if (!tbdy) {
-    for (int j = 0; j < nz - kb; ++j) to[C0[j * 32]] = A0[j * sa];
+    for (int j = 0; j < nz - kb; ++j) {
+      to[C0[j * 32]] = A0[j * sa];
+      bad |= isnan(A0[j * sa]);
+    }
     if (vdf && single) {
       const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
       to[ci.s] = (float)((double)A0[nk * sa] + F.dt * (0.0 - 0.0) / h);
@@ -528,6 +532,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
         float a = A0[j * sa];
         if (clip && a < mn_up) a = mnf;
         nwarn += (a < mn_up || a > mx_dn);
+        bad |= isnan(a);
         A0[j * sa] = a;
         const float4 lu = L0[j * 32];
         fwd = (lu.x * a - lu.y * fwd) * lu.z;
@@ -538,6 +543,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
         float a = A0[j * sa];
         if (clip && a < mn_up) a = mnf;
         nwarn += (a < mn_up || a > mx_dn);
+        bad |= isnan(a);
         to[C0[j * 32]] = a;
       }
     }
@@ -557,6 +563,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
     if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
     if (mn <= kClipEps && vs < mn) vs = mn;
     if (vs < mn || vs > mx) ++nwarn;
+    bad |= isnan(vs);
     const float vs32 = (float)vs;
     for (int j = nk; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
     if (vdf && single) {
@@ -607,7 +614,6 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
       A0[j * sa] = u;
     }
     float d = A0[nk * sa];
-    bool bad = false;
     {
       const float fin = (float)((double)S0[nk * sa] + (double)d);
       to[C0[nk * 32]] = fin;
@@ -619,8 +625,8 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
       to[C0[j * 32]] = fin;
       bad |= isnan(fin);
     }
-    if (bad) atomicOr(W.status, ST_NAN);
   }
+  if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
 }
 

@@ -297,7 +297,10 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
   double solp = 0.0;
   if (!tbdy) {
     // tracers without advection / diffusion keep their values, then diffuse
-    for (int j = 0; j < nl; ++j) to[C0[j * 32]] = A0[j * sa];
+    for (int j = 0; j < nl; ++j) {
+      to[C0[j * 32]] = A0[j * sa];
+      if (isnan(A0[j * sa])) stat |= ST_NAN;
+    }
     if (vdf && single) {
       const double h = W.dz[cs] > O.hmin ? W.dz[cs] : O.hmin;
       const double v = A0[nk * sa];
@@ -329,6 +332,7 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
       // tr_bounds clip and range check (:3278-3293)
       if (mn <= kClipEps && a < mn) a = mn;
       if (a < mn || a > mx) nwarn++;
+      if (isnan(a)) stat |= ST_NAN;
       if (solve) {
         A0[j * sa] = a;
         double rhs = __ldg(&vdzdt[cc]) * a;
@@ -370,6 +374,7 @@ __global__ void __launch_bounds__(256) k_vd64(Geo G, Flow F, Work W, Opt O, TrSe
     if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
     if (mn <= kClipEps && vs < mn) vs = mn;
     if (vs < mn || vs > mx) nwarn++;
+    if (isnan(vs)) stat |= ST_NAN;
     for (int j = nk; j < nl; ++j) to[C0[j * 32]] = vs;
     if (vdf && single) {
       const double h = W.dz[cs] > O.hmin ? W.dz[cs] : O.hmin;

@@ -22,7 +22,8 @@ EXPORTS = (
     "shoc_tr_gpu_create", "shoc_tr_gpu_destroy", "shoc_tr_gpu_step",
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
-    "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_compare", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
+    "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_compare", "shoc_tr_gpu_state_size",
+    "shoc_tr_gpu_save_state", "shoc_tr_gpu_load_state", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
@@ -56,6 +57,9 @@ def lib(path=None):
     L.shoc_tr_gpu_mass.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_compare.argtypes = [H, H, _abi.IP, C.c_int] + [_abi.DP] * 4
+    L.shoc_tr_gpu_state_size.argtypes = [H, C.POINTER(C.c_size_t)]
+    L.shoc_tr_gpu_save_state.argtypes = [H, C.c_void_p, C.c_size_t]
+    L.shoc_tr_gpu_load_state.argtypes = [H, C.c_void_p, C.c_size_t]
     L.shoc_tr_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
     L.shoc_tr_gpu_host_unregister.argtypes = [C.c_void_p]
     L.shoc_tr_gpu_stream.argtypes = [H]
@@ -224,6 +228,44 @@ class TracerStep:
             d["rms_rel"] = np.where(d["sumsq_ref"] > 0, np.sqrt(d["sumsq_diff"] / d["sumsq_ref"]),
                                     np.nan)
         return d
+
+    def save_state(self):
+        """The resident state as bytes (shoc_tr_gpu_save_state)."""
+        n = C.c_size_t()
+        _check("state_size", self.L.shoc_tr_gpu_state_size(self.h, C.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        _check("save_state", self.L.shoc_tr_gpu_save_state(self.h, buf.ctypes.data, n.value))
+        return buf
+
+    def load_state(self, buf):
+        buf = np.ascontiguousarray(buf, np.uint8)
+        _check("load_state", self.L.shoc_tr_gpu_load_state(self.h, buf.ctypes.data, buf.nbytes))
+
+    def checkpoint(self, path, **meta):
+        """Writes the resident state to `path`: a one-line JSON header (the
+        window, precision, sizes and `meta`, e.g. the step count), then the
+        raw image of shoc_tr_gpu_save_state."""
+        import json
+        img = self.save_state()
+        c = self.case
+        head = dict(meta, format="shoc_tr_gpu state v1", precision=self.precision,
+                    ntr=c.ntr, sgsiz=c.win.sgsiz, columns=c.win.ncol, nwet=c.nwet,
+                    bytes=int(img.nbytes))
+        with open(path, "wb") as f:
+            f.write((json.dumps(head) + "\n").encode())
+            f.write(img.tobytes())
+        return head
+
+    def resume(self, path):
+        """Loads a checkpoint written by checkpoint(); returns its header."""
+        import json
+        with open(path, "rb") as f:
+            head = json.loads(f.readline().decode())
+            img = np.frombuffer(f.read(), np.uint8)
+        if head.get("format") != "shoc_tr_gpu state v1" or img.nbytes != head["bytes"]:
+            raise ValueError("%s: not a shoc_tr_gpu checkpoint" % path)
+        self.load_state(img)
+        return head
 
     def stream(self):
         return self.L.shoc_tr_gpu_stream(self.h)

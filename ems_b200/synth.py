@@ -289,7 +289,7 @@ class Case:
         a = self.opts_arrays()
         keep.append(a)
         return _abi.Opts(self.trasc, self.ultimate, self.stab, self.hmin,
-                         self.ntr, iptr(a["tbdy"]), self.ntr, iptr(a["tdif_v"]),
+                         len(a["tbdy"]), iptr(a["tbdy"]), len(a["tdif_v"]), iptr(a["tdif_v"]),
                          iptr(a["advect"]), iptr(a["diffuse"]), dptr(a["mintr"]),
                          dptr(a["maxtr"]), iptr(self.ntr2d))
 

@@ -95,6 +95,20 @@ int shoc_tr_gpu_run(shoc_tr_gpu *h, int nsteps);
  * device since the last sync (and clears it). */
 int shoc_tr_gpu_sync(shoc_tr_gpu *h, shoc_tr_diag *diag);
 
+/* Checkpoint and resume of the device-resident state: the tracers in the
+ * handle's own precision, the FP32-mixed path's per-column mass carry and
+ * the surface vectors, as one versioned raw image (header: magic, version,
+ * precision, ntr, sgsiz, columns, carry flag).  state_size gives the image's
+ * bytes; save copies it into buf (host memory), load puts it back into a
+ * handle of the same window and precision (else SHOC_TR_EARG).  A resumed
+ * run (load + set_flow + run) continues bit for bit where the saved one
+ * left off.  The reference restarts from the NetCDF state it dumps
+ * (restart_name / restart_dt, model/hd/inputs/readparam.c:1143-1145); this
+ * image is the library's own device state, with no counterpart there. */
+int shoc_tr_gpu_state_size(shoc_tr_gpu *h, size_t *bytes);
+int shoc_tr_gpu_save_state(shoc_tr_gpu *h, void *buf, size_t bytes);
+int shoc_tr_gpu_load_state(shoc_tr_gpu *h, const void *buf, size_t bytes);
+
 /* Total tracer mass of every tracer: sum of tr * dz * cellarea over each
  * column from its current surface cell (top at eta) to the bottom (botz),
  * accumulated in FP64 with compensated (Neumaier) summation.  mass[ntr]. */
