@@ -453,7 +453,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const double vs = (double)A0[nk * 32];
         f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
         as64 = dzs > 0.0 ? vs + carry_in * ia / dzs : vs;
-        for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = A0[j * 32];
+        for (int j = nk + 1; j < nz - kb; ++j) {
+          to[C0[j * 32]] = A0[j * 32];
+          bad |= isnan(A0[j * 32]);
+        }
         if (solve) {
           for (int j = 0; j < nk; ++j) {
             const float4 lu = L0[j * 32];
@@ -466,6 +469,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         } else {
           for (int j = 0; j < nk; ++j) {
             to[C0[j * 32]] = A0[j * 32];
+            bad |= isnan(A0[j * 32]);
             f32::neumaier_add(mss, msc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
           }
         }
