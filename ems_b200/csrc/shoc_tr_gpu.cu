@@ -74,6 +74,7 @@ struct shoc_tr_gpu {
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
   double *fzs64 = nullptr;            // the same, FP64 path
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
+  double *cols = nullptr;             // column-solve entry points: their device arrays
   Fused fu{};                         // fused FP32-mixed sub-step (k_step32): tiles, carry
   bool fused = false;                 // FP32-mixed sub-steps run k_step32
   size_t fused_bytes = 0;             // its dynamic shared memory
@@ -559,6 +560,122 @@ __global__ void k_compare(Geo G, Tile Tl, const int *colntr_b, const TA *ta, con
     atomicAdd(&ssd[o], sd);
     atomicAdd(&ssr[o], sr);
   }
+}
+
+// ---------------------------------------------------------------------------
+// The other per-column tridiagonal solves, one thread per water column (from
+// its bottom cell up to its surface cell, the handle's current nsur_t; a
+// column whose surface is its sediment cell is dry).  The arithmetic is the
+// reference's, operation by operation (this file is compiled without FMA
+// contraction, with IEEE division), so the results are bitwise its own.  The
+// reference keeps the rows in layer-indexed work vectors; here every array is
+// indexed by SHOC cell (a cell carries the row of its layer).
+
+// tridiagonal (model/hd/closure/MY2-5.c:499-536): the closures' solve
+__global__ void k_tridiag(Geo G, Work W, const double *C, const double *Cm1, const double *Cp1,
+                          const double *rhs, double *var, double *sol, double *ud,
+                          double minvar) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= G.ncol) return;
+  const int cs = W.nsur_t[col], cb = G.col_bot[col];
+  if (cs == G.zm1[cs]) return;
+  int stat = 0;
+  double div = C[cb];
+  sol[cb] = rhs[cb] / div;
+  int c = cb;
+  for (int it = 0; c != cs && it < G.nz; ++it) {
+    const int cn = G.zp1[c];
+    ud[cn] = Cp1[c] / div;
+    div = C[cn] - Cm1[cn] * ud[cn];
+    if (div == 0.0) stat |= ST_PIVOT;
+    sol[cn] = (rhs[cn] - Cm1[cn] * sol[c]) / div;
+    c = cn;
+  }
+  if (c != cs) stat |= ST_GEOM;
+  for (int it = 0; c != cb && it < G.nz; ++it) {
+    const int cd = G.zm1[c];
+    sol[cd] -= ud[c] * sol[c];
+    c = cd;
+  }
+  for (int it = 0; it <= G.nz; ++it) {
+    var[c] = sol[c] > minvar ? sol[c] : minvar;
+    if (c == cs) break;
+    c = G.zp1[c];
+  }
+  if (stat) atomicOr(W.status, stat);
+}
+
+// implicit_vdiff_at_cc (model/hd/tracers/tracers.c:7407-7545): implicit
+// vertical diffusion of var with bottom / top fluxes fb, ft, sources Splus,
+// Sminus (may be null) and the scale factor, with no thin layers
+__global__ void k_vdiff_cols(Geo G, Work W, double *var, const double *dzcell, const double *C,
+                             const double *Cm1, const double *Cp1, const double *fb,
+                             const double *ft, const double *Splus, const double *Sminus,
+                             const double *scale, double *sol, double *ud, double dt,
+                             double dt_win, double hmin) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= G.ncol) return;
+  const int cs = W.nsur_t[col], cb = G.col_bot[col];
+  if (cs == G.zm1[cs]) return;
+  const int c2 = G.m2d[cs];
+  const int zm1 = G.zm1[cs];
+  int stat = 0;
+  // single layer (the surface in the bottom layer, :7459-7467)
+  if (zm1 == G.zm1[zm1] || !dzcell[zm1]) {
+    const double h = dzcell[cs] > hmin ? dzcell[cs] : hmin;
+    var[cs] += dt_win * (fb[c2] - ft[c2]) / h;
+    return;
+  }
+  // right-hand side (:7479-7508) into sol, the main diagonal with the
+  // negative sources into ud (both are rewritten by the sweep below)
+  int c = cb;
+  for (int it = 0; it <= G.nz; ++it) {
+    const double dzdt = dzcell[c] / dt;
+    double r = dzdt * var[c];
+    if (c == cb) r = r + fb[c2];
+    if (c == cs) r = r - ft[c2];
+    sol[c] = r;
+    ud[c] = C[c];
+    if (c == cs) break;
+    c = G.zp1[c];
+  }
+  if (c != cs) stat |= ST_GEOM;
+  if (Splus) {
+    for (int cc = cb, it = 0; it <= G.nz; cc = G.zp1[cc], ++it) {
+      sol[cc] += dzcell[cc] * Splus[cc];
+      if (cc == cs) break;
+    }
+  }
+  if (Sminus) {
+    for (int cc = cb, it = 0; it <= G.nz; cc = G.zp1[cc], ++it) {
+      ud[cc] += dzcell[cc] * Sminus[cc] / var[cc];
+      if (cc == cs) break;
+    }
+  }
+  // Thomas sweep (:7517-7526): the main diagonal B sits in ud until the row
+  // is eliminated, then ud holds the elimination factor
+  double div = ud[cb];
+  sol[cb] = sol[cb] / div;
+  c = cb;
+  for (int it = 0; c != cs && it < G.nz; ++it) {
+    const int cn = G.zp1[c];
+    const double B = ud[cn];
+    ud[cn] = Cp1[c] / div;
+    div = B - Cm1[cn] * ud[cn];
+    if (div == 0.0) stat |= ST_PIVOT;
+    sol[cn] = (sol[cn] - Cm1[cn] * sol[c]) / div;
+    c = cn;
+  }
+  // update (:7530-7536)
+  const double sc = scale[c2];
+  var[cs] += (sol[cs] - var[cs]) * sc;
+  for (int it = 0; c != cb && it < G.nz; ++it) {
+    const int cd = G.zm1[c];
+    sol[cd] -= ud[c] * sol[c];
+    var[cd] += (sol[cd] - var[cd]) * sc;
+    c = cd;
+  }
+  if (stat) atomicOr(W.status, stat);
 }
 
 // shared memory of the column kernel of the handle's precision
@@ -2065,6 +2182,77 @@ int shoc_tr_gpu_compare(shoc_tr_gpu *a, shoc_tr_gpu *b, const int *region, int n
   memcpy(sumsq_diff, out.data() + 2 * nout, nout * sizeof(double));
   memcpy(sumsq_ref, out.data() + 3 * nout, nout * sizeof(double));
   return SHOC_TR_OK;
+}
+
+// device arrays of the column-solve entry points: nine [S] fields and three
+// [S2] fields, allocated on the first call
+static int cols_buffer(shoc_tr_gpu *h) {
+  if (h->cols) return 0;
+  return dalloc(h, &h->cols, (size_t)9 * h->S + (size_t)3 * h->S2);
+}
+
+static int cols_status(shoc_tr_gpu *h) {
+  CK(cudaMemcpyAsync(h->h_status, h->W.status, 4, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemsetAsync(h->W.status, 0, 4, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return map_status(*h->h_status);
+}
+
+int shoc_tr_gpu_tridiag(shoc_tr_gpu *h, const double *C, const double *Cm1, const double *Cp1,
+                        const double *rhs, double *var, double minvar) {
+  if (!h || !C || !Cm1 || !Cp1 || !rhs || !var) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  int rc = cols_buffer(h);
+  if (rc) return rc;
+  const size_t S = (size_t)h->S, b = S * sizeof(double);
+  double *dC = h->cols, *dCm1 = dC + S, *dCp1 = dCm1 + S, *dr = dCp1 + S, *dv = dr + S;
+  double *dsol = dv + S, *dud = dsol + S;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(dC, C, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dCm1, Cm1, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dCp1, Cp1, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dr, rhs, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dv, var, b, cudaMemcpyHostToDevice, st));
+  k_tridiag<<<(h->ncol + 127) / 128, 128, 0, st>>>(h->G, h->W, dC, dCm1, dCp1, dr, dv, dsol, dud,
+                                                   minvar);
+  h->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(var, dv, b, cudaMemcpyDeviceToHost, st));
+  return cols_status(h);
+}
+
+int shoc_tr_gpu_vdiff_cols(shoc_tr_gpu *h, double *var, const double *dzcell, const double *C,
+                           const double *Cm1, const double *Cp1, const double *fb,
+                           const double *ft, const double *Splus, const double *Sminus,
+                           const double *scale, double dt) {
+  if (!h || !var || !dzcell || !C || !Cm1 || !Cp1 || !fb || !ft || !scale || !(dt > 0.0))
+    return SHOC_TR_EARG;
+  if (h->dt <= 0.0) return SHOC_TR_EARG;  // the window's dt (set_flow) is read too
+  DeviceScope dev_(h->device);
+  int rc = cols_buffer(h);
+  if (rc) return rc;
+  const size_t S = (size_t)h->S, b = S * sizeof(double), b2 = (size_t)h->S2 * sizeof(double);
+  double *dC = h->cols, *dCm1 = dC + S, *dCp1 = dCm1 + S, *ddz = dCp1 + S, *dv = ddz + S;
+  double *dsol = dv + S, *dud = dsol + S, *dsp = dud + S, *dsm = dsp + S;
+  double *dfb = dsm + S, *dft = dfb + h->S2, *dsc = dft + h->S2;
+  cudaStream_t st = h->stream;
+  CK(cudaMemcpyAsync(dC, C, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dCm1, Cm1, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dCp1, Cp1, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ddz, dzcell, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dv, var, b, cudaMemcpyHostToDevice, st));
+  if (Splus) CK(cudaMemcpyAsync(dsp, Splus, b, cudaMemcpyHostToDevice, st));
+  if (Sminus) CK(cudaMemcpyAsync(dsm, Sminus, b, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dfb, fb, b2, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dft, ft, b2, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(dsc, scale, b2, cudaMemcpyHostToDevice, st));
+  k_vdiff_cols<<<(h->ncol + 127) / 128, 128, 0, st>>>(
+      h->G, h->W, dv, ddz, dC, dCm1, dCp1, dfb, dft, Splus ? dsp : nullptr,
+      Sminus ? dsm : nullptr, dsc, dsol, dud, dt, h->dt, h->O.hmin);
+  h->launches++;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(var, dv, b, cudaMemcpyDeviceToHost, st));
+  return cols_status(h);
 }
 
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h) { return h ? (void *)h->stream : nullptr; }

@@ -23,7 +23,8 @@ EXPORTS = (
     "shoc_tr_gpu_upload_tracers", "shoc_tr_gpu_download_tracers", "shoc_tr_gpu_set_flow",
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
     "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_compare", "shoc_tr_gpu_state_size",
-    "shoc_tr_gpu_save_state", "shoc_tr_gpu_load_state", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
+    "shoc_tr_gpu_save_state", "shoc_tr_gpu_load_state", "shoc_tr_gpu_tridiag",
+    "shoc_tr_gpu_vdiff_cols", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
@@ -58,6 +59,8 @@ def lib(path=None):
     L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_compare.argtypes = [H, H, _abi.IP, C.c_int] + [_abi.DP] * 4
     L.shoc_tr_gpu_state_size.argtypes = [H, C.POINTER(C.c_size_t)]
+    L.shoc_tr_gpu_tridiag.argtypes = [H] + [_abi.DP] * 5 + [C.c_double]
+    L.shoc_tr_gpu_vdiff_cols.argtypes = [H] + [_abi.DP] * 10 + [C.c_double]
     L.shoc_tr_gpu_save_state.argtypes = [H, C.c_void_p, C.c_size_t]
     L.shoc_tr_gpu_load_state.argtypes = [H, C.c_void_p, C.c_size_t]
     L.shoc_tr_gpu_host_register.argtypes = [C.c_void_p, C.c_size_t]
@@ -228,6 +231,19 @@ class TracerStep:
             d["rms_rel"] = np.where(d["sumsq_ref"] > 0, np.sqrt(d["sumsq_diff"] / d["sumsq_ref"]),
                                     np.nan)
         return d
+
+    def tridiag(self, Cd, Cm1, Cp1, rhs, var, minvar):
+        """shoc_tr_gpu_tridiag on host arrays [sgsiz]; var updated in place."""
+        _check("tridiag", self.L.shoc_tr_gpu_tridiag(
+            self.h, _abi.dptr(Cd), _abi.dptr(Cm1), _abi.dptr(Cp1), _abi.dptr(rhs),
+            _abi.dptr(var), float(minvar)))
+
+    def vdiff_cols(self, var, dzcell, Cd, Cm1, Cp1, fb, ft, scale, dt, Splus=None, Sminus=None):
+        """shoc_tr_gpu_vdiff_cols on host arrays; var updated in place."""
+        _check("vdiff_cols", self.L.shoc_tr_gpu_vdiff_cols(
+            self.h, _abi.dptr(var), _abi.dptr(dzcell), _abi.dptr(Cd), _abi.dptr(Cm1),
+            _abi.dptr(Cp1), _abi.dptr(fb), _abi.dptr(ft), _abi.dptr(Splus), _abi.dptr(Sminus),
+            _abi.dptr(scale), float(dt)))
 
     def save_state(self):
         """The resident state as bytes (shoc_tr_gpu_save_state)."""

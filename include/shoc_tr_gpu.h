@@ -144,6 +144,34 @@ int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass);
 int shoc_tr_gpu_compare(shoc_tr_gpu *a, shoc_tr_gpu *b, const int *region, int nregion,
                         double *maxabs, double *maxref, double *sumsq_diff, double *sumsq_ref);
 
+/* The other per-column tridiagonal solves of SHOC, batched over every water
+ * column of the window (from its bottom cell to its current surface cell,
+ * nsur_t of the last step or of set_flow; dry columns are left alone), in
+ * FP64 with the reference's arithmetic (bitwise its results).  Arrays are
+ * host arrays indexed by SHOC cell, [sgsiz] (a cell carries the row of its
+ * layer; the reference gathers the rows into layer vectors first), or by 2D
+ * cell, [sgsizS].  A zero divisor returns SHOC_TR_EPIVOT where the
+ * reference quits.
+ *
+ * shoc_tr_gpu_tridiag replaces the closures' tridiagonal
+ * (model/hd/closure/MY2-5.c:499-536, called by the MY2-5, k-e and k-w
+ * closures): C (main diagonal), Cm1 (lower), Cp1 (upper), rhs; var receives
+ * max(solution, minvar).
+ *
+ * shoc_tr_gpu_vdiff_cols replaces implicit_vdiff_at_cc
+ * (model/hd/tracers/tracers.c:7407-7545) for every column at once: var is
+ * diffused in place with the coefficients C, Cm1, Cp1, the cell thicknesses
+ * dzcell, the fluxes out of the bottom and the top fb, ft [sgsizS], the
+ * source parts Splus, Sminus (NULL: none) and the scale [sgsizS]; a column
+ * whose surface lies in its bottom layer takes the reference's one-layer
+ * update with the window's dt (set_flow) and hmin.  No thin layers. */
+int shoc_tr_gpu_tridiag(shoc_tr_gpu *h, const double *C, const double *Cm1, const double *Cp1,
+                        const double *rhs, double *var, double minvar);
+int shoc_tr_gpu_vdiff_cols(shoc_tr_gpu *h, double *var, const double *dzcell, const double *C,
+                           const double *Cm1, const double *Cp1, const double *fb,
+                           const double *ft, const double *Splus, const double *Sminus,
+                           const double *scale, double dt);
+
 /* cudaStream_t of the handle, for event timing by the caller. */
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
 

@@ -43,6 +43,11 @@ def _load(name):
         L.ref_run.restype = C.c_int
         L.ref_last_message.restype = C.c_char_p
         L.ref_last_loop_seconds.restype = C.c_double
+        G, S, O, D = C.POINTER(_abi.Geom), C.POINTER(_abi.State), C.POINTER(_abi.Opts), _abi.DP
+        L.ref_tridiag.argtypes = [G, S, O, D, D, D, D, D, C.c_double]
+        L.ref_tridiag.restype = C.c_int
+        L.ref_vdiff_cols.argtypes = [G, S, O] + [D] * 10 + [C.c_double]
+        L.ref_vdiff_cols.restype = C.c_int
     _libs[name] = L
     return L
 
@@ -87,3 +92,35 @@ def max_rel_err(a, b, cells, floor=1e-300):
     a = np.asarray(a)[..., cells]
     b = np.asarray(b)[..., cells]
     return (np.abs(a - b) / np.maximum(np.abs(b), floor)).max(axis=-1)
+
+
+def _ref_call(fn_name, case, sur, nsur, *args):
+    L = _load("ref")
+    if L is None:
+        raise FileNotFoundError("reference build oracle/_ref not available")
+    keep = []
+    tr = case.tr.copy()
+    st = case.make_state(tr, sur, nsur, keep)
+    op = case.make_opts(keep)
+    return getattr(L, fn_name)(C.byref(case.win.geom), C.byref(st), C.byref(op), *args)
+
+
+def ref_tridiag(case, Cd, Cm1, Cp1, rhs, var, minvar, sur=None, nsur=None):
+    """The reference's closure tridiagonal (closure/MY2-5.c:499) on every
+    water column (surface cells nsur_t); var updated in place; status."""
+    sur = case.sur_t.copy() if sur is None else sur
+    nsur = case.nsur_t.copy() if nsur is None else nsur
+    P = _abi.dptr
+    return _ref_call("ref_tridiag", case, sur, nsur, P(Cd), P(Cm1), P(Cp1), P(rhs), P(var),
+                     C.c_double(minvar))
+
+
+def ref_vdiff_cols(case, var, dzcell, Cd, Cm1, Cp1, fb, ft, scale, dt, Splus=None,
+                   Sminus=None, sur=None, nsur=None):
+    """The reference's implicit_vdiff_at_cc (tracers.c:7407) on every water
+    column; var updated in place; status."""
+    sur = case.sur_t.copy() if sur is None else sur
+    nsur = case.nsur_t.copy() if nsur is None else nsur
+    P = _abi.dptr
+    return _ref_call("ref_vdiff_cols", case, sur, nsur, P(var), P(dzcell), P(Cd), P(Cm1),
+                     P(Cp1), P(fb), P(ft), P(Splus), P(Sminus), P(scale), C.c_double(dt))

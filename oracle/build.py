@@ -4,7 +4,8 @@
   oracle/_lib/libshoc_grid.so       the window builder (ems_b200/csrc/shoc_grid.c)
                                     compiled for the reference arm of bench.py,
                                     so that arm loads no library of the product
-  oracle/_ref/libshoc_ref.so        the reference's own model/hd/tracers/tracers.c,
+  oracle/_ref/libshoc_ref.so        the reference's own model/hd/tracers/tracers.c
+                                    and model/hd/closure/MY2-5.c (its tridiagonal),
                                     compiled unmodified, single thread
   oracle/_ref/libshoc_ref_omp.so    the same with -fopenmp -DHAVE_OMP (the
                                     reference's OpenMP tracer loop)
@@ -86,6 +87,7 @@ def ref_libs(force=False):
     for sub in ("sediments", "tracerstats", "waves", "ecology", "da"):
         inc += ["-I", os.path.join(R, "model", "lib", sub, "include")]
     srcs = [os.path.join(R, "model", "hd", "tracers", "tracers.c"),
+            os.path.join(R, "model", "hd", "closure", "MY2-5.c"),
             os.path.join(HERE, "ref", "ref_harness.c")]
     deps = srcs + [os.path.join(ROOT, "include", "shoc_tr.h")]
     for out, extra in ((outs[0], []), (outs[1], ["-fopenmp", "-DHAVE_OMP"])):

@@ -327,3 +327,106 @@ int ref_run(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
   ref_free(r);
   return rc;
 }
+
+/* ---- the other per-column tridiagonal solves ---- */
+void tridiagonal(geometry_t *window, int cs, int cb, double *C, double *Cm1, double *Cp1,
+                 double *rhs, double *var, double minvar);
+void implicit_vdiff_at_cc(geometry_t *window, window_t *windat, win_priv_t *wincon, double *var,
+                          double *Kz, double *dzcell, double *dzface, double *fb, double *ft,
+                          int *ctp, int *cbt, int cc, double *Splus, double *Sminus,
+                          double *scale, double *C, double *Cp1, double *Cm1, double dt);
+
+/* The reference's closure solve (tridiagonal, model/hd/closure/MY2-5.c:499)
+ * on every water column of the window: from the bottom cell bot_t[cc] to the
+ * surface cell st->nsur_t[cc] (a column whose surface is its sediment cell
+ * is dry and left out).  C, Cm1, Cp1 and rhs are [sgsiz] arrays by cell (the
+ * row of the cell's layer); the reference takes them by layer, so each
+ * column's rows are gathered into layer arrays first.  var [sgsiz]. */
+int ref_tridiag(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
+                const double *C, const double *Cm1, const double *Cp1, const double *rhs,
+                double *var, double minvar) {
+  ref_window *r = ref_make(g, st, op, 1);
+  geometry_t *w = r->win;
+  win_priv_t *c = r->con;
+  const int nz = g->nz;
+  w->wincon = c;
+  c->v11 = DA(nz + 1);
+  c->v12 = DA(nz + 1);
+  double *lC = DA(nz + 1), *lCm1 = DA(nz + 1), *lCp1 = DA(nz + 1), *lr = DA(nz + 1);
+  int rc = SHOC_TR_OK;
+  ref_err = 0;
+  if (setjmp(ref_jmp)) {
+    rc = ref_err ? ref_err : SHOC_TR_EUNSUPPORTED;
+  } else {
+    ref_jmp_armed = 1;
+    for (int cc = 1; cc <= g->b2_t; cc++) {
+      const int cs = st->nsur_t[cc], cb = g->bot_t[cc];
+      if (cs == g->zm1[cs]) continue;
+      for (int cl = cb, k = g->s2k[cb];; cl = g->zp1[cl], k++) {
+        lC[k] = C[cl]; lCm1[k] = Cm1[cl]; lCp1[k] = Cp1[cl]; lr[k] = rhs[cl];
+        if (cl == cs) break;
+      }
+      tridiagonal(w, cs, cb, lC, lCm1, lCp1, lr, var, minvar);
+    }
+  }
+  ref_jmp_armed = 0;
+  free(lC); free(lCm1); free(lCp1); free(lr);
+  free(c->v11); free(c->v12);
+  ref_free(r);
+  return rc;
+}
+
+/* The reference's single-column implicit diffusion (implicit_vdiff_at_cc,
+ * model/hd/tracers/tracers.c:7407) on every water column: var [sgsiz] by
+ * cell is gathered into the layer vector the reference works on (as its
+ * caller swr_assimilation does, tracers.c:4030-4045), diffused with the
+ * coefficients C, Cm1, Cp1 and thicknesses dzcell [sgsiz], the bottom and
+ * top fluxes fb, ft and the scale [sgsizS], the sources Splus, Sminus
+ * [sgsiz] (or NULL), and scattered back.  No thin layers: i4 = the surface. */
+int ref_vdiff_cols(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
+                   double *var, const double *dzcell, const double *C, const double *Cm1,
+                   const double *Cp1, const double *fb, const double *ft, const double *Splus,
+                   const double *Sminus, const double *scale, double dt) {
+  ref_window *r = ref_make(g, st, op, 1);
+  geometry_t *w = r->win;
+  window_t *d = r->dat;
+  win_priv_t *c = r->con;
+  const int nz = g->nz;
+  w->wincon = c;
+  int *ctp = IA(g->b2_t + 1), *cbt = IA(g->b2_t + 1);
+  double *temp = DA(nz + 1);
+  int n = 0;
+  for (int cc = 1; cc <= g->b2_t; cc++) {
+    const int cs = st->nsur_t[cc];
+    if (cs == g->zm1[cs]) continue;
+    n++;
+    ctp[n] = cs;
+    cbt[n] = g->bot_t[cc];
+    c->i4[n] = cs;
+  }
+  int rc = SHOC_TR_OK;
+  ref_err = 0;
+  if (setjmp(ref_jmp)) {
+    rc = ref_err ? ref_err : SHOC_TR_EUNSUPPORTED;
+  } else {
+    ref_jmp_armed = 1;
+    for (int cc = 1; cc <= n; cc++) {
+      const int cs = ctp[cc], cb = cbt[cc];
+      for (int cl = cs, k = g->s2k[cs];; cl = g->zm1[cl], k--) {
+        temp[k] = var[cl];
+        if (cl == cb) break;
+      }
+      implicit_vdiff_at_cc(w, d, c, temp, NULL, mutable(dzcell), NULL, mutable(fb),
+                           mutable(ft), ctp, cbt, cc, mutable(Splus), mutable(Sminus),
+                           mutable(scale), mutable(C), mutable(Cp1), mutable(Cm1), dt);
+      for (int cl = cs, k = g->s2k[cs];; cl = g->zm1[cl], k--) {
+        var[cl] = temp[k];
+        if (cl == cb) break;
+      }
+    }
+  }
+  ref_jmp_armed = 0;
+  free(ctp); free(cbt); free(temp);
+  ref_free(r);
+  return rc;
+}
