@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
       const double w9m = j >= 2 ? 0.5 * (dzm + dzmm) : 0.0;  // w9(j - 1)
       W.dz[cc] = dzc;
       if (fp32) W.dz32[cc] = (float)dzc;
-      if (quick) W.w5[cc] = dzm / (dzm + dzc);
+      if (quick || O.trasc == SHOC_TR_ORDER2) W.w5[cc] = dzm / (dzm + dzc);
       W.w9[cc] = w9c;
       W.dbz[cc] = 2.0 / (w9m + w9c);
       W.dfz[cc] = 2.0 / (w9c + w9p);
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     ci.cbs = cbs;
     ci.flags = flags;
     ci.ks = kb + js - 1;
-    if (staged_column(ci, bot)) ci.flags |= COL_STAGED;
+    if (O.tiled && staged_column(ci, bot)) ci.flags |= COL_STAGED;
     W.col[col] = ci;
     if ((flags & COL_SERIAL) || (list_all && !(ci.flags & COL_STAGED))) {
       int i = atomicAdd(W.serial_count, 1);
@@ -862,7 +862,11 @@ int map_status(int st) {
 
 int check_geom(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr) {
   if (!g || !o || ntr < 0) return SHOC_TR_EARG;
-  if (o->trasc != SHOC_TR_QUICKEST && o->trasc != SHOC_TR_VANLEER) return SHOC_TR_EUNSUPPORTED;
+  switch (o->trasc) {  // FFSL and LAGRANGE are not built
+    case SHOC_TR_QUICKEST: case SHOC_TR_VANLEER: case SHOC_TR_ORDER1: case SHOC_TR_ORDER2:
+    case SHOC_TR_ORDER4: case SHOC_TR_QUICKEST_CO: case SHOC_TR_ORDER2_UW: break;
+    default: return SHOC_TR_EUNSUPPORTED;
+  }
   if (g->v3_t != g->b3_t || g->b3_t != g->a3_t) return SHOC_TR_EUNSUPPORTED;  // OBC / aux cells
   if (g->v2_t != g->b2_t || g->b2_t != g->a2_t) return SHOC_TR_EUNSUPPORTED;
   if (g->nz < 1 || g->nz > kSerialMaxLayers) return SHOC_TR_EUNSUPPORTED;
@@ -1075,7 +1079,9 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
 
   // ---- options and tracers ----
   h->O.trasc = o->trasc;
-  h->O.ultimate = o->ultimate;
+  // order1 is monotonic and switches the limiter off (tracers.c:497-503)
+  h->O.ultimate = o->trasc == SHOC_TR_ORDER1 ? 0 : o->ultimate;
+  h->O.tiled = (o->trasc == SHOC_TR_QUICKEST || o->trasc == SHOC_TR_VANLEER) ? 1 : 0;
   h->O.substep =
       (o->stab & (SHOC_TR_SUB_STEP | SHOC_TR_SUB_STEP_NOSURF | SHOC_TR_SUB_STEP_TRACER)) ? 1 : 0;
   h->O.hmin = o->hmin;

@@ -104,6 +104,8 @@ struct Flow32 {
 struct Opt {
   int trasc, ultimate, substep;
   double hmin;
+  int tiled;  // the scheme has tile kernels (QUICKEST, Van Leer); else every
+              // column takes the general path
 };
 
 // Per-tracer attributes (device arrays indexed by tracer number).
@@ -210,6 +212,59 @@ __device__ __forceinline__ double ultimate_face(double cr, double F, double tm2,
   return F;
 }
 
+// Face values of the other schemes (advect's dispatch, tracers.c:1509-1527),
+// tm2..tp1 the tracer at i-2, i-1, i, i+1 of the face's cell:
+//   order2_do (:1690-1709)        d (t0 - tm1) + tm1 (d: d3 / d4 / w5)
+//   order4_do (:1757-1776)        (7 (tm1 + t0) - (tp1 + tm2)) / 12
+//   quickest_uniform (:1944-2031) QUICKEST with uniform-grid curvature
+//   order2_upwind_do (:3008-3036) the upwind pair weighted by the Courant number
+__device__ __forceinline__ double order2_face(double d, double tm1, double t0) {
+  return d * (t0 - tm1) + tm1;
+}
+__device__ __forceinline__ double order4_face(double tm2, double tm1, double t0, double tp1) {
+  return (7.0 * (tm1 + t0) - (tp1 + tm2)) / 12.0;
+}
+__device__ __forceinline__ double quickest_co_face(double cr, double tm2, double tm1, double t0,
+                                                   double tp1) {
+  double face = 0.5 * (t0 + tm1);
+  double grad = t0 - tm1;
+  double curv = 0.0;
+  if (cr > 0.0)
+    curv = t0 - 2.0 * tm1 + tm2;
+  else if (cr < 0.0)
+    curv = tp1 - 2.0 * t0 + tm1;
+  return face - 0.5 * cr * grad - (1.0 - cr * cr) * curv / 6.0;
+}
+__device__ __forceinline__ double order2_uw_face(double vel, double cn, double tm2, double tm1,
+                                                 double t0, double tp1) {
+  if (vel > 0.0) return 0.5 * (3.0 - cn) * tm1 - 0.5 * (1.0 - cn) * tm2;
+  if (vel < 0.0) return 0.5 * (3.0 - cn) * t0 - 0.5 * (1.0 - cn) * tp1;
+  return 0.0;
+}
+// order1 (:1584-1617): the upwind value times the volume flux, split by sign
+// (w6..w9 of :497-513), with no limiter
+__device__ __forceinline__ double order1_flux(double U, double tm1, double t0) {
+  const double up = 0.5 * (U + fabs(U)), dn = 0.5 * (U - fabs(U));
+  return up * tm1 + dn * t0;
+}
+
+// Face value of a horizontal face of scheme trasc before the limiter; eb: the
+// face is an interior face (w3_e1 / w3_e2), the only faces the centred and
+// second-order upwind schemes and Van Leer fill.
+__device__ __forceinline__ double hface_value(int trasc, bool eb, double cr, double vel,
+                                              const Face2D &m, double tm2, double tm1,
+                                              double t0, double tp1) {
+  switch (trasc) {
+    case SHOC_TR_QUICKEST: return quickest_face(cr, m, tm2, tm1, t0, tp1);
+    case SHOC_TR_QUICKEST_CO: return quickest_co_face(cr, tm2, tm1, t0, tp1);
+    case SHOC_TR_VANLEER: return eb ? vanleer_face(vel, cr, tm2, tm1, t0, tp1) : 0.0;
+    case SHOC_TR_ORDER2: return eb ? order2_face(m.d, tm1, t0) : 0.0;
+    case SHOC_TR_ORDER4: return eb ? order4_face(tm2, tm1, t0, tp1) : 0.0;
+    case SHOC_TR_ORDER2_UW: return eb ? order2_uw_face(vel, cr, tm2, tm1, t0, tp1) : 0.0;
+  }
+  return 0.0;
+}
+
 // Final e1 flux through the west face of wet cell c (advect + hor_diffuse):
 // tm2..tp1 = tr at xm1[xm1[c]], xm1[c], c, xp1[c].
 __device__ __forceinline__ double flux_x(const Geo &G, const Flow &F, const Work &W,
@@ -217,12 +272,11 @@ __device__ __forceinline__ double flux_x(const Geo &G, const Flow &F, const Work
                                          int c2, double tm2, double tm1, double t0,
                                          double tp1) {
   double v = 0.0;
-  if (adv) {
+  if (adv && O.trasc == SHOC_TR_ORDER1) {
+    v = order1_flux(F.u1flux3d[c], tm1, t0);
+  } else if (adv) {
     double cr = W.w6[c];
-    if (O.trasc == SHOC_TR_QUICKEST)
-      v = quickest_face(cr, G.fx[c2], tm2, tm1, t0, tp1);
-    else if (fl & CF_E1)
-      v = vanleer_face(F.u1[c], cr, tm2, tm1, t0, tp1);
+    v = hface_value(O.trasc, (fl & CF_E1) != 0, cr, F.u1[c], G.fx[c2], tm2, tm1, t0, tp1);
     if (O.ultimate && (fl & CF_E1)) v = ultimate_face(cr, v, tm2, tm1, t0, tp1);
     v *= F.u1flux3d[c];
   }
@@ -238,12 +292,11 @@ __device__ __forceinline__ double flux_y(const Geo &G, const Flow &F, const Work
                                          int c2, double tm2, double tm1, double t0,
                                          double tp1) {
   double v = 0.0;
-  if (adv) {
+  if (adv && O.trasc == SHOC_TR_ORDER1) {
+    v = order1_flux(F.u2flux3d[c], tm1, t0);
+  } else if (adv) {
     double cr = W.w7[c];
-    if (O.trasc == SHOC_TR_QUICKEST)
-      v = quickest_face(cr, G.fy[c2], tm2, tm1, t0, tp1);
-    else if (fl & CF_E2)
-      v = vanleer_face(F.u2[c], cr, tm2, tm1, t0, tp1);
+    v = hface_value(O.trasc, (fl & CF_E2) != 0, cr, F.u2[c], G.fy[c2], tm2, tm1, t0, tp1);
     if (O.ultimate && (fl & CF_E2)) v = ultimate_face(cr, v, tm2, tm1, t0, tp1);
     v *= F.u2flux3d[c];
   }
@@ -259,15 +312,24 @@ __device__ __forceinline__ double flux_y(const Geo &G, const Flow &F, const Work
 __device__ __forceinline__ double flux_z(const Flow &F, const Work &W, const Opt &O, int c,
                                          double w9m, double w90, double w9p, double tm2,
                                          double tm1, double t0, double tp1, double dtu) {
+  const double wc = F.w[c];
+  if (O.trasc == SHOC_TR_ORDER1)  // order1 (:1611-1616)
+    return dtu * (0.5 * (wc + fabs(wc)) * tm1 + 0.5 * (wc - fabs(wc)) * t0);
   double cz = W.w8[c];
   double v;
-  if (O.trasc == SHOC_TR_QUICKEST) {
-    v = quickest_zface(cz, W.w5[c], W.dbz[c], W.dfz[c], w9m, w90, w9p, tm2, tm1, t0, tp1);
-  } else {
-    v = vanleer_face(F.w[c], cz, tm2, tm1, t0, tp1);
+  switch (O.trasc) {
+    case SHOC_TR_QUICKEST:
+      v = quickest_zface(cz, W.w5[c], W.dbz[c], W.dfz[c], w9m, w90, w9p, tm2, tm1, t0, tp1);
+      break;
+    case SHOC_TR_VANLEER: v = vanleer_face(wc, cz, tm2, tm1, t0, tp1); break;
+    case SHOC_TR_QUICKEST_CO: v = quickest_co_face(cz, tm2, tm1, t0, tp1); break;
+    case SHOC_TR_ORDER2: v = order2_face(W.w5[c], tm1, t0); break;
+    case SHOC_TR_ORDER4: v = order4_face(tm2, tm1, t0, tp1); break;
+    case SHOC_TR_ORDER2_UW: v = order2_uw_face(wc, cz, tm2, tm1, t0, tp1); break;
+    default: v = 0.0;
   }
   if (O.ultimate) v = ultimate_face(cz, v, tm2, tm1, t0, tp1);
-  return v * (F.w[c] * dtu);
+  return v * (wc * dtu);
 }
 
 }  // namespace shoc
@@ -406,8 +468,12 @@ __device__ __forceinline__ void column_pass(const Geo &G, const Flow &F, const W
       double Fxe = 0.0, Fyn = 0.0;
       if (fe & CF_WET)
         Fxe = flux_x(G, F, W, O, fe, adv, hd, xp1, G.m2d[xp1], txm1, t0, txp1, tri[G.xp1[xp1]]);
+      else if (adv && O.trasc == SHOC_TR_ORDER1)  // order1 fills the ghost cells' faces too
+        Fxe = order1_flux(F.u1flux3d[xp1], t0, txp1);
       if (fn & CF_WET)
         Fyn = flux_y(G, F, W, O, fn, adv, hd, yp1, G.m2d[yp1], tym1, t0, typ1, tri[G.yp1[yp1]]);
+      else if (adv && O.trasc == SHOC_TR_ORDER1)
+        Fyn = order1_flux(F.u2flux3d[yp1], t0, typ1);
       dtr = (Fxe - Fxw + Fyn - Fys) * dtu;
     }
     if (c > s) {

@@ -23,9 +23,14 @@
 extern "C" {
 #endif
 
-/* Advection scheme flags: same values as model/hd/include/hd_params.h:332-340 */
-#define SHOC_TR_QUICKEST 0x000020
-#define SHOC_TR_VANLEER 0x000080
+/* Advection scheme flags: same values as model/hd/include/hd_params.h:331-344 */
+#define SHOC_TR_ORDER1 0x000002      /* first-order upwind (order1) */
+#define SHOC_TR_ORDER2 0x000004      /* second-order centred (order2) */
+#define SHOC_TR_ORDER4 0x000010      /* fourth-order centred, uniform grid (order4) */
+#define SHOC_TR_QUICKEST 0x000020    /* QUICKEST, non-uniform grid (quickest) */
+#define SHOC_TR_QUICKEST_CO 0x000040 /* QUICKEST, uniform grid (quickest_uniform) */
+#define SHOC_TR_VANLEER 0x000080     /* Van Leer (van_leer) */
+#define SHOC_TR_ORDER2_UW 0x002000   /* second-order upwind (order2_upwind) */
 
 /* Stability flags: same values as model/hd/include/hd_params.h:237-242 */
 #define SHOC_TR_ORIGINAL 1

@@ -135,7 +135,9 @@ void semi_lagrange_atc(geometry_t *w, window_t *d, win_priv_t *c, double *t, dou
   (void)w; (void)d; (void)c; (void)t; (void)n; (void)x;
 }
 void semi_lagrange_c(geometry_t *w, window_t *d, win_priv_t *c) { (void)w; (void)d; (void)c; }
+#if !defined(REF_WITH_VEL3D)
 void set_flux_3d(geometry_t *w, window_t *d, win_priv_t *c, int m) { (void)w; (void)d; (void)c; (void)m; }
+#endif
 void set_sbc(geometry_t *w, window_t *d, win_priv_t *c) { (void)w; (void)d; (void)c; }
 void ss_tracer(geometry_t *w, window_t *d, win_priv_t *c, int n, double *dtr, double dt) {
   (void)w; (void)d; (void)c; (void)n; (void)dtr; (void)dt;

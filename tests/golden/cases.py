@@ -40,9 +40,30 @@ CASES = {
 }
 
 
+# The other advection schemes (advect's dispatch, tracers.c:1509-1527),
+# pinned directly against the reference build (the C restatement in
+# oracle/shoc_oracle.c covers QUICKEST and Van Leer only).
+O1, O2, O4, QCO, O2UW = 0x2, 0x4, 0x10, 0x40, 0x2000
+SCHEME_CASES = {
+    "small_order1": ("small", dict(trasc=O1, ultimate=0), 10),
+    "small_order1_substeps": ("small", dict(trasc=O1, ultimate=1, dt=2000.0), 2),
+    "small_order2": ("small", dict(trasc=O2, ultimate=0), 10),
+    "small_order2_ultimate": ("small", dict(trasc=O2, ultimate=1), 10),
+    "small_order4": ("small", dict(trasc=O4, ultimate=0), 10),
+    "small_order4_ultimate_moving": ("small", dict(trasc=O4, ultimate=1,
+                                                   eta_offset=(1.9, -1.7), **MOVING), 6),
+    "small_quickest_co": ("small", dict(trasc=QCO, ultimate=0), 10),
+    "small_quickest_co_ultimate_hdiff": ("small", dict(trasc=QCO, ultimate=1,
+                                                       hdiff=(40.0, [1, 0, 1])), 10),
+    "small_order2_uw": ("small", dict(trasc=O2UW, ultimate=0), 10),
+    "small_order2_uw_ultimate_substeps": ("small", dict(trasc=O2UW, ultimate=1, dt=2000.0), 2),
+}
+ALL_CASES = dict(CASES, **SCHEME_CASES)
+
+
 def build(name):
     from ems_b200 import synth
-    wl, kw, nsteps = CASES[name]
+    wl, kw, nsteps = ALL_CASES[name]
     return synth.make(wl, **kw), nsteps
 
 

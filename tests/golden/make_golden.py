@@ -16,13 +16,13 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 sys.path.insert(0, HERE)
 
 import oracle  # noqa: E402
-from cases import CASES, build, input_digest  # noqa: E402
+from cases import ALL_CASES, build, input_digest  # noqa: E402
 
 
 def main():
     if not oracle.ref_available():
         raise SystemExit("reference build oracle/_ref missing (run oracle/build.py)")
-    for name in sys.argv[1:] or CASES:
+    for name in sys.argv[1:] or ALL_CASES:
         case, nsteps = build(name)
         rc, tr, sur, nsur, d = oracle.run_ref(case, nsteps)
         path = os.path.join(HERE, name + ".npz")

@@ -69,7 +69,7 @@ def test_bad_geometry_is_refused_at_create(field, how):
 
 
 def test_unsupported_scheme_is_refused_at_create():
-    case = synth.make("small", seed=82, trasc=0x4)  # an advection scheme the library lacks
+    case = synth.make("small", seed=82, trasc=0x080000)  # FFSL, not built
     with pytest.raises(_abi.StatusError) as e:
         gpu.TracerStep(case)
     assert e.value.code == EUNSUPPORTED

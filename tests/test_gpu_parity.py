@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "golden"))
 
 import oracle  # noqa: E402
-from cases import CASES, build, input_digest  # noqa: E402
+from cases import CASES, SCHEME_CASES, build, input_digest  # noqa: E402
 from ems_b200 import _abi, gpu, synth  # noqa: E402
 
 pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("need_gpu")]
@@ -160,3 +160,22 @@ def test_autotune_keeps_results(prec):
     b = t.download()
     t.close()
     np.testing.assert_array_equal(a[:, 1:], b[:, 1:])
+
+
+@pytest.mark.parametrize("name", sorted(SCHEME_CASES))
+def test_other_schemes_match_reference_fixture(name):
+    """ORDER1, ORDER2, ORDER4, QUICKEST_CO and ORDER2_UW, with and without
+    ULTIMATE, sub-steps, a moving surface and horizontal diffusion: bitwise
+    equal to the reference's own tracers.c (tests/golden, make_golden.py)."""
+    case, nsteps = build(name)
+    g = np.load(os.path.join(HERE, "golden", name + ".npz"))
+    assert input_digest(case) == str(g["digest"])
+    tr, sur, nsur, d = run_resident(case, nsteps)
+    np.testing.assert_array_equal(sur, g["sur_t"])
+    np.testing.assert_array_equal(nsur, g["nsur_t"])
+    assert_same(tr, g["tr"], case, name)
+    # the same scheme with FP32 storage (FP64 arithmetic in the general path)
+    tr32 = run_resident(case, nsteps, precision=gpu.FP32_MIXED)[0]
+    wet = case.win.wet_cells()
+    err = np.abs(tr32[:, wet] - g["tr"][:, wet]).max(axis=1) / np.abs(g["tr"][:, wet]).max(axis=1)
+    assert np.all(err <= 1e-5), err

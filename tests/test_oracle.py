@@ -89,3 +89,23 @@ def test_substep_limit_is_an_error():
     assert rc == 1
     if oracle.ref_available():
         assert oracle.run_ref(case, 1)[0] == 1
+
+
+def test_scheme_fixtures_are_distinct_and_reproducible():
+    """The other schemes' fixtures come from the same regenerated inputs and
+    differ from each other and from QUICKEST (each scheme really ran)."""
+    from cases import SCHEME_CASES
+    seen = {}
+    for name in sorted(SCHEME_CASES):
+        case, nsteps = build(name)
+        g = load_golden(name)
+        assert input_digest(case) == str(g["digest"]) and int(g["status"]) == 0
+        seen[name] = g["tr"][:, 1:]
+    base = load_golden("small_quickest_ultimate")["tr"][:, 1:]
+    for a in ("small_order1", "small_order2", "small_order4", "small_quickest_co",
+              "small_order2_uw"):
+        assert np.abs(seen[a] - base).max() > 0.0
+        for b in ("small_order1", "small_order2", "small_order4", "small_quickest_co",
+                  "small_order2_uw"):
+            if a < b:
+                assert np.abs(seen[a] - seen[b]).max() > 0.0, (a, b)
