@@ -75,6 +75,10 @@ struct shoc_tr_gpu {
   double *fzs64 = nullptr;            // the same, FP64 path
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
   double *cols = nullptr;             // column-solve entry points: their device arrays
+  int *halo_send = nullptr, *halo_recv = nullptr;  // halo exchange plan (device cell lists)
+  int *colown = nullptr;              // columns counted in the sub-step minimum (null: all)
+  double dmin_set = 0.0;              // sub-step minimum imposed by the caller (0: own)
+  int nhalo_send = 0, nhalo_recv = 0;
   Fused fu{};                         // fused FP32-mixed sub-step (k_step32): tiles, carry
   bool fused = false;                 // FP32-mixed sub-steps run k_step32
   size_t fused_bytes = 0;             // its dynamic shared memory
@@ -212,9 +216,12 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
 // list_all: put every column the tile kernels do not handle on the
 // general-path list (else only the tracer-coupled thin-surface columns).
 // fp32: also write the FP32 thickness and LU factors.
+// own (or null): 1 for the columns whose cells count in the sub-step minimum
+// (a strip of a decomposed basin counts its own columns, not its halo).
+// probe: compute the minimum only and leave the surface vectors as they are.
 __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Tile Tl,
                                                 int any_vdiff, int *counts, int list_all,
-                                                int fp32) {
+                                                int fp32, const int *own, int probe) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   double dtmin = __longlong_as_double(0x7ff0000000000000ll);
   if (col < G.ncol) {
@@ -234,8 +241,11 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     const double etat = F.eta[top];
     while (jn > 0 && G.gridz[cell(jn)] >= etat) --jn;
     int nsur = cell(jn);
-    W.sur_t[col] = sur;
-    W.nsur_t[col] = nsur;
+    if (!probe) {
+      W.sur_t[col] = sur;
+      W.nsur_t[col] = nsur;
+    }
+    const bool counts_min = !own || own[col];
     const int js0 = jof(sur);
     // cells-to-process membership (:5778-5800): s is the lower of the two
     int s = sur > nsur ? sur : nsur;
@@ -281,7 +291,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
       if (j <= jn && ja < 0 && !dzc) ja = j;
       if (wet && j <= js) {
         nc++;
-        if (substep) {
+        if (substep && counts_min) {
           const int xp = G.xp1[cc], yp = G.yp1[cc], zp = cell(j < nk ? j + 1 : nk);
           double d4 = 0.5 * (F.u1[cc] + F.u1[xp]);
           if (fabs(d4) < kMinVal) d4 = kMinVal;
@@ -493,13 +503,16 @@ __global__ void k_khfac(Geo G, Flow F, float *khx, float *khy) {
 
 // carry (FP32-mixed fused path, else null): [ntr][ncol] mass the stored
 // values owe each column, part of the state's mass.
+// colreg (or null): the region of each column; only region `reg` is summed.
 template <class TR>
-__global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry, double *out) {
+__global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry, double *out,
+                       const int *colreg = nullptr, int reg = 0) {
   const int n = blockIdx.y;
   const TR *t = tr + (size_t)n * G.S;
   double s = 0.0, comp = 0.0;
   for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
        col += gridDim.x * blockDim.x) {
+    if (colreg && colreg[col] != reg) continue;
     const int top = G.col_top[col], bot = G.col_bot[col];
     int c = W.nsur_t[col];
     if (n >= G.colntr[col]) continue;  // tracer not carried in this column
@@ -676,6 +689,31 @@ __global__ void k_vdiff_cols(Geo G, Work W, double *var, const double *dzcell, c
     c = cd;
   }
   if (stat) atomicOr(W.status, stat);
+}
+
+// Halo exchange of a strip of a decomposed basin: gather the send cells of
+// every tracer into a contiguous buffer, or scatter a buffer into the
+// receive cells of both tracer buffers.
+template <class TR>
+__global__ void k_halo_pack(const TR *tr, int S, int ntr, const int *cells, int n, TR *buf) {
+  const long long tot = (long long)ntr * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / n), j = (int)(i % n);
+    buf[i] = tr[(size_t)t * S + cells[j]];
+  }
+}
+template <class TR>
+__global__ void k_halo_unpack(TR *tra, TR *trb, int S, int ntr, const int *cells, int n,
+                              const TR *buf) {
+  const long long tot = (long long)ntr * n;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int t = (int)(i / n), j = (int)(i % n);
+    const size_t o = (size_t)t * S + cells[j];
+    tra[o] = buf[i];
+    trb[o] = buf[i];
+  }
 }
 
 // shared memory of the column kernel of the handle's precision
@@ -1319,7 +1357,8 @@ int launch_part_a(shoc_tr_gpu *h, int cur, bool lateral = true) {
   if (lateral) launch_lateral(h, cur, h->T);
   int nb = (h->ncol + 127) / 128;
   k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->tl, h->any_vdiff ? 1 : 0, h->d_counts,
-                               h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0);
+                               h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0, h->colown,
+                               0);
   h->launches++;
   CK(cudaGetLastError());
   return 0;
@@ -1518,6 +1557,7 @@ int probe_schedule(shoc_tr_gpu *h, bool lateral, Sched &s) {
   double dmin;
   unsigned long long b = *h->h_dtm;
   memcpy(&dmin, &b, 8);
+  if (h->dmin_set > 0.0) dmin = h->dmin_set;  // the basin-wide minimum, given
   rc = make_schedule(h, dmin, s);
   if (rc) h->last_status = rc;
   return rc;
@@ -2259,6 +2299,161 @@ int shoc_tr_gpu_vdiff_cols(shoc_tr_gpu *h, double *var, const double *dzcell, co
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(var, dv, b, cudaMemcpyDeviceToHost, st));
   return cols_status(h);
+}
+
+int shoc_tr_gpu_halo_plan(shoc_tr_gpu *h, int nsend, const int *send_cells, int nrecv,
+                          const int *recv_cells) {
+  if (!h || nsend < 0 || nrecv < 0 || (nsend && !send_cells) || (nrecv && !recv_cells))
+    return SHOC_TR_EARG;
+  for (int i = 0; i < nsend; i++)
+    if (send_cells[i] < 1 || send_cells[i] >= h->S) return SHOC_TR_EARG;
+  for (int i = 0; i < nrecv; i++)
+    if (recv_cells[i] < 1 || recv_cells[i] >= h->S) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  int rc;
+  if (nsend > h->nhalo_send && (rc = dalloc(h, &h->halo_send, (size_t)nsend))) return rc;
+  if (nrecv > h->nhalo_recv && (rc = dalloc(h, &h->halo_recv, (size_t)nrecv))) return rc;
+  if (nsend)
+    CK(cudaMemcpy(h->halo_send, send_cells, (size_t)nsend * sizeof(int), cudaMemcpyHostToDevice));
+  if (nrecv)
+    CK(cudaMemcpy(h->halo_recv, recv_cells, (size_t)nrecv * sizeof(int), cudaMemcpyHostToDevice));
+  h->nhalo_send = nsend;
+  h->nhalo_recv = nrecv;
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_halo_pack(shoc_tr_gpu *h, void *buf) {
+  if (!h || (h->nhalo_send && !buf)) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  const int n = h->nhalo_send;
+  if (n && h->ntr) {
+    const long long tot = (long long)n * h->ntr;
+    const int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 8);
+    if (h->esize == sizeof(float))
+      k_halo_pack<float><<<blocks, 256, 0, h->stream>>>((const float *)h->tr[h->cur], h->S,
+                                                        h->ntr, h->halo_send, n, (float *)buf);
+    else
+      k_halo_pack<double><<<blocks, 256, 0, h->stream>>>((const double *)h->tr[h->cur], h->S,
+                                                         h->ntr, h->halo_send, n, (double *)buf);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_halo_unpack(shoc_tr_gpu *h, const void *buf) {
+  if (!h || (h->nhalo_recv && !buf)) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  const int n = h->nhalo_recv;
+  if (n && h->ntr) {
+    const long long tot = (long long)n * h->ntr;
+    const int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 8);
+    if (h->esize == sizeof(float))
+      k_halo_unpack<float><<<blocks, 256, 0, h->stream>>>(
+          (float *)h->tr[h->cur], (float *)h->tr[h->cur ^ 1], h->S, h->ntr, h->halo_recv, n,
+          (const float *)buf);
+    else
+      k_halo_unpack<double><<<blocks, 256, 0, h->stream>>>(
+          (double *)h->tr[h->cur], (double *)h->tr[h->cur ^ 1], h->S, h->ntr, h->halo_recv, n,
+          (const double *)buf);
+    h->launches++;
+    CK(cudaGetLastError());
+  }
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_mass_region(shoc_tr_gpu *h, const int *region, int reg, double *mass) {
+  if (!h || !region || !mass) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  const int nb = 148 * 2;
+  std::vector<int> top(h->ncol), cr(h->ncol);
+  CK(cudaMemcpyAsync(top.data(), h->G.col_top, (size_t)h->ncol * sizeof(int),
+                     cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int c = 0; c < h->ncol; c++) cr[c] = region[top[c]];
+  char *buf = nullptr;
+  const size_t pb = (size_t)nb * std::max(h->ntr, 1) * sizeof(double);
+  CK(cudaMallocAsync((void **)&buf, pb + (size_t)h->ncol * sizeof(int), h->stream));
+  double *part = (double *)buf;
+  int *dreg = (int *)(buf + pb);
+  CK(cudaMemcpyAsync(dreg, cr.data(), (size_t)h->ncol * sizeof(int), cudaMemcpyHostToDevice,
+                     h->stream));
+  if (h->ntr > 0) {
+    if (h->esize == sizeof(float))
+      k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
+          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part, dreg, reg);
+    else
+      k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
+          h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part, dreg, reg);
+    h->launches++;
+  }
+  std::vector<double> hp((size_t)nb * h->ntr);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream));
+  CK(cudaFreeAsync(buf, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  for (int n = 0; n < h->ntr; n++) {
+    double s = 0.0, comp = 0.0;
+    for (int b = 0; b < nb; b++) {
+      double v = hp[(size_t)n * nb + b], u = s + v;
+      comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
+      s = u;
+    }
+    mass[n] = s + comp;
+  }
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_set_owned(shoc_tr_gpu *h, const int *owned2d) {
+  if (!h) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  if (!owned2d) {
+    h->colown = nullptr;  // every column counts again (the array stays allocated)
+    return SHOC_TR_OK;
+  }
+  std::vector<int> top(h->ncol), own(h->ncol);
+  CK(cudaMemcpy(top.data(), h->G.col_top, (size_t)h->ncol * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int c = 0; c < h->ncol; c++) own[c] = owned2d[top[c]] ? 1 : 0;
+  int *d = nullptr;
+  int rc = dupload(h, &d, own.data(), (size_t)h->ncol);
+  if (rc) return rc;
+  h->colown = d;
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_substep_min(shoc_tr_gpu *h, double *dmin) {
+  if (!h || !dmin || h->dt <= 0.0) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  cudaStream_t st = h->stream;
+  k_reset<<<1, 32, 0, st>>>(h->W, h->d_counts);
+  const int nb = (h->ncol + 127) / 128;
+  k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->tl, h->any_vdiff ? 1 : 0, h->d_counts,
+                               h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0, h->colown,
+                               1);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(h->h_dtm, h->W.dtm_bits, 8, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  unsigned long long b = *h->h_dtm;
+  memcpy(dmin, &b, 8);
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_set_substep_min(shoc_tr_gpu *h, double dmin) {
+  if (!h || dmin < 0.0) return SHOC_TR_EARG;
+  if (dmin != h->dmin_set) {
+    DeviceScope dev_(h->device);
+    h->dmin_set = dmin;
+    for (int i = 0; i < 2; i++)
+      if (h->graph[i]) {
+        cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+      }
+    h->have_sched = false;
+    h->probe_left = 2;
+  }
+  return SHOC_TR_OK;
 }
 
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h) { return h ? (void *)h->stream : nullptr; }

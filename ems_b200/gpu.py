@@ -24,7 +24,9 @@ EXPORTS = (
     "shoc_tr_gpu_get_surface", "shoc_tr_gpu_run", "shoc_tr_gpu_sync", "shoc_tr_gpu_mass",
     "shoc_tr_gpu_mass_noalloc", "shoc_tr_gpu_compare", "shoc_tr_gpu_state_size",
     "shoc_tr_gpu_save_state", "shoc_tr_gpu_load_state", "shoc_tr_gpu_tridiag",
-    "shoc_tr_gpu_vdiff_cols", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
+    "shoc_tr_gpu_vdiff_cols", "shoc_tr_gpu_halo_plan", "shoc_tr_gpu_halo_pack",
+    "shoc_tr_gpu_halo_unpack", "shoc_tr_gpu_mass_region", "shoc_tr_gpu_set_owned",
+    "shoc_tr_gpu_substep_min", "shoc_tr_gpu_set_substep_min", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror",
@@ -59,6 +61,13 @@ def lib(path=None):
     L.shoc_tr_gpu_mass_noalloc.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_compare.argtypes = [H, H, _abi.IP, C.c_int] + [_abi.DP] * 4
     L.shoc_tr_gpu_state_size.argtypes = [H, C.POINTER(C.c_size_t)]
+    L.shoc_tr_gpu_halo_plan.argtypes = [H, C.c_int, _abi.IP, C.c_int, _abi.IP]
+    L.shoc_tr_gpu_halo_pack.argtypes = [H, C.c_void_p]
+    L.shoc_tr_gpu_halo_unpack.argtypes = [H, C.c_void_p]
+    L.shoc_tr_gpu_mass_region.argtypes = [H, _abi.IP, C.c_int, _abi.DP]
+    L.shoc_tr_gpu_set_owned.argtypes = [H, _abi.IP]
+    L.shoc_tr_gpu_substep_min.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_set_substep_min.argtypes = [H, C.c_double]
     L.shoc_tr_gpu_tridiag.argtypes = [H] + [_abi.DP] * 5 + [C.c_double]
     L.shoc_tr_gpu_vdiff_cols.argtypes = [H] + [_abi.DP] * 10 + [C.c_double]
     L.shoc_tr_gpu_save_state.argtypes = [H, C.c_void_p, C.c_size_t]
@@ -244,6 +253,38 @@ class TracerStep:
             self.h, _abi.dptr(var), _abi.dptr(dzcell), _abi.dptr(Cd), _abi.dptr(Cm1),
             _abi.dptr(Cp1), _abi.dptr(fb), _abi.dptr(ft), _abi.dptr(Splus), _abi.dptr(Sminus),
             _abi.dptr(scale), float(dt)))
+
+    def halo_plan(self, send_cells, recv_cells):
+        s = np.ascontiguousarray(send_cells, np.int32)
+        r = np.ascontiguousarray(recv_cells, np.int32)
+        _check("halo_plan", self.L.shoc_tr_gpu_halo_plan(self.h, len(s), _abi.iptr(s), len(r),
+                                                         _abi.iptr(r)))
+
+    def halo_pack(self, dev_ptr):
+        """Send-cell values of every tracer into device memory at dev_ptr."""
+        _check("halo_pack", self.L.shoc_tr_gpu_halo_pack(self.h, C.c_void_p(dev_ptr)))
+
+    def halo_unpack(self, dev_ptr):
+        _check("halo_unpack", self.L.shoc_tr_gpu_halo_unpack(self.h, C.c_void_p(dev_ptr)))
+
+    def mass_region(self, region, reg):
+        m = np.zeros(self.case.ntr)
+        region = np.ascontiguousarray(region, np.int32)
+        _check("mass_region", self.L.shoc_tr_gpu_mass_region(self.h, _abi.iptr(region), int(reg),
+                                                             _abi.dptr(m)))
+        return m
+
+    def set_owned(self, owned2d):
+        o = None if owned2d is None else np.ascontiguousarray(owned2d, np.int32)
+        _check("set_owned", self.L.shoc_tr_gpu_set_owned(self.h, _abi.iptr(o)))
+
+    def substep_min(self):
+        d = np.zeros(1)
+        _check("substep_min", self.L.shoc_tr_gpu_substep_min(self.h, _abi.dptr(d)))
+        return float(d[0])
+
+    def set_substep_min(self, dmin):
+        _check("set_substep_min", self.L.shoc_tr_gpu_set_substep_min(self.h, float(dmin)))
 
     def save_state(self):
         """The resident state as bytes (shoc_tr_gpu_save_state)."""

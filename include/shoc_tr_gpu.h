@@ -172,6 +172,46 @@ int shoc_tr_gpu_vdiff_cols(shoc_tr_gpu *h, double *var, const double *dzcell, co
                            const double *ft, const double *Splus, const double *Sminus,
                            const double *scale, double dt);
 
+/* One basin decomposed over several GPUs: each GPU steps one strip of
+ * columns as its own window, widened by halo columns that are copies of its
+ * neighbours' columns.  QUICKEST and ULTIMATE reach two cells across a face
+ * (tracers.c:1854-1855, :3528-3530), so with halos 2 x (sub-steps per step)
+ * columns wide, exchanged once per step, every owned column steps exactly as
+ * in the undivided basin (the halos' outer columns go wrong and are
+ * overwritten at the next exchange).  This replaces, for this path, SHOC's
+ * window transfers (win_data_fill_3d / win_data_empty_3d,
+ * model/hd/slaves/transfers.c:349,769, over the MPI buffers of
+ * model/hd/slaves/TransferBuffer.cpp:282-443); the caller moves the buffers
+ * between GPUs (NCCL send/recv, or a peer copy into a local buffer).
+ *   halo_plan    the cells this window sends and receives (SHOC cell
+ *                numbers, host arrays; copied to the device).
+ *   halo_pack    writes every tracer's send-cell values into buf (device
+ *                memory, [ntr][nsend] values of the handle's precision) and
+ *                waits for its stream, so buf is ready for the transfer.
+ *   halo_unpack  enqueues on the handle's stream the copy of buf ([ntr][nrecv]
+ *                values, device memory) into the receive cells of both
+ *                tracer buffers; the next run sees it.
+ *   mass_region  shoc_tr_gpu_mass over the columns whose 2D cell has
+ *                region[c2] == reg (a strip's own columns). */
+int shoc_tr_gpu_halo_plan(shoc_tr_gpu *h, int nsend, const int *send_cells, int nrecv,
+                          const int *recv_cells);
+int shoc_tr_gpu_halo_pack(shoc_tr_gpu *h, void *buf);
+int shoc_tr_gpu_halo_unpack(shoc_tr_gpu *h, const void *buf);
+int shoc_tr_gpu_mass_region(shoc_tr_gpu *h, const int *region, int reg, double *mass);
+/* The sub-step length of a step is the basin-wide minimum of the stability
+ * criterion (tracers.c:591-668): a strip must take the basin's, not its own.
+ *   set_owned        owned2d[sgsizS] (1: the strip's own column, 0: halo;
+ *                    NULL: every column) -- only owned columns count below.
+ *   substep_min      the criterion's minimum over the owned columns for the
+ *                    current flow and surface (+inf: no sub-stepping
+ *                    needed); changes no state.
+ *   set_substep_min  the basin-wide minimum (the smallest substep_min of
+ *                    all strips) the window's steps then use; 0 goes back to
+ *                    the window's own.  Call after set_flow, before run. */
+int shoc_tr_gpu_set_owned(shoc_tr_gpu *h, const int *owned2d);
+int shoc_tr_gpu_substep_min(shoc_tr_gpu *h, double *dmin);
+int shoc_tr_gpu_set_substep_min(shoc_tr_gpu *h, double dmin);
+
 /* cudaStream_t of the handle, for event timing by the caller. */
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
 

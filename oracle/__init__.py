@@ -30,6 +30,10 @@ def _load(name):
         L.oracle_run.argtypes = [C.POINTER(_abi.Geom), C.POINTER(_abi.State),
                                  C.POINTER(_abi.Opts), C.c_int, C.POINTER(_abi.Diag)]
         L.oracle_run.restype = C.c_int
+        L.oracle_set_owned.argtypes = [_abi.IP]
+        L.oracle_set_owned.restype = None
+        L.oracle_set_substep_min.argtypes = [C.c_double]
+        L.oracle_set_substep_min.restype = None
     else:
         fname = "libshoc_ref_omp.so" if name == "ref_omp" else "libshoc_ref.so"
         path = os.path.join(HERE, "_ref", fname)
@@ -124,3 +128,17 @@ def ref_vdiff_cols(case, var, dzcell, Cd, Cm1, Cp1, fb, ft, scale, dt, Splus=Non
     P = _abi.dptr
     return _ref_call("ref_vdiff_cols", case, sur, nsur, P(var), P(dzcell), P(Cd), P(Cm1),
                      P(Cp1), P(fb), P(ft), P(Splus), P(Sminus), P(scale), C.c_double(dt))
+
+
+def set_strip(owned2d=None, dmin=0.0):
+    """The oracle steps a strip of a decomposed basin: only owned2d's columns
+    count in its sub-step minimum, and dmin (> 0) is the basin-wide minimum
+    it uses.  set_strip() goes back to whole windows."""
+    L = _load("oracle")
+    global _owned_keep
+    _owned_keep = None if owned2d is None else np.ascontiguousarray(owned2d, np.int32)
+    L.oracle_set_owned(_abi.iptr(_owned_keep))
+    L.oracle_set_substep_min(float(dmin))
+
+
+_owned_keep = None

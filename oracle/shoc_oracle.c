@@ -14,6 +14,14 @@
 #include "shoc_oracle.h"
 
 #define SF 0.8          /* fraction of the Courant limit, tracers.c:427 */
+
+/* Strips of a decomposed basin (tests of ems_b200.decomp): the columns whose
+ * cells count in the sub-step minimum (owned2d[c2] != 0; NULL: all), and a
+ * basin-wide minimum imposed on the schedule (0: the window's own). */
+static const int *oracle_owned = NULL;
+static double oracle_dmin_given = 0.0;
+void oracle_set_owned(const int *owned2d) { oracle_owned = owned2d; }
+void oracle_set_substep_min(double dmin) { oracle_dmin_given = dmin; }
 #define MINVAL 1e-10    /* minimum velocity, tracers.c:428 */
 #define ITERMAX 20      /* maximum sub-steps, tracers.c:430 */
 #define CLIP_EPS 1e-5   /* tr_bounds clipping threshold, tracers.c:3230 */
@@ -415,6 +423,7 @@ static int advect_diffuse(oracle_ctx *o, const shoc_tr_geom *g, shoc_tr_state *s
   if (op->stab & (SHOC_TR_SUB_STEP | SHOC_TR_SUB_STEP_NOSURF | SHOC_TR_SUB_STEP_TRACER)) {
     for (int cc = 1; cc <= vc; cc++) {
       int c = o->s1[cc], c2 = g->m2d[c];
+      if (oracle_owned && !oracle_owned[c2]) continue;
       int xp1 = g->xp1[c], yp1 = g->yp1[c], zp1 = g->zp1[c];
       double d4 = 0.5 * (u1[c] + u1[xp1]);
       if (fabs(d4) < MINVAL) d4 = MINVAL;
@@ -430,6 +439,11 @@ static int advect_diffuse(oracle_ctx *o, const shoc_tr_geom *g, shoc_tr_state *s
       if (d3 > 0.0 && d3 < dtm) dtm = d3;
     }
     if (dtm != dtu) dtm = floor(dtm);
+    if (oracle_dmin_given > 0.0) {  /* a decomposed basin's minimum */
+      dtm = dtu;
+      if (oracle_dmin_given < dtm) dtm = oracle_dmin_given;
+      if (dtm != dtu) dtm = floor(dtm);
+    }
   }
   if (diag) diag->dtm = dtm;
   if (dtm == 0.0 || (int)(dtu / dtm) > ITERMAX) return SHOC_TR_ESUBSTEP;

@@ -35,6 +35,12 @@ void oracle_destroy(oracle_ctx *o);
 int oracle_step(oracle_ctx *o, const shoc_tr_geom *g, shoc_tr_state *st,
                 const shoc_tr_opts *op, shoc_tr_diag *diag);
 
+/* Strips of a decomposed basin: only columns with owned2d[c2] != 0 count in
+ * the sub-step minimum (NULL: all; the array must outlive the steps), and a
+ * given basin-wide minimum replaces the window's own (0: none). */
+void oracle_set_owned(const int *owned2d);
+void oracle_set_substep_min(double dmin);
+
 /* nsteps steps; stops at the first non-zero status. */
 int oracle_run(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op,
                int nsteps, shoc_tr_diag *diag);
