@@ -405,6 +405,15 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     float *Aj = A + w * nd * 32 + lane;
     float *Sj = Sv + w * nd * 32 + lane;
     const bool steady = F.eta[c2] == F.oldeta[c2];
+    const int *const C0 = colC + (kb - kbase) * 32 + lane;
+    const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
+    const int nk = ks - kb;  // cells below the surface cell
+    // the water depth the carry is spread over, and 1 / dt for the FP64
+    // diagonal of the residual (dz / dt exactly, so the refined solve keeps
+    // the same column mass as the mass diagnostic measures)
+    double H = 0.0;
+    for (int j = 0; j <= nk; ++j) H += W.dz[C0[j * 32]];
+    const double idt = 1.0 / F.dt;
     long long nwarn = 0;
     for (int slot = w; slot < T.nslot; slot += nwb) {
       const int n = T.slot_tr[slot];
@@ -419,9 +428,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       float *to = tro + (size_t)n * G.S;
       float *const A0 = Aj + (kb - kbase) * 32;
       float *const S0 = Sj + (kb - kbase) * 32;
-      const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
-      const int *const C0 = colC + (kb - kbase) * 32 + lane;
-      const int nk = ks - kb;  // cells below the surface cell
       // the column's values: advection results below the surface (advected
       // tracers) or the old values (the rest, every layer)
       if (tbdy) {
@@ -439,44 +445,28 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       const double dzs = W.dz[ci.s];
       double carry_in = 0.0;
       if (Fu.carry && steady) carry_in = Fu.carry[(size_t)n * G.ncol + col];
+      // the carry goes back as a uniform shift of the column's values
+      const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
       // FP64 mass bookkeeping per unit area: what the step computed (mx*) and
       // what is stored (ms*), compensated sums
       double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
-      f32::neumaier_add(mxs, mxc, carry_in * ia);
+      if (H > 0.0) f32::neumaier_add(mxs, mxc, carry_in * ia);
       long long nw = 0;
       float fwd = 0.f;
-      double as64;  // the surface row's value in FP64 (with the carry put back)
+      double vs = ts_old;  // the surface value
       bool bad = false;
       if (!tbdy) {
         for (int j = 0; j < nk; ++j)
           f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
-        const double vs = (double)A0[nk * 32];
+        vs = (double)A0[nk * 32];
         f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
-        as64 = dzs > 0.0 ? vs + carry_in * ia / dzs : vs;
         for (int j = nk + 1; j < nz - kb; ++j) {
           to[C0[j * 32]] = A0[j * 32];
           bad |= isnan(A0[j * 32]);
         }
-        if (solve) {
-          for (int j = 0; j < nk; ++j) {
-            const float4 lu = L0[j * 32];
-            fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
-            S0[j * 32] = fwd;
-          }
-          A0[nk * 32] = (float)as64;
-          const float4 lu = L0[nk * 32];
-          S0[nk * 32] = (lu.x * A0[nk * 32] - lu.y * fwd) * lu.z;
-        } else {
-          for (int j = 0; j < nk; ++j) {
-            to[C0[j * 32]] = A0[j * 32];
-            bad |= isnan(A0[j * 32]);
-            f32::neumaier_add(mss, msc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
-          }
-        }
       } else {
         // tr_bounds clip and range check (:3278-3293) of the cells below the
         // surface; a < mn and a > mx of a float a, exactly, as float compares
-        const double a_below = nk > 0 ? (double)A0[(nk - 1) * 32] : 0.0;
         const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
         const bool clip = mn <= kClipEps;
         f32::neumaier_add(mxs, mxc, accM[slot * 32 + lane]);
@@ -487,19 +477,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
             a = mnf;
           }
           nw += (a < mn_up || a > mx_dn);
-          if (solve) {
-            A0[j * 32] = a;
-            const float4 lu = L0[j * 32];
-            fwd = (lu.x * a - lu.y * fwd) * lu.z;
-            S0[j * 32] = fwd;
-          } else {
-            to[C0[j * 32]] = a;
-            bad |= isnan(a);
-            f32::neumaier_add(mss, msc, __dmul_rn((double)a, W.dz[C0[j * 32]]));
-          }
+          A0[j * 32] = a;
         }
+        const double a_below = nk > 0 ? (double)A0[(nk - 1) * 32] : 0.0;
         // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
-        double vs = ts_old;
         if (adv) {
           const double Fzb_s = (double)accF[slot * 32 + lane];
           const double wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
@@ -519,40 +500,47 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
         if (mn <= kClipEps && vs < mn) vs = mn;
         if (vs < mn || vs > mx) ++nw;
+        bad |= isnan(vs);
         f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
-        as64 = dzs > 0.0 ? vs + carry_in * ia / dzs : vs;
         const float vs32 = (float)vs;
         for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
-        if (solve) {
-          const float4 lu = L0[nk * 32];
-          A0[nk * 32] = (float)as64;
-          S0[nk * 32] = (lu.x * A0[nk * 32] - lu.y * fwd) * lu.z;
-        }
       }
-      if (vdf && single) {
+      if (!solve) {
+        // the values as they are, plus the carry's shift (tr_bounds has run)
+        for (int j = 0; j < nk; ++j) {
+          const double dz = W.dz[C0[j * 32]];
+          const float fin = (float)((double)A0[j * 32] + dl);
+          to[C0[j * 32]] = fin;
+          bad |= isnan(fin);
+          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dz));
+        }
         const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-        const float fin = (float)(as64 + F.dt * (0.0 - 0.0) / h);
-        to[ci.s] = fin;
-        bad |= isnan(fin);
-        f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
-      } else if (!solve) {
-        const float fin = (float)as64;
+        const float fin = (vdf && single) ? (float)(vs + dl + F.dt * (0.0 - 0.0) / h)
+                                          : (float)(vs + dl);
         to[ci.s] = fin;
         bad |= isnan(fin);
         f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
       } else {
+        A0[nk * 32] = (float)vs;
+        // FP32 forward sweep
+        for (int j = 0; j <= nk; ++j) {
+          const float4 lu = L0[j * 32];
+          fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
+          S0[j * 32] = fwd;
+        }
         // back substitution (FP32) and, one row behind, the FP64 residual
-        //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
+        //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
         // (cp1(j) = cm1(j+1)); the surface row's value is the FP64 one
         float x1 = S0[nk * 32];
         float4 l1 = L0[nk * 32];
         double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
+        double dzdt1 = dzs * idt;
         for (int j = nk - 1; j >= 0; --j) {
           const float x = S0[j * 32] - l1.w * x1;
           S0[j * 32] = x;
           const double xd = (double)x, l1y = (double)l1.y;
-          const double aj1 = (j + 1 == nk) ? as64 : (double)A0[(j + 1) * 32];
-          double r = (double)l1.x * (aj1 - xd1) - l1y * (xd - xd1);
+          const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * 32]) + dl;
+          double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
           if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
           A0[(j + 1) * 32] = (float)r;
           x1 = x;
@@ -560,10 +548,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
           xd1 = xd;
           l2y = l1y;
           l1 = L0[j * 32];
+          dzdt1 = W.dz[C0[j * 32]] * idt;
         }
         {
-          const double a0 = (nk == 0) ? as64 : (double)A0[0];
-          double r = (double)l1.x * (a0 - xd1) - (double)l1.y * (xd1 - xd1);
+          const double a0 = ((nk == 0) ? vs : (double)A0[0]) + dl;
+          double r = dzdt1 * (a0 - xd1) - (double)l1.y * (xd1 - xd1);
           if (nk > 0) r = r - l2y * (xd2 - xd1);
           A0[0] = (float)r;
         }

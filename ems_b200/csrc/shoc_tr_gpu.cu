@@ -1684,9 +1684,6 @@ int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
     CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
     k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S);
     h->launches++;
-    if (h->fu.carry)
-      CK(cudaMemsetAsync(h->fu.carry + (size_t)n * h->ncol, 0, (size_t)h->ncol * sizeof(double),
-                         s));
   }
   return 0;
 }

@@ -67,7 +67,11 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h);
  * the later ones and the step of every chunk; the results are those of
  * shoc_tr_gpu_upload_tracers + shoc_tr_gpu_run(h, 1) +
  * shoc_tr_gpu_download_tracers, bit for bit.  Copies reach the host link's
- * speed only from page-locked memory: see shoc_tr_gpu_host_register. */
+ * speed only from page-locked memory: see shoc_tr_gpu_host_register.  With
+ * SHOC_TR_FP32_MIXED the handle keeps its per-column mass carry (the FP64
+ * mass the FP32-stored values owe each column) from one call to the next:
+ * the values it belongs to come back unchanged through the FP64 host arrays,
+ * so a run of drop-in steps equals the same steps on resident tracers. */
 int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag);
 
 /* Page-locks (cudaHostRegister) / releases a host array the caller passes to
@@ -79,7 +83,8 @@ int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag);
 int shoc_tr_gpu_host_register(void *ptr, size_t bytes);
 int shoc_tr_gpu_host_unregister(void *ptr);
 
-/* Device-resident use. */
+/* Device-resident use.  Uploading tracers starts from new values: the
+ * FP32-mixed path's mass carry is cleared. */
 int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc);
 int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc);
 /* Copies flow fields (u1, u2, w, fluxes, Kz, dzu1/dzu2/u1kh/u2kh when any
