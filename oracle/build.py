@@ -9,6 +9,9 @@
                                     compiled unmodified, single thread
   oracle/_ref/libshoc_ref_omp.so    the same with -fopenmp -DHAVE_OMP (the
                                     reference's OpenMP tracer loop)
+  oracle/_ref/libshoc_shim.so       include/shoc_tr_shim.h (the SHOC-side binding)
+                                    compiled against the reference's headers,
+                                    linked with the product library
 
 The reference libraries are built only where the reference source tree is
 present: the directory named by the REF_ROOT environment variable or the
@@ -96,9 +99,37 @@ def ref_libs(force=False):
     return outs
 
 
+def shim_lib(force=False):
+    """include/shoc_tr_shim.h compiled against the reference's headers and
+    linked with the product library it binds (oracle/_ref/libshoc_shim.so);
+    only where the reference sources exist."""
+    out = os.path.join(REF_OUT, "libshoc_shim.so")
+    if not ref_available():
+        return out if os.path.exists(out) else None
+    R = REF_ROOT
+    gpulib = os.path.join(ROOT, "ems_b200", "_lib")
+    inc = ["-I", os.path.join(HERE, "ref", "stub"), "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(R, "lib", "include"), "-I", os.path.join(R, "model", "hd", "include")]
+    for sub in ("sediments", "tracerstats", "waves", "ecology", "da"):
+        inc += ["-I", os.path.join(R, "model", "lib", sub, "include")]
+    srcs = [os.path.join(R, "model", "hd", "tracers", "tracers.c"),
+            os.path.join(R, "model", "hd", "closure", "MY2-5.c"),
+            os.path.join(HERE, "ref", "ref_harness.c"), os.path.join(HERE, "ref", "shim_check.c")]
+    deps = srcs + [os.path.join(ROOT, "include", n) for n in
+                   ("shoc_tr.h", "shoc_tr_gpu.h", "shoc_tr_shim.h")]
+    if force or _stale(out, deps):
+        os.makedirs(REF_OUT, exist_ok=True)
+        _run(["gcc", "-w"] + CFLAGS + inc + ["-o", out] + srcs +
+             ["-L", gpulib, "-lshoc_tr_gpu", "-Wl,-rpath,$ORIGIN/../../ems_b200/_lib", "-lm"])
+    return out
+
+
 def build_all(force=False):
     out = [oracle_lib(force), grid_lib(force)]
     out += ref_libs(force)
+    shim = shim_lib(force)
+    if shim:
+        out.append(shim)
     return out
 
 

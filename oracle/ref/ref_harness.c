@@ -432,3 +432,12 @@ int ref_vdiff_cols(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts 
   ref_free(r);
   return rc;
 }
+
+/* ---- the window structs for other checkers (the shim check) ---- */
+void *ref_window_new(const shoc_tr_geom *g, shoc_tr_state *st, const shoc_tr_opts *op) {
+  return ref_make(g, st, op, 1);
+}
+geometry_t *ref_window_geom(void *r) { return ((ref_window *)r)->win; }
+window_t *ref_window_data(void *r) { return ((ref_window *)r)->dat; }
+win_priv_t *ref_window_con(void *r) { return ((ref_window *)r)->con; }
+void ref_window_delete(void *r) { ref_free((ref_window *)r); }
