@@ -11,23 +11,27 @@
 //  A  advection, layer chunk by layer chunk from the top down: warp w holds
 //     layer k0 - w of the chunk, so a thread holds one cell and folds its
 //     tracer-independent face coefficients once, then loops over the
-//     advected tracers two at a time.  Of a cell's six face fluxes it
-//     computes the west, south and bottom ones; the east and north fluxes are
-//     the west / south fluxes of the lanes at ix + 1 / iy + 1 (shuffles) and
-//     the top flux is the bottom flux of the warp above (shared memory) --
-//     each computed by the cell itself where that neighbour is not in the
-//     tile.  The flux divergence and the interior update are FP64; the new
-//     value of every cell below the surface goes to the output array (FP32),
-//     while per (column, tracer) the exact FP64 mass of those values (the sum
-//     of a * dz), the FP64 divergence of the surface cell and the cells above
-//     it, and the surface cell's bottom-face flux are accumulated in shared
-//     memory in a fixed order (results do not depend on the schedule).
-//  B  one thread per (column, tracer): tr_bounds, surf_conc's column-mass
-//     balance (FP64), the copy above the surface and, on the last sub-step,
-//     the FP32 Thomas sweep with an FP64 residual and one FP32 correction
-//     solve, as k_vd32 (shoc_tr_tile.cuh) does.  The column's values come back
-//     from the output array, written a few microseconds earlier by phase A of
-//     the same block (an L2 round trip, not an HBM one); the LU factors were
+//     advected tracers two at a time with no block barrier in the loop.  Of
+//     a cell's six face fluxes it computes the west, south, bottom and top
+//     ones; the east and north fluxes are the west / south fluxes of the
+//     lanes at ix + 1 / iy + 1 (shuffles), computed by the cell itself where
+//     that neighbour is not in the tile.  The flux divergence and the
+//     interior update are FP64; the new value of every cell below the
+//     surface goes to the output array (FP32).  Per (column, tracer) the
+//     exact FP64 mass of those values (the sum of a * dz), the FP64
+//     divergence of the surface cell and the cells above it, and the surface
+//     cell's bottom-face flux are accumulated: each cell's contribution goes
+//     to shared memory and one pass per chunk (and group of tracers) adds
+//     them up in layer order, so the sums do not depend on the schedule.
+//  B  one thread per (column, tracer), every warp: tr_bounds, surf_conc's
+//     column-mass balance (FP64), the copy above the surface and, on the
+//     last sub-step, the FP32 Thomas sweep with an FP64 residual and one FP32
+//     correction solve, as k_vd32 (shoc_tr_tile.cuh) does.  The column's
+//     values come back from the output array (written a few microseconds
+//     earlier by phase A of the same block: an L2 round trip, not an HBM one)
+//     in one batch of asynchronous copies, and the forward sweep keeps its
+//     values in the output array's cells of the column until the back
+//     substitution overwrites them with the results; the LU factors were
 //     copied into shared memory while phase A ran.
 //
 // Mass carry.  Storing FP32 values loses mass at every rounding (and the
@@ -57,17 +61,22 @@ struct Fused {
   int ntile;
   double *carry;      // [ntr][ncol] FP64 mass the stored values owe each column
   int nwb;            // warps of phase B (tracers in flight per tile)
+  int ngrp;           // advected tracers per phase-A reduction pass
 };
 
 // shared memory of k_step32 (bytes) for columns of at most nd layers, nwb
-// phase-B warps and ntb advected tracers
-inline size_t fused_smem(int nd, int nwb, int ntb) {
-  return (size_t)nd * 32 * 16                   // LU factors float4 [nd][32]
-         + (size_t)nd * 32 * 4                  // cells int [nd][32]
-         + (size_t)2 * nwb * nd * 32 * 4        // A, S float [nwb][nd][32]
-         + (size_t)kFusedWarps * 32 * 8         // bottom fluxes float2 [8][32]
-         + (size_t)kFusedWarps * 4 * 32 * 8     // reduction double [8][2][2][32]
-         + (size_t)ntb * 32 * (8 + 8 + 4);      // accumulators per (tracer, lane)
+// phase-B warps, ntb advected tracers and reduction groups of ngrp tracers:
+// LU float4 [nd][32], cells int [nd][32], a union of the phase-B column
+// arrays float [nwb][nd][32] and the phase-A contributions double
+// [8][ngrp][32], the accumulators double [ntb][32] x 2 and float [ntb][32],
+// and the surface layer of each lane
+__host__ __device__ inline size_t fused_union(int nd, int nwb, int ngrp) {
+  const size_t a = (size_t)nwb * nd * 32 * 4, r = (size_t)kFusedWarps * ngrp * 32 * 8;
+  return a > r ? a : r;
+}
+inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
+  return (size_t)nd * 32 * 16 + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
+         (size_t)ntb * 32 * (8 + 8 + 4) + 32 * 4;
 }
 
 namespace f32x {
@@ -196,16 +205,16 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   using namespace f32x;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb;
-  float4 *LU = reinterpret_cast<float4 *>(smem);                 // [nd][32]
-  int *colC = reinterpret_cast<int *>(LU + nd * 32);             // [nd][32]
-  float *A = reinterpret_cast<float *>(colC + nd * 32);          // [nwb][nd][32]
-  float *Sv = A + nwb * nd * 32;                                 // [nwb][nd][32]
-  float2 *fzx = reinterpret_cast<float2 *>(Sv + nwb * nd * 32);  // [8][32]
-  double *red = reinterpret_cast<double *>(fzx + kFusedWarps * 32);  // [8][2][2][32]
-  double *accM = red + kFusedWarps * 4 * 32;                     // [ntb][32]
-  double *accD = accM + ntb * 32;                                // [ntb][32]
-  float *accF = reinterpret_cast<float *>(accD + ntb * 32);      // [ntb][32]
+  const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb, ngrp = Fu.ngrp;
+  float4 *LU = reinterpret_cast<float4 *>(smem);                  // [nd][32]
+  int *colC = reinterpret_cast<int *>(LU + nd * 32);              // [nd][32]
+  unsigned char *uni = reinterpret_cast<unsigned char *>(colC + nd * 32);
+  float *A = reinterpret_cast<float *>(uni);                      // [nwb][nd][32]
+  double *red = reinterpret_cast<double *>(uni);                  // [8][ngrp][32]
+  double *accM = reinterpret_cast<double *>(uni + fused_union(nd, nwb, ngrp));  // [ntb][32]
+  double *accD = accM + ntb * 32;                                 // [ntb][32]
+  float *accF = reinterpret_cast<float *>(accD + ntb * 32);       // [ntb][32]
+  int *sks = reinterpret_cast<int *>(accF + ntb * 32);            // [32]
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int tile = blockIdx.x;
@@ -230,6 +239,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     accD[i] = 0.0;
     accF[i] = 0.f;
   }
+  if (w == 0) sks[lane] = tc.act ? ks : -1;
   __syncthreads();
 
   // ---------------- phase A: advection, one layer of the chunk per warp
@@ -258,8 +268,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const bool sxp1 = on && (lane & 7) != 7 && cE != 0 && n1.y == cE;
     const bool syp1 = on && lane < 24 && cN != 0 && n1.w == cN;
     const bool zf = on && k <= ks, zt = on && k < ks;
-    // the top face comes from the warp above, except in the chunk's first warp
-    const bool top_self = zt && w == 0;
     Face fw, fs, fn, fe, fzb, fzt;
     f32::face_zero(fw);
     f32::face_zero(fs);
@@ -296,7 +304,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const bool top = (nzv.z == c);
         const float dzp1 = W.dz32[nzv.z];
         fold_zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
-        if (top_self) {
+        if (zt) {  // the bottom face of the cell above, folded alike
           const bool top1 = (nzv.w == nzv.z);
           const float dzp2 = W.dz32[nzv.w];
           fold_zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1,
@@ -313,88 +321,87 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int vp1 = nzv.z, vp2 = nzv.w;
     const bool needE = on && !sxp1, needN = on && !syp1;
 
-    for (int s0 = 0; s0 < ntb; s0 += 2) {
-      float Fb[2], Fw[2], Fs[2], Fe[2], Fn[2], Ftop[2], t0v[2];
-      int nn[2];
-      bool adv[2];
+    for (int g0 = 0; g0 < ntb; g0 += ngrp) {
+      const int g1 = min(ntb, g0 + ngrp);
+      for (int s0 = g0; s0 < g1; s0 += 2) {
+        float Fb[2], Fw[2], Fs[2], Fe[2], Fn[2], Ft[2], t0v[2];
+        int nn[2];
+        bool adv[2];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int s = s0 + u < ntb ? s0 + u : s0;
-        const int n = T.slot_tr[s];
-        const int tf = T.trf[n];
-        nn[u] = n;
-        adv[u] = (tf & TR_ADV) != 0;
-        const bool hd = (tf & TR_HDIFF) != 0;
-        const float *__restrict__ tr = tri + (size_t)n * G.S;
-        const bool hor = on && (adv[u] || hd);
-        const bool vz = on && adv[u] && zf;
-        const float t0 = on ? tr[c] : 0.f;
-        const float tym1 = hor ? tr[n1.z] : 0.f, tym2 = hor ? tr[n2.z] : 0.f;
-        const float typ1 = hor ? tr[n1.w] : 0.f, typ2 = (hor && needN) ? tr[n2.w] : 0.f;
-        const float txm1 = hor ? tr[n1.x] : 0.f, txm2 = hor ? tr[n2.x] : 0.f;
-        const float txp1 = hor ? tr[n1.y] : 0.f, txp2 = (hor && needE) ? tr[n2.y] : 0.f;
-        const float tm1 = vz ? tr[vm1] : 0.f, tm2 = vz ? tr[vm2] : 0.f;
-        const float tp1 = vz ? tr[vp1] : 0.f, tp2 = (vz && top_self) ? tr[vp2] : 0.f;
-        t0v[u] = t0;
-        Fw[u] = hor ? face_flux<QUICK, ULT>(fw, adv[u], hd, txm2, txm1, t0, txp1) : 0.f;
-        Fs[u] = hor ? face_flux<QUICK, ULT>(fs, adv[u], hd, tym2, tym1, t0, typ1) : 0.f;
-        Fe[u] = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv[u], hd, txm1, t0, txp1, txp2)
-                               : 0.f;
-        Fn[u] = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv[u], hd, tym1, t0, typ1, typ2)
-                               : 0.f;
-        Fb[u] = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
-        Ftop[u] =
-            (vz && top_self) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2) : 0.f;
-      }
+        for (int u = 0; u < 2; ++u) {
+          const int s = s0 + u < g1 ? s0 + u : s0;
+          const int n = T.slot_tr[s];
+          const int tf = T.trf[n];
+          nn[u] = n;
+          adv[u] = (tf & TR_ADV) != 0;
+          const bool hd = (tf & TR_HDIFF) != 0;
+          const float *__restrict__ tr = tri + (size_t)n * G.S;
+          const bool hor = on && (adv[u] || hd);
+          const bool vz = on && adv[u] && zf;
+          const float t0 = on ? tr[c] : 0.f;
+          const float tym1 = hor ? tr[n1.z] : 0.f, tym2 = hor ? tr[n2.z] : 0.f;
+          const float typ1 = hor ? tr[n1.w] : 0.f, typ2 = (hor && needN) ? tr[n2.w] : 0.f;
+          const float txm1 = hor ? tr[n1.x] : 0.f, txm2 = hor ? tr[n2.x] : 0.f;
+          const float txp1 = hor ? tr[n1.y] : 0.f, txp2 = (hor && needE) ? tr[n2.y] : 0.f;
+          const float tm1 = vz ? tr[vm1] : 0.f, tm2 = vz ? tr[vm2] : 0.f;
+          const float tp1 = vz ? tr[vp1] : 0.f, tp2 = (vz && zt) ? tr[vp2] : 0.f;
+          t0v[u] = t0;
+          Fw[u] = hor ? face_flux<QUICK, ULT>(fw, adv[u], hd, txm2, txm1, t0, txp1) : 0.f;
+          Fs[u] = hor ? face_flux<QUICK, ULT>(fs, adv[u], hd, tym2, tym1, t0, typ1) : 0.f;
+          Fe[u] = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv[u], hd, txm1, t0, txp1, txp2)
+                                 : 0.f;
+          Fn[u] = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv[u], hd, tym1, t0, typ1, typ2)
+                                 : 0.f;
+          Fb[u] = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+          Ft[u] = (vz && zt) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2) : 0.f;
+        }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const float e = __shfl_down_sync(FULL, Fw[u], 1), nb = __shfl_down_sync(FULL, Fs[u], 8);
-        if (sxp1) Fe[u] = e;
-        if (syp1) Fn[u] = nb;
-      }
-      fzx[w * 32 + lane] = make_float2(Fb[0], Fb[1]);
-      __syncthreads();
-      if (w > 0) {
-        const float2 up = fzx[(w - 1) * 32 + lane];
-        Ftop[0] = up.x;
-        Ftop[1] = up.y;
-      }
-      double cm[2] = {0.0, 0.0}, cd[2] = {0.0, 0.0};
+        for (int u = 0; u < 2; ++u) {
+          const float e = __shfl_down_sync(FULL, Fw[u], 1);
+          const float nb = __shfl_down_sync(FULL, Fs[u], 8);
+          if (sxp1) Fe[u] = e;
+          if (syp1) Fn[u] = nb;
+        }
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int s = s0 + u;
-        if (s >= ntb || !on || nn[u] >= ntc) continue;
-        // FP64 flux divergence (tracers.c:888-892)
-        const double dtr =
-            (((double)Fe[u] - (double)Fw[u]) + ((double)Fn[u] - (double)Fs[u])) * dtu;
-        if (zt) {
-          const double Fzt = adv[u] ? (double)Ftop[u] : 0.0;
-          const double a = (double)t0v[u] - (dtr * ia + (Fzt - (double)Fb[u])) * idz;
-          const float a32 = (float)a;
-          tro[(size_t)nn[u] * G.S + c] = a32;
-          nstat |= isnan(a32) ? ST_NAN : 0;
-          cm[u] = a * dz0d;
-        } else {
-          cd[u] = dtr;
-          if (k == ks) accF[s * 32 + lane] = Fb[u];
+        for (int u = 0; u < 2; ++u) {
+          const int s = s0 + u;
+          if (s >= g1) break;
+          double contrib = 0.0;
+          if (on && nn[u] < ntc) {
+            // FP64 flux divergence (tracers.c:888-892)
+            const double dtr =
+                (((double)Fe[u] - (double)Fw[u]) + ((double)Fn[u] - (double)Fs[u])) * dtu;
+            if (zt) {
+              const double a =
+                  (double)t0v[u] - (dtr * ia + ((double)Ft[u] - (double)Fb[u])) * idz;
+              const float a32 = (float)a;
+              tro[(size_t)nn[u] * G.S + c] = a32;
+              nstat |= isnan(a32) ? ST_NAN : 0;
+              contrib = a * dz0d;
+            } else {
+              contrib = dtr;
+              if (k == ks) accF[s * 32 + lane] = Fb[u];
+            }
+          }
+          red[(w * ngrp + (s - g0)) * 32 + lane] = contrib;
         }
       }
-      // per (column, tracer) sums over the chunk's layers, in warp order
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        red[((w * 2 + u) * 2 + 0) * 32 + lane] = cm[u];
-        red[((w * 2 + u) * 2 + 1) * 32 + lane] = cd[u];
+      // the group's per (column, tracer) sums over the chunk's layers, in
+      // layer order: a * dz below the surface, the divergence at and above it
+      __syncthreads();
+      for (int i = threadIdx.x; i < (g1 - g0) * 32; i += kFusedThreads) {
+        const int sg = i >> 5, ln = i & 31, ksl = sks[ln];
+        double m = 0.0, dv = 0.0;
+        for (int ww = 0; ww < kFusedWarps; ++ww) {
+          const int kk = k0 - ww;
+          if (kk < kmin || ksl < 0) continue;
+          const double v = red[(ww * ngrp + sg) * 32 + ln];
+          if (kk < ksl) m += v; else dv += v;
+        }
+        accM[(g0 + sg) * 32 + ln] += m;
+        accD[(g0 + sg) * 32 + ln] += dv;
       }
       __syncthreads();
-      if (w < 4) {
-        const int u = w >> 1, q = w & 1, s = s0 + u;
-        if (s < ntb) {
-          double sum = 0.0;
-          for (int ww = 0; ww < kFusedWarps; ++ww) sum += red[((ww * 2 + u) * 2 + q) * 32 + lane];
-          double *acc = q ? accD : accM;
-          acc[s * 32 + lane] += sum;
-        }
-      }
     }
   }
   cp_async_wait<0>();
@@ -402,8 +409,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
 
   // ---------------- phase B: one thread per (column, tracer)
   if (w < nwb && tc.act) {
-    float *Aj = A + w * nd * 32 + lane;
-    float *Sj = Sv + w * nd * 32 + lane;
+    float *const A0 = A + w * nd * 32 + lane + (kb - kbase) * 32;
     const bool steady = F.eta[c2] == F.oldeta[c2];
     const int *const C0 = colC + (kb - kbase) * 32 + lane;
     const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
@@ -426,14 +432,14 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       const bool solve = vdf && !single;
       const float *tr = tri + (size_t)n * G.S;
       float *to = tro + (size_t)n * G.S;
-      float *const A0 = Aj + (kb - kbase) * 32;
-      float *const S0 = Sj + (kb - kbase) * 32;
-      // the column's values: advection results below the surface (advected
-      // tracers) or the old values (the rest, every layer)
-      if (tbdy) {
-        for (int j = 0; j < nk; ++j) A0[j * 32] = to[C0[j * 32]];
-      } else {
-        for (int j = 0; j < nz - kb; ++j) A0[j * 32] = tr[C0[j * 32]];
+      // the column's values, one batch of asynchronous copies: advection
+      // results below the surface (advected tracers) or the old values (the
+      // rest, every layer)
+      {
+        const float *src = tbdy ? to : tr;
+        const int nl = tbdy ? nk : nz - kb;
+        for (int j = 0; j < nl; ++j) cp_async4(&A0[j * 32], src + C0[j * 32]);
+        cp_async_commit();
       }
       const double mn = T.mintr[n], mx = T.maxtr[n];
       {  // sediment ghost (tracers.c:827-830)
@@ -452,9 +458,9 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
       if (H > 0.0) f32::neumaier_add(mxs, mxc, carry_in * ia);
       long long nw = 0;
-      float fwd = 0.f;
       double vs = ts_old;  // the surface value
       bool bad = false;
+      cp_async_wait<0>();
       if (!tbdy) {
         for (int j = 0; j < nk; ++j)
           f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
@@ -522,22 +528,27 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
       } else {
         A0[nk * 32] = (float)vs;
-        // FP32 forward sweep
+        // FP32 forward sweep; its values wait in the output array's cells of
+        // the column (free once read) for the back substitution
+        float fwd = 0.f;
         for (int j = 0; j <= nk; ++j) {
           const float4 lu = L0[j * 32];
           fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
-          S0[j * 32] = fwd;
+          to[C0[j * 32]] = fwd;
         }
         // back substitution (FP32) and, one row behind, the FP64 residual
         //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
-        // (cp1(j) = cm1(j+1)); the surface row's value is the FP64 one
-        float x1 = S0[nk * 32];
+        // (cp1(j) = cm1(j+1)); the results x go back to the output array
+        float x1 = fwd;
         float4 l1 = L0[nk * 32];
         double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
         double dzdt1 = dzs * idt;
+        float sn = nk > 0 ? to[C0[(nk - 1) * 32]] : 0.f;  // the next row's forward value
         for (int j = nk - 1; j >= 0; --j) {
-          const float x = S0[j * 32] - l1.w * x1;
-          S0[j * 32] = x;
+          const float sj = sn;
+          if (j > 0) sn = to[C0[(j - 1) * 32]];
+          const float x = sj - l1.w * x1;
+          to[C0[j * 32]] = x;
           const double xd = (double)x, l1y = (double)l1.y;
           const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * 32]) + dl;
           double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
@@ -565,17 +576,19 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         }
         float d = A0[nk * 32];
         {
-          const float fin = (float)((double)S0[nk * 32] + (double)d);
-          to[C0[nk * 32]] = fin;
+          const int cc = C0[nk * 32];
+          const float fin = (float)((double)to[cc] + (double)d);
+          to[cc] = fin;
           bad |= isnan(fin);
           f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
         }
         for (int j = nk - 1; j >= 0; --j) {
           d = A0[j * 32] - L0[(j + 1) * 32].w * d;
-          const float fin = (float)((double)S0[j * 32] + (double)d);
-          to[C0[j * 32]] = fin;
+          const int cc = C0[j * 32];
+          const float fin = (float)((double)to[cc] + (double)d);
+          to[cc] = fin;
           bad |= isnan(fin);
-          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, W.dz[C0[j * 32]]));
+          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, W.dz[cc]));
         }
       }
       if (Fu.carry && steady)

@@ -1237,16 +1237,25 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     // column arrays of as many phase-B warps as keep two blocks per SM
     const char *env = getenv("SHOC_TR_GPU_KERNELS");
     const bool want = !(env && strcmp(env, "split") == 0);
+    // (phase-B warps, tracers per reduction pass): the most phase-B warps
+    // that keep two blocks per SM, the reduction groups fitting the space
+    // the phase-B arrays leave
     const int ntb = o->ntbdy;
-    int nwb = 0;
-    for (int c = 4; c >= 1 && !nwb; c--)
-      if (fused_smem(g->nz, c, ntb) <= 113 * 1024) nwb = c;
-    if (!nwb && fused_smem(g->nz, 1, ntb) <= 227 * 1024) nwb = 1;
+    int nwb = 0, ngrp = 0;
+    for (int c = kFusedWarps; c >= 1 && !nwb; c--) {
+      const int gmax = (int)((size_t)c * g->nz * 32 * 4 / ((size_t)kFusedWarps * 32 * 8));
+      const int gq = std::max(1, std::min(std::max(ntb, 1), gmax));
+      if (fused_smem(g->nz, c, ntb, gq) <= 113 * 1024) {
+        nwb = c;
+        ngrp = gq;
+      }
+    }
     if (want && nwb && ntb <= kFusedMaxTracers) {
       TRY(build_fused_tiles(h, g, col_kb));
       h->fu.nwb = nwb;
+      h->fu.ngrp = ngrp;
       TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
-      h->fused_bytes = fused_smem(g->nz, nwb, ntb);
+      h->fused_bytes = fused_smem(g->nz, nwb, ntb, ngrp);
       h->fused = true;
       if (fused32_set_smem_attr((int)h->fused_bytes) != cudaSuccess) TRY(SHOC_TR_ECUDA);
     }
