@@ -67,11 +67,17 @@ struct Fused {
 // shared memory of k_step32 (bytes) for columns of at most nd layers, nwb
 // phase-B warps, ntb advected tracers and reduction groups of ngrp tracers:
 // LU float4 [nd][32], cells int [nd][32], a union of the phase-B column
-// arrays float [nwb][nd][32] and the phase-A contributions double
-// [8][ngrp][32], the accumulators double [ntb][32] x 2 and float [ntb][32],
-// and the surface layer of each lane
+// arrays float [nwb][nd][32] with the phase-A contributions double
+// [8][ngrp][32] followed by its stencil double buffer float [2][13][256],
+// the accumulators double [ntb][32] x 2 and float [ntb][32], and the surface
+// layer of each lane
+constexpr int kStencil = 13;  // values of a cell's advection stencil
+__host__ __device__ inline size_t fused_red(int ngrp) {
+  return (size_t)kFusedWarps * ngrp * 32 * 8;
+}
 __host__ __device__ inline size_t fused_union(int nd, int nwb, int ngrp) {
-  const size_t a = (size_t)nwb * nd * 32 * 4, r = (size_t)kFusedWarps * ngrp * 32 * 8;
+  const size_t a = (size_t)nwb * nd * 32 * 4;
+  const size_t r = fused_red(ngrp) + (size_t)2 * kStencil * kFusedThreads * 4;
   return a > r ? a : r;
 }
 inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
@@ -211,6 +217,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   unsigned char *uni = reinterpret_cast<unsigned char *>(colC + nd * 32);
   float *A = reinterpret_cast<float *>(uni);                      // [nwb][nd][32]
   double *red = reinterpret_cast<double *>(uni);                  // [8][ngrp][32]
+  float *pf = reinterpret_cast<float *>(uni + fused_red(ngrp));   // [2][13][256]
   double *accM = reinterpret_cast<double *>(uni + fused_union(nd, nwb, ngrp));  // [ntb][32]
   double *accD = accM + ntb * 32;                                 // [ntb][32]
   float *accF = reinterpret_cast<float *>(accD + ntb * 32);       // [ntb][32]
@@ -321,70 +328,68 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int vp1 = nzv.z, vp2 = nzv.w;
     const bool needE = on && !sxp1, needN = on && !syp1;
 
+    // the stencil of the cell: its own value, y-1, y-2, y+1, y+2, z-1, z-2,
+    // z+1, z+2, x-1, x-2, x+1, x+2 (cells that are not used are valid cells)
+    const int idx[kStencil] = {c,   n1.z, n2.z, n1.w, n2.w, vm1, vm2,
+                               vp1, vp2,  n1.x, n2.x, n1.y, n2.y};
+    // copies the stencil of slot s into this thread's slots of buffer b
+    auto issue = [&](int s, int b) {
+      const float *tr = tri + (size_t)T.slot_tr[s] * G.S;
+      float *d = pf + b * kStencil * kFusedThreads + threadIdx.x;
+#pragma unroll
+      for (int q = 0; q < kStencil; ++q) cp_async4(d + q * kFusedThreads, tr + idx[q]);
+      cp_async_commit();
+    };
     for (int g0 = 0; g0 < ntb; g0 += ngrp) {
       const int g1 = min(ntb, g0 + ngrp);
-      for (int s0 = g0; s0 < g1; s0 += 2) {
-        float Fb[2], Fw[2], Fs[2], Fe[2], Fn[2], Ft[2], t0v[2];
-        int nn[2];
-        bool adv[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int s = s0 + u < g1 ? s0 + u : s0;
-          const int n = T.slot_tr[s];
-          const int tf = T.trf[n];
-          nn[u] = n;
-          adv[u] = (tf & TR_ADV) != 0;
-          const bool hd = (tf & TR_HDIFF) != 0;
-          const float *__restrict__ tr = tri + (size_t)n * G.S;
-          const bool hor = on && (adv[u] || hd);
-          const bool vz = on && adv[u] && zf;
-          const float t0 = on ? tr[c] : 0.f;
-          const float tym1 = hor ? tr[n1.z] : 0.f, tym2 = hor ? tr[n2.z] : 0.f;
-          const float typ1 = hor ? tr[n1.w] : 0.f, typ2 = (hor && needN) ? tr[n2.w] : 0.f;
-          const float txm1 = hor ? tr[n1.x] : 0.f, txm2 = hor ? tr[n2.x] : 0.f;
-          const float txp1 = hor ? tr[n1.y] : 0.f, txp2 = (hor && needE) ? tr[n2.y] : 0.f;
-          const float tm1 = vz ? tr[vm1] : 0.f, tm2 = vz ? tr[vm2] : 0.f;
-          const float tp1 = vz ? tr[vp1] : 0.f, tp2 = (vz && zt) ? tr[vp2] : 0.f;
-          t0v[u] = t0;
-          Fw[u] = hor ? face_flux<QUICK, ULT>(fw, adv[u], hd, txm2, txm1, t0, txp1) : 0.f;
-          Fs[u] = hor ? face_flux<QUICK, ULT>(fs, adv[u], hd, tym2, tym1, t0, typ1) : 0.f;
-          Fe[u] = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv[u], hd, txm1, t0, txp1, txp2)
-                                 : 0.f;
-          Fn[u] = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv[u], hd, tym1, t0, typ1, typ2)
-                                 : 0.f;
-          Fb[u] = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
-          Ft[u] = (vz && zt) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2) : 0.f;
+      issue(g0, 0);
+      for (int s = g0; s < g1; ++s) {
+        const int b = (s - g0) & 1;
+        if (s + 1 < g1) {
+          issue(s + 1, b ^ 1);
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
         }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const float e = __shfl_down_sync(FULL, Fw[u], 1);
-          const float nb = __shfl_down_sync(FULL, Fs[u], 8);
-          if (sxp1) Fe[u] = e;
-          if (syp1) Fn[u] = nb;
-        }
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int s = s0 + u;
-          if (s >= g1) break;
-          double contrib = 0.0;
-          if (on && nn[u] < ntc) {
-            // FP64 flux divergence (tracers.c:888-892)
-            const double dtr =
-                (((double)Fe[u] - (double)Fw[u]) + ((double)Fn[u] - (double)Fs[u])) * dtu;
-            if (zt) {
-              const double a =
-                  (double)t0v[u] - (dtr * ia + ((double)Ft[u] - (double)Fb[u])) * idz;
-              const float a32 = (float)a;
-              tro[(size_t)nn[u] * G.S + c] = a32;
-              nstat |= isnan(a32) ? ST_NAN : 0;
-              contrib = a * dz0d;
-            } else {
-              contrib = dtr;
-              if (k == ks) accF[s * 32 + lane] = Fb[u];
-            }
+        const float *v = pf + b * kStencil * kFusedThreads + threadIdx.x;
+        const int n = T.slot_tr[s];
+        const int tf = T.trf[n];
+        const bool adv = (tf & TR_ADV) != 0, hd = (tf & TR_HDIFF) != 0;
+        const bool hor = on && (adv || hd), vz = on && adv && zf;
+        const float t0 = v[0];
+        const float tym1 = v[1 * kFusedThreads], tym2 = v[2 * kFusedThreads];
+        const float typ1 = v[3 * kFusedThreads], typ2 = v[4 * kFusedThreads];
+        const float tm1 = v[5 * kFusedThreads], tm2 = v[6 * kFusedThreads];
+        const float tp1 = v[7 * kFusedThreads], tp2 = v[8 * kFusedThreads];
+        const float txm1 = v[9 * kFusedThreads], txm2 = v[10 * kFusedThreads];
+        const float txp1 = v[11 * kFusedThreads], txp2 = v[12 * kFusedThreads];
+        const float Fw = hor ? face_flux<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1) : 0.f;
+        const float Fs = hor ? face_flux<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1) : 0.f;
+        float Fe = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2) : 0.f;
+        float Fn = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2) : 0.f;
+        const float Fb = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+        const float Ft = (vz && zt) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
+                                    : 0.f;
+        const float e = __shfl_down_sync(FULL, Fw, 1);
+        const float nb = __shfl_down_sync(FULL, Fs, 8);
+        if (sxp1) Fe = e;
+        if (syp1) Fn = nb;
+        double contrib = 0.0;
+        if (on && n < ntc) {
+          // FP64 flux divergence (tracers.c:888-892)
+          const double dtr = (((double)Fe - (double)Fw) + ((double)Fn - (double)Fs)) * dtu;
+          if (zt) {
+            const double a = (double)t0 - (dtr * ia + ((double)Ft - (double)Fb)) * idz;
+            const float a32 = (float)a;
+            tro[(size_t)n * G.S + c] = a32;
+            nstat |= isnan(a32) ? ST_NAN : 0;
+            contrib = a * dz0d;
+          } else {
+            contrib = dtr;
+            if (k == ks) accF[s * 32 + lane] = Fb;
           }
-          red[(w * ngrp + (s - g0)) * 32 + lane] = contrib;
         }
+        red[(w * ngrp + (s - g0)) * 32 + lane] = contrib;
       }
       // the group's per (column, tracer) sums over the chunk's layers, in
       // layer order: a * dz below the surface, the divergence at and above it
