@@ -23,16 +23,14 @@
 //     cell's bottom-face flux are accumulated: each cell's contribution goes
 //     to shared memory and one pass per chunk (and group of tracers) adds
 //     them up in layer order, so the sums do not depend on the schedule.
-//  B  one thread per (column, tracer), every warp: tr_bounds, surf_conc's
+//  B  one thread per (column, tracer): tr_bounds, surf_conc's
 //     column-mass balance (FP64), the copy above the surface and, on the
 //     last sub-step, the FP32 Thomas sweep with an FP64 residual and one FP32
 //     correction solve, as k_vd32 (shoc_tr_tile.cuh) does.  The column's
 //     values come back from the output array (written a few microseconds
 //     earlier by phase A of the same block: an L2 round trip, not an HBM one)
-//     in one batch of asynchronous copies, and the forward sweep keeps its
-//     values in the output array's cells of the column until the back
-//     substitution overwrites them with the results; the LU factors were
-//     copied into shared memory while phase A ran.
+//     in one batch of asynchronous copies; the LU factors and the layer
+//     thicknesses were copied into shared memory while phase A ran.
 //
 // Mass carry.  Storing FP32 values loses mass at every rounding (and the
 // FP32 solve conserves the column mass only to its residual).  Per (tracer,
@@ -66,8 +64,9 @@ struct Fused {
 
 // shared memory of k_step32 (bytes) for columns of at most nd layers, nwb
 // phase-B warps, ntb advected tracers and reduction groups of ngrp tracers:
-// LU float4 [nd][32], cells int [nd][32], a union of the phase-B column
-// arrays float [nwb][nd][32] with the phase-A contributions double
+// LU float4 [nd][32], thicknesses double [nd][32], cells int [nd][32], a
+// union of the phase-B column arrays float [2][nwb][nd][32] with the phase-A
+// contributions double
 // [8][ngrp][32] followed by its stencil double buffer float [2][13][256],
 // the accumulators double [ntb][32] x 2 and float [ntb][32], and the surface
 // layer of each lane
@@ -76,12 +75,12 @@ __host__ __device__ inline size_t fused_red(int ngrp) {
   return (size_t)kFusedWarps * ngrp * 32 * 8;
 }
 __host__ __device__ inline size_t fused_union(int nd, int nwb, int ngrp) {
-  const size_t a = (size_t)nwb * nd * 32 * 4;
+  const size_t a = (size_t)2 * nwb * nd * 32 * 4;
   const size_t r = fused_red(ngrp) + (size_t)2 * kStencil * kFusedThreads * 4;
   return a > r ? a : r;
 }
 inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
-  return (size_t)nd * 32 * 16 + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
+  return (size_t)nd * 32 * (16 + 8) + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
          (size_t)ntb * 32 * (8 + 8 + 4) + 32 * 4;
 }
 
@@ -213,9 +212,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   extern __shared__ __align__(16) unsigned char smem[];
   const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb, ngrp = Fu.ngrp;
   float4 *LU = reinterpret_cast<float4 *>(smem);                  // [nd][32]
-  int *colC = reinterpret_cast<int *>(LU + nd * 32);              // [nd][32]
+  double *DZ = reinterpret_cast<double *>(LU + nd * 32);          // [nd][32]
+  int *colC = reinterpret_cast<int *>(DZ + nd * 32);              // [nd][32]
   unsigned char *uni = reinterpret_cast<unsigned char *>(colC + nd * 32);
   float *A = reinterpret_cast<float *>(uni);                      // [nwb][nd][32]
+  float *Sv = A + nwb * nd * 32;                                  // [nwb][nd][32]
   double *red = reinterpret_cast<double *>(uni);                  // [8][ngrp][32]
   float *pf = reinterpret_cast<float *>(uni + fused_red(ngrp));   // [2][13][256]
   double *accM = reinterpret_cast<double *>(uni + fused_union(nd, nwb, ngrp));  // [ntb][32]
@@ -239,6 +240,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int r = k - kbase;
     colC[r * 32 + lane] = c;
     if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &W.lu32[c]);
+    if (c && k <= ks) cp_async8(&DZ[r * 32 + lane], &W.dz[c]);
   }
   cp_async_commit();
   for (int i = threadIdx.x; i < ntb * 32; i += kFusedThreads) {
@@ -415,6 +417,8 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   // ---------------- phase B: one thread per (column, tracer)
   if (w < nwb && tc.act) {
     float *const A0 = A + w * nd * 32 + lane + (kb - kbase) * 32;
+    float *const S0 = Sv + w * nd * 32 + lane + (kb - kbase) * 32;
+    const double *const D0 = DZ + (kb - kbase) * 32 + lane;
     const bool steady = F.eta[c2] == F.oldeta[c2];
     const int *const C0 = colC + (kb - kbase) * 32 + lane;
     const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
@@ -423,7 +427,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     // diagonal of the residual (dz / dt exactly, so the refined solve keeps
     // the same column mass as the mass diagnostic measures)
     double H = 0.0;
-    for (int j = 0; j <= nk; ++j) H += W.dz[C0[j * 32]];
+    for (int j = 0; j <= nk; ++j) H += D0[j * 32];
     const double idt = 1.0 / F.dt;
     long long nwarn = 0;
     for (int slot = w; slot < T.nslot; slot += nwb) {
@@ -453,7 +457,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       }
       const double dzs_old = (double)W.dz32[ci.s];
       const double ts_old = (double)tr[ci.s];
-      const double dzs = W.dz[ci.s];
+      const double dzs = D0[nk * 32];
       double carry_in = 0.0;
       if (Fu.carry && steady) carry_in = Fu.carry[(size_t)n * G.ncol + col];
       // the carry goes back as a uniform shift of the column's values
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       cp_async_wait<0>();
       if (!tbdy) {
         for (int j = 0; j < nk; ++j)
-          f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], W.dz[C0[j * 32]]));
+          f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], D0[j * 32]));
         vs = (double)A0[nk * 32];
         f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
         for (int j = nk + 1; j < nz - kb; ++j) {
@@ -484,7 +488,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         for (int j = 0; j < nk; ++j) {
           float a = A0[j * 32];
           if (clip && a < mn_up) {
-            f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, W.dz[C0[j * 32]]));
+            f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, D0[j * 32]));
             a = mnf;
           }
           nw += (a < mn_up || a > mx_dn);
@@ -519,7 +523,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       if (!solve) {
         // the values as they are, plus the carry's shift (tr_bounds has run)
         for (int j = 0; j < nk; ++j) {
-          const double dz = W.dz[C0[j * 32]];
+          const double dz = D0[j * 32];
           const float fin = (float)((double)A0[j * 32] + dl);
           to[C0[j * 32]] = fin;
           bad |= isnan(fin);
@@ -533,27 +537,23 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
       } else {
         A0[nk * 32] = (float)vs;
-        // FP32 forward sweep; its values wait in the output array's cells of
-        // the column (free once read) for the back substitution
+        // FP32 forward sweep
         float fwd = 0.f;
         for (int j = 0; j <= nk; ++j) {
           const float4 lu = L0[j * 32];
           fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
-          to[C0[j * 32]] = fwd;
+          S0[j * 32] = fwd;
         }
         // back substitution (FP32) and, one row behind, the FP64 residual
         //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
-        // (cp1(j) = cm1(j+1)); the results x go back to the output array
+        // (cp1(j) = cm1(j+1))
         float x1 = fwd;
         float4 l1 = L0[nk * 32];
         double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
         double dzdt1 = dzs * idt;
-        float sn = nk > 0 ? to[C0[(nk - 1) * 32]] : 0.f;  // the next row's forward value
         for (int j = nk - 1; j >= 0; --j) {
-          const float sj = sn;
-          if (j > 0) sn = to[C0[(j - 1) * 32]];
-          const float x = sj - l1.w * x1;
-          to[C0[j * 32]] = x;
+          const float x = S0[j * 32] - l1.w * x1;
+          S0[j * 32] = x;
           const double xd = (double)x, l1y = (double)l1.y;
           const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * 32]) + dl;
           double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
           xd1 = xd;
           l2y = l1y;
           l1 = L0[j * 32];
-          dzdt1 = W.dz[C0[j * 32]] * idt;
+          dzdt1 = D0[j * 32] * idt;
         }
         {
           const double a0 = ((nk == 0) ? vs : (double)A0[0]) + dl;
@@ -581,19 +581,17 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         }
         float d = A0[nk * 32];
         {
-          const int cc = C0[nk * 32];
-          const float fin = (float)((double)to[cc] + (double)d);
-          to[cc] = fin;
+          const float fin = (float)((double)S0[nk * 32] + (double)d);
+          to[C0[nk * 32]] = fin;
           bad |= isnan(fin);
           f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
         }
         for (int j = nk - 1; j >= 0; --j) {
           d = A0[j * 32] - L0[(j + 1) * 32].w * d;
-          const int cc = C0[j * 32];
-          const float fin = (float)((double)to[cc] + (double)d);
-          to[cc] = fin;
+          const float fin = (float)((double)S0[j * 32] + (double)d);
+          to[C0[j * 32]] = fin;
           bad |= isnan(fin);
-          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, W.dz[cc]));
+          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
         }
       }
       if (Fu.carry && steady)

@@ -1243,7 +1243,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     const int ntb = o->ntbdy;
     int nwb = 0, ngrp = 0;
     for (int c = kFusedWarps; c >= 1 && !nwb; c--) {
-      const size_t room = (size_t)c * g->nz * 32 * 4, buf = (size_t)2 * kStencil * kFusedThreads * 4;
+      const size_t room = (size_t)2 * c * g->nz * 32 * 4;
+      const size_t buf = (size_t)2 * kStencil * kFusedThreads * 4;
       const int gmax = room > buf ? (int)((room - buf) / fused_red(1)) : 1;
       const int gq = std::max(1, std::min(std::max(ntb, 1), gmax));
       if (fused_smem(g->nz, c, ntb, gq) <= 113 * 1024) {

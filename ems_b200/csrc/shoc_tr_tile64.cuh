@@ -30,11 +30,6 @@ inline size_t vd64_smem(int nd, int nw) {
   return (size_t)nd * 32 * 4 + (size_t)2 * nd * nw * 32 * 8;
 }
 
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
-}
-
 // One horizontal face (advect + hor_diffuse) at a cell with Courant number cr,
 // velocity vel (Van Leer's sign), metric factors m, volume flux U; the
 // diffusion term is (P (t0 - tm1)) / H with P = dzu h2au1 1.0 u1kh and
