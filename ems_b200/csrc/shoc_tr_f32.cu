@@ -15,21 +15,21 @@ cudaError_t attr(K k, int bytes = 227 * 1024) {
 template <bool Q, bool U, int M>
 void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
-         const float *tin, float *tout, float *fzs, int hd) {
+         const float *tin, float *tout, float *rnd, float *fzs, int hd) {
   k_adv32<Q, U, M><<<grid, kAdv32Block, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
-                                                                  tin, tout, fzs, hd);
+                                                                  tin, tout, rnd, fzs, hd);
 }
 template <bool Q, bool U>
 void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F3,
               const Work &W, const TrSet &T, const SubStep &ss, const Tile &Tl,
               const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin, float *tout,
-              float *fzs, int hd) {
+              float *rnd, float *fzs, int hd) {
   if (mode == 1)
-    adv<Q, U, 1>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+    adv<Q, U, 1>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd, fzs, hd);
   else if (mode == 2)
-    adv<Q, U, 2>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+    adv<Q, U, 2>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd, fzs, hd);
   else
-    adv<Q, U, 0>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs, hd);
+    adv<Q, U, 0>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd, fzs, hd);
 }
 }  // namespace
 
@@ -50,23 +50,24 @@ cudaError_t tile32_set_smem_attr() {
 void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo &G,
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
-                    const f32::Face2 *fy2, const float *tin, float *tout, float *fzs, int vd_nw,
-                    int any_hd, int adv_flags, cudaEvent_t *ev) {
+                    const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
+                    double *carry, float *fzs, int vd_nw, int any_hd, int adv_flags,
+                    cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {
     const int grid = (Tl.nwet + kAdv32Block - 1) / kAdv32Block;
     if (quick && ult)
-      adv_mode<true, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
-                           any_hd);
+      adv_mode<true, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd,
+                           fzs, any_hd);
     else if (quick)
-      adv_mode<true, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
-                            any_hd);
+      adv_mode<true, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd,
+                            fzs, any_hd);
     else if (ult)
-      adv_mode<false, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
-                            any_hd);
+      adv_mode<false, true>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd,
+                            fzs, any_hd);
     else
-      adv_mode<false, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, fzs,
-                             any_hd);
+      adv_mode<false, false>(adv_flags, grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd,
+                             fzs, any_hd);
   }
   if (ev) cudaEventRecord(ev[1], st);
   const int nchunk = (T.nslot + vd_nw - 1) / vd_nw;
@@ -76,11 +77,11 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
     if (nt <= 0) continue;
     const size_t smem = vd32_smem(G.nz - kbase, vd_nw);
     if (last)
-      k_vd32<true><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
-                                                   tout, fzs, vd_nw, nchunk, t0, kbase);
+      k_vd32<true><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd,
+                                                   carry, fzs, vd_nw, nchunk, t0, kbase);
     else
-      k_vd32<false><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, W.dz32, tin,
-                                                    tout, fzs, vd_nw, nchunk, t0, kbase);
+      k_vd32<false><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout,
+                                                    rnd, carry, fzs, vd_nw, nchunk, t0, kbase);
   }
   if (ev) cudaEventRecord(ev[2], st);
 }

@@ -32,18 +32,11 @@
 //     in one batch of asynchronous copies; the LU factors and the layer
 //     thicknesses were copied into shared memory while phase A ran.
 //
-// Mass carry.  Storing FP32 values loses mass at every rounding (and the
-// FP32 solve conserves the column mass only to its residual).  Per (tracer,
-// column) the kernel keeps, in FP64, the mass the stored values owe the
-// column: carry' = carry + M_exact - M_stored, where M_exact is the FP64 mass
-// the step computed (the exact advected values, the surf_conc surface value,
-// tr_bounds' clipping) and M_stored the mass of what was stored.  The carry
-// goes back into the column at the next sub-step (into the surface row of
-// the solve's FP64 residual, or into the surface value when nothing is
-// solved), so the stored values plus the carry conserve mass to FP64
-// round-off and the carry stays within a few FP32 ulps of the column mass.
-// The mass diagnostic adds it.  Columns whose surface moves during the step
-// (eta != oldeta) keep their carry as it is.
+// The column's end of the sub-step (tr_bounds, surf_conc, the solve and the
+// FP64 mass carry) is column_finish, as in k_vd32 (shoc_tr_tile.cuh): the
+// fused and the two-kernel sub-steps differ only in where the advected
+// values' FP64 column sums come from (phase A's accumulators here, the
+// advection kernel's rounding residuals there).
 #pragma once
 #include "shoc_tr_tile.cuh"
 
@@ -84,121 +77,6 @@ inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
          (size_t)ntb * 32 * (8 + 8 + 4) + 32 * 4;
 }
 
-namespace f32x {
-
-using f32::Face;
-using f32::Face2;
-using f32::FB_NEG;
-using f32::FB_POS;
-using f32::FB_ULT;
-
-// Face weights (as f32::set_face) with every rounding explicit, so two
-// threads folding the same face from the same inputs get the same bits: a
-// cell's east (north) face, computed where the neighbour is not in the tile,
-// equals the neighbour's own west (south) face, and no mass is created
-// between them.
-__device__ __forceinline__ void fold_face(Face &f, bool quick, float cr, float d, float Ap,
-                                          float Bp, float Am, float Bm, float U, bool ult,
-                                          float K) {
-  f.bits = (cr > 0.f ? FB_POS : 0) | (cr < 0.f ? FB_NEG : 0) | ((ult && cr != 0.f) ? FB_ULT : 0);
-  if (quick) {
-    const float a = __fmaf_rn(-0.5f, cr, d);
-    const float b = __fmul_rn(__fmaf_rn(-cr, cr, 1.f), 1.f / 6.f);
-    if (cr > 0.f) {
-      f.wa = __fmul_rn(-b, Bp);
-      f.w1 = __fmaf_rn(2.f, b, __fsub_rn(1.f, a));
-      f.w2 = __fmaf_rn(-b, Ap, a);
-    } else if (cr < 0.f) {
-      f.wa = __fmul_rn(-b, Am);
-      f.w1 = __fmaf_rn(-b, Bm, __fsub_rn(1.f, a));
-      f.w2 = __fmaf_rn(2.f, b, a);
-    } else {
-      f.wa = 0.f;
-      f.w1 = __fsub_rn(1.f, d);
-      f.w2 = d;
-    }
-  } else {
-    f.wa = cr > 0.f ? __fmul_rn(0.5f, __fsub_rn(1.f, cr)) : __fmul_rn(0.5f, __fadd_rn(1.f, cr));
-    f.w1 = f.w2 = 0.f;
-  }
-  f.ircr = cr != 0.f ? __frcp_rn(fabsf(cr)) : 0.f;
-  f.U = U;
-  f.K = K;
-}
-
-__device__ __forceinline__ void fold_hface(Face &f, bool wet, bool eb, bool quick, bool ult,
-                                           float cr, float U, float K, const Face2 &m) {
-  if (!wet) {
-    f32::face_zero(f);
-    return;
-  }
-  if (!quick && !eb) {  // Van Leer advects interior faces only
-    f32::face_zero(f);
-    f.K = K;
-    return;
-  }
-  fold_face(f, quick, cr, m.d, m.Ap, m.Bp, m.Am, m.Bm, U, ult && eb, K);
-}
-
-__device__ __forceinline__ void fold_zface(Face &f, bool quick, bool ult, float dzm2, float dzm1,
-                                           float dz0, float dzp1, bool top, float wv) {
-  const float w9m = __fmul_rn(0.5f, __fadd_rn(dzm1, dzm2));
-  const float w90 = __fmul_rn(0.5f, __fadd_rn(dz0, dzm1));
-  const float w9p = top ? w90 : __fmul_rn(0.5f, __fadd_rn(dzp1, dz0));
-  const float cz = __fdiv_rn(wv, w90);
-  const float db = __fdiv_rn(2.f, __fadd_rn(w9m, w90)), df = __fdiv_rn(2.f, __fadd_rn(w90, w9p));
-  fold_face(f, quick, cz, __fdiv_rn(dzm1, __fadd_rn(dzm1, dz0)), __fmul_rn(db, w9m),
-            __fmul_rn(db, w90), __fmul_rn(df, w90), __fmul_rn(df, w9p), wv, ult, 0.f);
-}
-
-// One face flux (f32::face with every rounding explicit): QUICKEST or Van
-// Leer, then ULTIMATE (tracers.c:3526-3554 without its divisions), times the
-// volume flux, minus the horizontal-diffusion term.
-template <bool QUICK, bool ULT>
-__device__ __forceinline__ float face_flux(const Face &f, bool adv, bool hd, float tm2, float tm1,
-                                          float t0, float tp1) {
-  float F = 0.f;
-  if (adv) {
-    const bool pos = (f.bits & FB_POS) != 0;
-    const float tu = pos ? tm2 : tp1;
-    if (QUICK) {
-      F = __fmaf_rn(f.wa, tu, __fmaf_rn(f.w1, tm1, __fmul_rn(f.w2, t0)));
-    } else {
-      const bool neg = (f.bits & FB_NEG) != 0;
-      const float p = pos ? __fsub_rn(tm1, tm2) : __fsub_rn(t0, tm1);
-      const float q = pos ? __fsub_rn(t0, tm1) : __fsub_rn(tp1, t0);
-      const float den = pos ? __fsub_rn(t0, tm2) : __fsub_rn(tp1, tm1);
-      const float pq = __fmul_rn(p, q);
-      const float df = pq > 0.f ? __fmul_rn(2.f, __fdiv_rn(pq, den)) : 0.f;
-      F = pos ? __fmaf_rn(f.wa, df, tm1) : (neg ? __fmaf_rn(-f.wa, df, t0) : 0.f);
-    }
-    if (ULT) {
-      // with s = sign(td - tu) and the normalised variables scaled back by
-      // |td - tu|: nc in [0, 1] is 0 <= c <= d, nu > 1 is a > d, nu < nc is
-      // a < c and nu > nc / |cr| is a > c / |cr|; tu + nc (td - tu) is tc.
-      // Upwind and downwind equal in FP32 (d = 0) limit to tc (in FP64 they
-      // almost always differ by a few ulps and the limiter falls back to
-      // upwind).
-      const float tc = pos ? tm1 : t0, td = pos ? t0 : tm1;
-      const float diff = __fsub_rn(td, tu);
-      const float sg = diff < 0.f ? -1.f : 1.f;
-      const float d = fabsf(diff);
-      const float c = __fmul_rn(__fsub_rn(tc, tu), sg), a = __fmul_rn(__fsub_rn(F, tu), sg);
-      const float q = __fmul_rn(c, f.ircr);
-      float G = F;
-      if (a > q) G = __fmaf_rn(sg, q, tu);
-      if (a < c) G = tc;
-      if (a > d) G = td;
-      if (!(c >= 0.f && c <= d)) G = tc;
-      F = (f.bits & FB_ULT) ? G : F;
-    }
-    F = __fmul_rn(F, f.U);
-  }
-  if (hd) F = __fmaf_rn(-f.K, __fsub_rn(t0, tm1), F);
-  return F;
-}
-
-}  // namespace f32x
 
 // ---------------------------------------------------------------------------
 
@@ -207,7 +85,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     k_step32(Geo G, Flow F, Flow32 F3, Work W, Opt O, TrSet T, SubStep ss, Tile Tl, Fused Fu,
              const f32::Face2 *__restrict__ fx2, const f32::Face2 *__restrict__ fy2,
              const float *__restrict__ tri, float *__restrict__ tro, int any_hd, int kbase) {
-  using namespace f32x;
+  using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb, ngrp = Fu.ngrp;
@@ -229,7 +107,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   const int col = Fu.tcol[tile * 32 + lane];
   const TileCol tc = tile_column(G, W, Tl, col);
   const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
-  const ColInfo ci = tc.ci;
   const int ntc = tc.act ? G.colntr[col] : 0;
   const int kmin = Fu.tkmin[tile];
 
@@ -287,23 +164,23 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     double dz0d = 1.0, idz = 0.0;
     if (on) {
       const Face2 mx = fx2[c2], my = fy2[c2];
-      fold_hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT,
+      hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT,
                  __fmul_rn(__fmul_rn(F3.u1[c], fdtu), mx.ih), F3.u1flux3d[c],
                  hdf ? F3.khx[c] : 0.f, mx);
-      fold_hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT,
+      hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT,
                  __fmul_rn(__fmul_rn(F3.u2[c], fdtu), my.ih), F3.u2flux3d[c],
                  hdf ? F3.khy[c] : 0.f, my);
       if (!syp1 && (fl & FL_YP_WET)) {
         const int yp = n1.w;
         const Face2 mn = fy2[me.y];
-        fold_hface(fn, true, fl & FL_YP_E2, QUICK, ULT,
+        hface(fn, true, fl & FL_YP_E2, QUICK, ULT,
                    __fmul_rn(__fmul_rn(F3.u2[yp], fdtu), mn.ih), F3.u2flux3d[yp],
                    hdf ? F3.khy[yp] : 0.f, mn);
       }
       if (!sxp1 && (fl & FL_XP_WET)) {
         const int xp = n1.y;
         const Face2 mxe = fx2[me.x];
-        fold_hface(fe, true, fl & FL_XP_E1, QUICK, ULT,
+        hface(fe, true, fl & FL_XP_E1, QUICK, ULT,
                    __fmul_rn(__fmul_rn(F3.u1[xp], fdtu), mxe.ih), F3.u1flux3d[xp],
                    hdf ? F3.khx[xp] : 0.f, mxe);
       }
@@ -312,11 +189,11 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
         const bool top = (nzv.z == c);
         const float dzp1 = W.dz32[nzv.z];
-        fold_zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
+        zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
         if (zt) {  // the bottom face of the cell above, folded alike
           const bool top1 = (nzv.w == nzv.z);
           const float dzp2 = W.dz32[nzv.w];
-          fold_zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1,
+          zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1,
                      __fmul_rn(F3.w[nzv.z], fdtu));
         }
       }
@@ -365,12 +242,12 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const float tp1 = v[7 * kFusedThreads], tp2 = v[8 * kFusedThreads];
         const float txm1 = v[9 * kFusedThreads], txm2 = v[10 * kFusedThreads];
         const float txp1 = v[11 * kFusedThreads], txp2 = v[12 * kFusedThreads];
-        const float Fw = hor ? face_flux<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1) : 0.f;
-        const float Fs = hor ? face_flux<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1) : 0.f;
-        float Fe = (hor && needE) ? face_flux<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2) : 0.f;
-        float Fn = (hor && needN) ? face_flux<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2) : 0.f;
-        const float Fb = vz ? face_flux<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
-        const float Ft = (vz && zt) ? face_flux<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
+        const float Fw = hor ? face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1) : 0.f;
+        const float Fs = hor ? face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1) : 0.f;
+        float Fe = (hor && needE) ? face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2) : 0.f;
+        float Fn = (hor && needN) ? face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2) : 0.f;
+        const float Fb = vz ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+        const float Ft = (vz && zt) ? face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
                                     : 0.f;
         const float e = __shfl_down_sync(FULL, Fw, 1);
         const float nb = __shfl_down_sync(FULL, Fs, 8);
@@ -437,8 +314,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       const bool tbdy = slot < ntb;
       const bool adv = tbdy && (tf & TR_ADV);
       const bool vdf = LAST && (tf & TR_VDIFF);
-      const bool single = (ci.flags & COL_SINGLE) != 0;
-      const bool solve = vdf && !single;
       const float *tr = tri + (size_t)n * G.S;
       float *to = tro + (size_t)n * G.S;
       // the column's values, one batch of asynchronous copies: advection
@@ -450,154 +325,17 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         for (int j = 0; j < nl; ++j) cp_async4(&A0[j * 32], src + C0[j * 32]);
         cp_async_commit();
       }
-      const double mn = T.mintr[n], mx = T.maxtr[n];
       {  // sediment ghost (tracers.c:827-830)
         const int sed = G.zm1[cbot];
         to[sed] = tbdy ? tr[cbot] : tr[sed];
       }
-      const double dzs_old = (double)W.dz32[ci.s];
-      const double ts_old = (double)tr[ci.s];
-      const double dzs = D0[nk * 32];
-      double carry_in = 0.0;
-      if (Fu.carry && steady) carry_in = Fu.carry[(size_t)n * G.ncol + col];
-      // the carry goes back as a uniform shift of the column's values
-      const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
-      // FP64 mass bookkeeping per unit area: what the step computed (mx*) and
-      // what is stored (ms*), compensated sums
-      double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
-      if (H > 0.0) f32::neumaier_add(mxs, mxc, carry_in * ia);
-      long long nw = 0;
-      double vs = ts_old;  // the surface value
+      const ColSums cs{accM[slot * 32 + lane], accD[slot * 32 + lane],
+                       adv ? accF[slot * 32 + lane] : 0.f};
       bool bad = false;
       cp_async_wait<0>();
-      if (!tbdy) {
-        for (int j = 0; j < nk; ++j)
-          f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * 32], D0[j * 32]));
-        vs = (double)A0[nk * 32];
-        f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
-        for (int j = nk + 1; j < nz - kb; ++j) {
-          to[C0[j * 32]] = A0[j * 32];
-          bad |= isnan(A0[j * 32]);
-        }
-      } else {
-        // tr_bounds clip and range check (:3278-3293) of the cells below the
-        // surface; a < mn and a > mx of a float a, exactly, as float compares
-        const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
-        const bool clip = mn <= kClipEps;
-        f32::neumaier_add(mxs, mxc, accM[slot * 32 + lane]);
-        for (int j = 0; j < nk; ++j) {
-          float a = A0[j * 32];
-          if (clip && a < mn_up) {
-            f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, D0[j * 32]));
-            a = mnf;
-          }
-          nw += (a < mn_up || a > mx_dn);
-          A0[j * 32] = a;
-        }
-        const double a_below = nk > 0 ? (double)A0[(nk - 1) * 32] : 0.0;
-        // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
-        if (adv) {
-          const double Fzb_s = (double)accF[slot * 32 + lane];
-          const double wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
-          const double eta = F.eta[c2], oe = F.oldeta[c2];
-          const double osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
-          const double sub = oe + ss.subeta_f * (eta - oe);
-          double ssum = 0.0, scomp = 0.0;
-          f32::neumaier_add(ssum, scomp, __dmul_rn(Fzb_s, area));
-          f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
-          f32::neumaier_add(ssum, scomp, -accD[slot * 32 + lane]);
-          const double dzn = sub - wb;
-          const double svol = dzn * area;
-          const double st = ssum + scomp;
-          const double sv = (svol == 0.0 || (st < 0.0 && dzn <= O.hmin)) ? 0.0 : st / svol;
-          vs = (G.botz[c2] > 0.0 && dzs_old < O.hmin) ? ts_old : sv;
-        }
-        if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
-        if (mn <= kClipEps && vs < mn) vs = mn;
-        if (vs < mn || vs > mx) ++nw;
-        bad |= isnan(vs);
-        f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
-        const float vs32 = (float)vs;
-        for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
-      }
-      if (!solve) {
-        // the values as they are, plus the carry's shift (tr_bounds has run)
-        for (int j = 0; j < nk; ++j) {
-          const double dz = D0[j * 32];
-          const float fin = (float)((double)A0[j * 32] + dl);
-          to[C0[j * 32]] = fin;
-          bad |= isnan(fin);
-          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dz));
-        }
-        const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-        const float fin = (vdf && single) ? (float)(vs + dl + F.dt * (0.0 - 0.0) / h)
-                                          : (float)(vs + dl);
-        to[ci.s] = fin;
-        bad |= isnan(fin);
-        f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
-      } else {
-        A0[nk * 32] = (float)vs;
-        // FP32 forward sweep
-        float fwd = 0.f;
-        for (int j = 0; j <= nk; ++j) {
-          const float4 lu = L0[j * 32];
-          fwd = (lu.x * A0[j * 32] - lu.y * fwd) * lu.z;
-          S0[j * 32] = fwd;
-        }
-        // back substitution (FP32) and, one row behind, the FP64 residual
-        //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
-        // (cp1(j) = cm1(j+1))
-        float x1 = fwd;
-        float4 l1 = L0[nk * 32];
-        double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
-        double dzdt1 = dzs * idt;
-        for (int j = nk - 1; j >= 0; --j) {
-          const float x = S0[j * 32] - l1.w * x1;
-          S0[j * 32] = x;
-          const double xd = (double)x, l1y = (double)l1.y;
-          const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * 32]) + dl;
-          double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
-          if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
-          A0[(j + 1) * 32] = (float)r;
-          x1 = x;
-          xd2 = xd1;
-          xd1 = xd;
-          l2y = l1y;
-          l1 = L0[j * 32];
-          dzdt1 = D0[j * 32] * idt;
-        }
-        {
-          const double a0 = ((nk == 0) ? vs : (double)A0[0]) + dl;
-          double r = dzdt1 * (a0 - xd1) - (double)l1.y * (xd1 - xd1);
-          if (nk > 0) r = r - l2y * (xd2 - xd1);
-          A0[0] = (float)r;
-        }
-        // correction solve (FP32 forward and back) and the update in FP64
-        float u = 0.f;
-        for (int j = 0; j <= nk; ++j) {
-          const float4 lu = L0[j * 32];
-          u = (A0[j * 32] - lu.y * u) * lu.z;
-          A0[j * 32] = u;
-        }
-        float d = A0[nk * 32];
-        {
-          const float fin = (float)((double)S0[nk * 32] + (double)d);
-          to[C0[nk * 32]] = fin;
-          bad |= isnan(fin);
-          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
-        }
-        for (int j = nk - 1; j >= 0; --j) {
-          d = A0[j * 32] - L0[(j + 1) * 32].w * d;
-          const float fin = (float)((double)S0[j * 32] + (double)d);
-          to[C0[j * 32]] = fin;
-          bad |= isnan(fin);
-          f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
-        }
-      }
-      if (Fu.carry && steady)
-        Fu.carry[(size_t)n * G.ncol + col] = ((mxs + mxc) - (mss + msc)) * area;
+      column_finish<LAST>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, 32, L0, C0, D0,
+                          tr, to, area, ia, H, idt, cs, Fu.carry, steady, nwarn, bad);
       if (bad) nstat |= ST_NAN;
-      nwarn += nw;
     }
     if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
   }

@@ -11,10 +11,11 @@
 //               vert_diffuse_3d / implicit_vdiff_tr (:3841-3889, :4185-4195)
 //   per sub-step:
 //     k_courant   w6/w7/w8 (:726-737) of the general-path columns
-//     k_adv32 + k_vd32 (FP32-mixed, shoc_tr_tile.cuh) or k_adv64 + k_vd64
-//                 (FP64, shoc_tr_tile64.cuh): the columns whose surface cell
-//                 stays in its layer, one thread per cell, then one per
-//                 (column, tracer)
+//     k_adv32 + k_vd32 (FP32-mixed, shoc_tr_tile.cuh; or the one fused
+//                 k_step32 of shoc_tr_fused.cuh, SHOC_TR_GPU_KERNELS=fused)
+//                 or k_adv64 + k_vd64 (FP64, shoc_tr_tile64.cuh): the
+//                 columns whose surface cell stays in its layer, one thread
+//                 per cell, then one per (column, tracer)
 //     k_serial    the other columns (surface crossing a layer face, thin-
 //                 surface fix coupling tracers, degenerate solve range), one
 //                 thread per column looping over tracers: column_pass
@@ -72,6 +73,7 @@ struct shoc_tr_gpu {
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
   Tile tl{};                          // static tables of the column-tile kernels
   float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
+  float *rnd = nullptr;               // [ntr][S] FP32 rounding residual of k_adv32's values
   double *fzs64 = nullptr;            // the same, FP64 path
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
   double *cols = nullptr;             // column-solve entry points: their device arrays
@@ -79,7 +81,7 @@ struct shoc_tr_gpu {
   int *colown = nullptr;              // columns counted in the sub-step minimum (null: all)
   double dmin_set = 0.0;              // sub-step minimum imposed by the caller (0: own)
   int nhalo_send = 0, nhalo_recv = 0;
-  Fused fu{};                         // fused FP32-mixed sub-step (k_step32): tiles, carry
+  Fused fu{};                         // FP32-mixed: the columns' mass carry; k_step32's tiles
   bool fused = false;                 // FP32-mixed sub-steps run k_step32
   size_t fused_bytes = 0;             // its dynamic shared memory
   std::vector<int> vd_depth;          // layers of the k_vd32 tiles, in their (sorted) order
@@ -501,7 +503,7 @@ __global__ void k_khfac(Geo G, Flow F, float *khx, float *khy) {
   }
 }
 
-// carry (FP32-mixed fused path, else null): [ntr][ncol] mass the stored
+// carry (FP32-mixed path, else null): [ntr][ncol] mass the stored
 // values owe each column, part of the state's mass.
 // colreg (or null): the region of each column; only region `reg` is summed.
 template <class TR>
@@ -1228,15 +1230,19 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     TRY(dupload(h, &h->fx2, ax.data(), S2));
     TRY(dupload(h, &h->fy2, ay.data(), S2));
     TRY(dupload<float>(h, &h->fzs, nullptr, (size_t)ntr * ncol));
+    // the FP64 mass each column's stored values owe it
+    TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
   } else {
     TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   }
   TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
   if (f32p) {
-    // the fused sub-step kernel: every advected tracer's accumulators and the
-    // column arrays of as many phase-B warps as keep two blocks per SM
+    // the fused sub-step kernel (SHOC_TR_GPU_KERNELS=fused; the two-kernel
+    // sub-step is the default, measured faster): every advected tracer's
+    // accumulators and the column arrays of as many phase-B warps as keep
+    // two blocks per SM
     const char *env = getenv("SHOC_TR_GPU_KERNELS");
-    const bool want = !(env && strcmp(env, "split") == 0);
+    const bool want = env && strcmp(env, "fused") == 0;
     // (phase-B warps, tracers per reduction pass): the most phase-B warps
     // that keep two blocks per SM, the reduction groups fitting the space
     // the phase-B arrays leave
@@ -1256,11 +1262,11 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
       TRY(build_fused_tiles(h, g, col_kb));
       h->fu.nwb = nwb;
       h->fu.ngrp = ngrp;
-      TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
       h->fused_bytes = fused_smem(g->nz, nwb, ntb, ngrp);
       h->fused = true;
       if (fused32_set_smem_attr((int)h->fused_bytes) != cudaSuccess) TRY(SHOC_TR_ECUDA);
     }
+    if (!h->fused) TRY(dupload<float>(h, &h->rnd, nullptr, (size_t)ntr * S));
   }
   // flow fields
   Flow &F = h->F;
@@ -1495,7 +1501,8 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
       } else {
         const Tile tl = vd_classes(h, tw);
         tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
-                       h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->fzs, tw,
+                       h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->rnd,
+                       h->fu.carry, h->fzs, tw,
                        h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
         if (prof) {  // pairs share events; sync destroys each event once
           h->ev.push_back({0, ev[0], ev[2]});
@@ -1895,7 +1902,7 @@ int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
 
 // ---- checkpoint / resume: a versioned raw image of the resident state ----
 // [header 8 x int64][tracers: ntr x S values of the handle's precision]
-// [carry: ntr x ncol doubles, FP32-mixed fused path only][sur_t, nsur_t: ncol ints each]
+// [carry: ntr x ncol doubles, FP32-mixed path only][sur_t, nsur_t: ncol ints each]
 namespace {
 constexpr long long kStateMagic = 0x53484f4354524731ll;  // "SHOCTRG1"
 void state_layout(const shoc_tr_gpu *h, long long hd[8]) {

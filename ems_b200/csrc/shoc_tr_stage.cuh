@@ -56,36 +56,43 @@ __device__ __forceinline__ void face_zero(Face &f) {
   f.bits = 0;
 }
 
-// weights of one face from its Courant number and metric factors
+// Weights of one face from its Courant number and metric factors, with every
+// rounding explicit (FMA contraction cannot change them): two threads folding
+// the same face from the same inputs get the same bits, so a cell's east
+// (north, top) face computed by the cell itself equals its neighbour's own
+// west (south, bottom) face, and no mass is made between them.
 __device__ __forceinline__ void set_face(Face &f, bool quick, float cr, float d, float Ap,
                                          float Bp, float Am, float Bm, float U, bool ult,
                                          float K) {
   f.bits = (cr > 0.f ? FB_POS : 0) | (cr < 0.f ? FB_NEG : 0) | ((ult && cr != 0.f) ? FB_ULT : 0);
   if (quick) {
-    const float a = d - 0.5f * cr, b = (1.f - cr * cr) * (1.f / 6.f);
+    const float a = __fmaf_rn(-0.5f, cr, d);
+    const float b = __fmul_rn(__fmaf_rn(-cr, cr, 1.f), 1.f / 6.f);
     if (cr > 0.f) {
-      f.wa = -b * Bp;
-      f.w1 = 1.f - a + 2.f * b;
-      f.w2 = a - b * Ap;
+      f.wa = __fmul_rn(-b, Bp);
+      f.w1 = __fmaf_rn(2.f, b, __fsub_rn(1.f, a));
+      f.w2 = __fmaf_rn(-b, Ap, a);
     } else if (cr < 0.f) {
-      f.wa = -b * Am;
-      f.w1 = 1.f - a - b * Bm;
-      f.w2 = a + 2.f * b;
+      f.wa = __fmul_rn(-b, Am);
+      f.w1 = __fmaf_rn(-b, Bm, __fsub_rn(1.f, a));
+      f.w2 = __fmaf_rn(2.f, b, a);
     } else {
       f.wa = 0.f;
-      f.w1 = 1.f - d;
+      f.w1 = __fsub_rn(1.f, d);
       f.w2 = d;
     }
   } else {
-    f.wa = cr > 0.f ? 0.5f * (1.f - cr) : 0.5f * (1.f + cr);
+    f.wa = cr > 0.f ? __fmul_rn(0.5f, __fsub_rn(1.f, cr)) : __fmul_rn(0.5f, __fadd_rn(1.f, cr));
     f.w1 = f.w2 = 0.f;
   }
-  f.ircr = cr != 0.f ? __fdividef(1.f, fabsf(cr)) : 0.f;
+  f.ircr = cr != 0.f ? __frcp_rn(fabsf(cr)) : 0.f;
   f.U = U;
   f.K = K;
 }
 
-// one face value: tm2..tp1 at i-2..i+1 of the face's cell
+// One face flux, every rounding explicit: QUICKEST or Van Leer from the
+// values tm2..tp1 at i-2..i+1 of the face's cell, then ULTIMATE, times the
+// volume flux, minus the horizontal-diffusion term.
 template <bool QUICK, bool ULT>
 __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm2, float tm1,
                                       float t0, float tp1) {
@@ -94,14 +101,15 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
     const bool pos = (f.bits & FB_POS) != 0;
     const float tu = pos ? tm2 : tp1;
     if (QUICK) {
-      F = f.wa * tu + f.w1 * tm1 + f.w2 * t0;
+      F = __fmaf_rn(f.wa, tu, __fmaf_rn(f.w1, tm1, __fmul_rn(f.w2, t0)));
     } else {
       const bool neg = (f.bits & FB_NEG) != 0;
-      const float p = pos ? (tm1 - tm2) : (t0 - tm1), q = pos ? (t0 - tm1) : (tp1 - t0);
-      const float den = pos ? (t0 - tm2) : (tp1 - tm1);
-      const float pq = p * q;
-      const float df = pq > 0.f ? 2.f * __fdividef(pq, den) : 0.f;
-      F = pos ? tm1 + f.wa * df : (neg ? t0 - f.wa * df : 0.f);
+      const float p = pos ? __fsub_rn(tm1, tm2) : __fsub_rn(t0, tm1);
+      const float q = pos ? __fsub_rn(t0, tm1) : __fsub_rn(tp1, t0);
+      const float den = pos ? __fsub_rn(t0, tm2) : __fsub_rn(tp1, tm1);
+      const float pq = __fmul_rn(p, q);
+      const float df = pq > 0.f ? __fmul_rn(2.f, __fdiv_rn(pq, den)) : 0.f;
+      F = pos ? __fmaf_rn(f.wa, df, tm1) : (neg ? __fmaf_rn(-f.wa, df, t0) : 0.f);
     }
     if (ULT) {
       // ulimate_filter (tracers.c:3526-3554) without its divisions: with
@@ -113,12 +121,13 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       // and the limiter falls back to upwind, so FP32 rounding of the stored
       // tracer does not flip the limiter's decision.
       const float tc = pos ? tm1 : t0, td = pos ? t0 : tm1;
-      const float diff = td - tu;
+      const float diff = __fsub_rn(td, tu);
       const float sg = diff < 0.f ? -1.f : 1.f;
-      const float d = fabsf(diff), c = (tc - tu) * sg, a = (F - tu) * sg;
-      const float q = c * f.ircr;
+      const float d = fabsf(diff);
+      const float c = __fmul_rn(__fsub_rn(tc, tu), sg), a = __fmul_rn(__fsub_rn(F, tu), sg);
+      const float q = __fmul_rn(c, f.ircr);
       float G = F;
-      if (a > q) G = tu + sg * q;
+      if (a > q) G = __fmaf_rn(sg, q, tu);
       if (a < c) G = tc;
       if (a > d) G = td;
       if (!(c >= 0.f && c <= d)) G = tc;
@@ -126,9 +135,9 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       // one straight-line block the compiler can interleave
       F = (f.bits & FB_ULT) ? G : F;
     }
-    F *= f.U;
+    F = __fmul_rn(F, f.U);
   }
-  if (hd) F -= f.K * (t0 - tm1);
+  if (hd) F = __fmaf_rn(-f.K, __fsub_rn(t0, tm1), F);
   return F;
 }
 

@@ -9,23 +9,41 @@
 //           layer and its loads coalesce.  The thread folds its cell's
 //           tracer-independent face coefficients once (QUICKEST weights,
 //           ULTIMATE 1/|cr|, volume flux, horizontal-diffusion factor) and
-//           then loops over the advected tracers, two at a time: the stencil
-//           values are independent loads, the west-face flux of the next
-//           lane's cell is this cell's east-face flux (shuffle).  Output, in
-//           the destination tracer array: the new value of cells below the
-//           surface, the FP64-summed horizontal flux divergence of the
-//           surface cell and the cells above it; the surface cell's
-//           bottom-face flux goes to a per-(tracer, column) array.
+//           then loops over the advected tracers: the stencil values are
+//           independent loads, the west-face flux of the next lane's cell is
+//           this cell's east-face flux (shuffle), and every face a cell
+//           computes for itself is rounded as its neighbour rounds it.  The
+//           flux divergence and the new value are FP64.  Output, in the
+//           destination tracer array (FP32): the new value of cells below
+//           the surface, the horizontal flux divergence of the surface cell
+//           and the cells above it; beside it, the FP32 rounding residual of
+//           each of those values (value - stored, so stored + residual is the
+//           FP64 value to 2^-48); the surface cell's bottom-face flux goes to
+//           a per-(tracer, column) array.
 //
 //  k_vd32   one thread per (column, tracer): tr_bounds (tracers.c:3217-3324),
 //           surf_conc's column-mass balance (:3097-3206, FP64 Neumaier), the
 //           copy above the surface and, on the last sub-step, the implicit
 //           vertical diffusion (implicit_vdiff_tr, :4067-4214) as an FP32
-//           Thomas sweep, an FP64 residual and one FP32 correction solve.
-//           A block owns 32 columns of similar depth (a static depth-sorted
-//           column order) so its lanes loop over similar layer ranges; the
-//           columns' values and LU factors are staged into shared memory in
-//           one batch of asynchronous copies.
+//           Thomas sweep, an FP64 residual and one FP32 correction solve,
+//           with the column's FP64 mass carry (column_finish).  A block owns
+//           32 columns of similar depth (a static depth-sorted column order)
+//           so its lanes loop over similar layer ranges; the columns' values,
+//           residuals, LU factors and FP64 thicknesses are staged into shared
+//           memory in one batch of asynchronous copies.
+//
+// Mass carry.  Storing FP32 values loses mass at every rounding (and the
+// FP32 solve conserves the column mass only to its residual).  Per (tracer,
+// column) the kernels keep, in FP64, the mass the stored values owe the
+// column: carry' = carry + M_exact - M_stored, where M_exact is the FP64 mass
+// the sub-step computed (the FP64 advected values, the surf_conc surface
+// value, tr_bounds' clipping) and M_stored the mass of what was stored.  The
+// carry goes back into the column at the next sub-step as a uniform shift of
+// its values (carry / (area x depth)), inside the solve's FP64 residual when
+// there is a solve, so the stored values plus the carry conserve mass to
+// FP64 round-off and the carry stays within a few FP32 ulps of the column
+// mass.  The mass diagnostic adds it.  Columns whose surface moves during the
+// step (eta != oldeta) keep their carry as it is.
 //
 // The cells of a column at every layer come from a static layer-by-column
 // table, so no thread walks a column to find them.
@@ -110,7 +128,8 @@ __device__ __forceinline__ TileCol tile_column(const Geo &G, const Work &W, cons
 
 namespace f32 {
 
-// Face coefficients of one horizontal face at a cell with the given flags.
+// Face coefficients of one horizontal face at a cell with the given flags
+// (cr = u dt / h, rounded by the caller as __fmul_rn(__fmul_rn(u, dt), 1/h)).
 __device__ __forceinline__ void hface(Face &f, bool wet, bool eb, bool quick, bool ult,
                                       float cr, float U, float K, const Face2 &m) {
   if (!wet) {  // a ghost: the face carries nothing
@@ -127,16 +146,17 @@ __device__ __forceinline__ void hface(Face &f, bool wet, bool eb, bool quick, bo
 
 // Vertical face at the bottom of a cell from the thicknesses of the two cells
 // below it (dzm2, dzm1), the cell (dz0) and the one above (dzp1; the
-// surface-layer cell maps onto itself, top != 0), and w * dtu.
+// surface-layer cell maps onto itself, top != 0), and w * dtu; IEEE
+// divisions, so the cell below folds its top face to the same bits.
 __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2, float dzm1,
                                       float dz0, float dzp1, bool top, float wv) {
-  const float w9m = 0.5f * (dzm1 + dzm2);
-  const float w90 = 0.5f * (dz0 + dzm1);
-  const float w9p = top ? w90 : 0.5f * (dzp1 + dz0);
-  const float cz = __fdividef(wv, w90);
-  const float db = __fdividef(2.f, w9m + w90), df = __fdividef(2.f, w90 + w9p);
-  set_face(f, quick, cz, __fdividef(dzm1, dzm1 + dz0), db * w9m, db * w90, df * w90, df * w9p,
-           wv, ult, 0.f);
+  const float w9m = __fmul_rn(0.5f, __fadd_rn(dzm1, dzm2));
+  const float w90 = __fmul_rn(0.5f, __fadd_rn(dz0, dzm1));
+  const float w9p = top ? w90 : __fmul_rn(0.5f, __fadd_rn(dzp1, dz0));
+  const float cz = __fdiv_rn(wv, w90);
+  const float db = __fdiv_rn(2.f, __fadd_rn(w9m, w90)), df = __fdiv_rn(2.f, __fadd_rn(w90, w9p));
+  set_face(f, quick, cz, __fdiv_rn(dzm1, __fadd_rn(dzm1, dz0)), __fmul_rn(db, w9m),
+           __fmul_rn(db, w90), __fmul_rn(df, w90), __fmul_rn(df, w9p), wv, ult, 0.f);
 }
 
 }  // namespace f32
@@ -164,6 +184,7 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
                                                      const f32::Face2 *__restrict__ fy2,
                                                      const float *__restrict__ tri,
                                                      float *__restrict__ tro,
+                                                     float *__restrict__ rso,
                                                      float *__restrict__ fzs, int any_hd) {
   using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
@@ -227,21 +248,21 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
   double idz = 0.0, ia = 0.0;
   if (on) {
     const Face2 mx = fx2[c2], my = fy2[c2];
-    hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT, F3.u1[c] * fdtu * mx.ih, F3.u1flux3d[c],
-          hdf ? F3.khx[c] : 0.f, mx);
-    hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT, F3.u2[c] * fdtu * my.ih, F3.u2flux3d[c],
-          hdf ? F3.khy[c] : 0.f, my);
+    hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT, __fmul_rn(__fmul_rn(F3.u1[c], fdtu), mx.ih),
+          F3.u1flux3d[c], hdf ? F3.khx[c] : 0.f, mx);
+    hface(fs, fl & CF_WET, fl & CF_E2, QUICK, ULT, __fmul_rn(__fmul_rn(F3.u2[c], fdtu), my.ih),
+          F3.u2flux3d[c], hdf ? F3.khy[c] : 0.f, my);
     if (fl & FL_YP_WET) {
       const int yp = n1.w;
       const Face2 mn = fy2[me.y];
-      hface(fn, true, fl & FL_YP_E2, QUICK, ULT, F3.u2[yp] * fdtu * mn.ih, F3.u2flux3d[yp],
-            hdf ? F3.khy[yp] : 0.f, mn);
+      hface(fn, true, fl & FL_YP_E2, QUICK, ULT, __fmul_rn(__fmul_rn(F3.u2[yp], fdtu), mn.ih),
+            F3.u2flux3d[yp], hdf ? F3.khy[yp] : 0.f, mn);
     }
     if (!sxp1 && (fl & FL_XP_WET)) {
       const int xp = n1.y;
       const Face2 mxe = fx2[me.x];
-      hface(fe, true, fl & FL_XP_E1, QUICK, ULT, F3.u1[xp] * fdtu * mxe.ih, F3.u1flux3d[xp],
-            hdf ? F3.khx[xp] : 0.f, mxe);
+      hface(fe, true, fl & FL_XP_E1, QUICK, ULT, __fmul_rn(__fmul_rn(F3.u1[xp], fdtu), mxe.ih),
+            F3.u1flux3d[xp], hdf ? F3.khx[xp] : 0.f, mxe);
     }
     const float dz0 = W.dz32[c];
     if (k <= ks) {
@@ -250,14 +271,14 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
       const bool top = (nzv.z == c);
       const float dzp1 = W.dz32[nzv.z];
-      zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, F3.w[c] * fdtu);
+      zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
       if (k < ks) {  // the bottom face of the cell above
         const bool top1 = (nzv.w == nzv.z);
         const float dzp2 = W.dz32[nzv.w];
-        zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, F3.w[nzv.z] * fdtu);
+        zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, __fmul_rn(F3.w[nzv.z], fdtu));
       }
     }
-    idz = (double)__fdividef(1.f, dz0);
+    idz = 1.0 / W.dz[c];  // the FP64 thickness: the update conserves mass to FP64 round-off
     ia = 1.0 / G.cellarea[c2];
   }
   // vertical neighbours (bottom: the sediment ghost holds the bottom value,
@@ -327,15 +348,16 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         if (!on || n >= ntc) continue;
         // FP64 flux divergence (tracers.c:888-892)
         const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
-        float val;
+        double a = dtr;
         if (zt) {
           const float Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
-          val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
-        } else {
-          val = (float)dtr;
-          if (zf) fzs[(size_t)n * G.ncol + col] = Fzb;
+          a = (double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz;
+        } else if (zf) {
+          fzs[(size_t)n * G.ncol + col] = Fzb;
         }
+        const float val = (float)a;
         tro[(size_t)n * G.S + c] = val;
+        rso[(size_t)n * G.S + c] = (float)(a - (double)val);
       }
     }
   } else {
@@ -396,45 +418,225 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       if (sxp1) Fxe = Fnext;
       // FP64 flux divergence (tracers.c:888-892)
       const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
-      float val;
-      if (zt) {
-        val = (float)((double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz);
-      } else {
-        val = (float)dtr;
-        if (k == ks) fzs[(size_t)nn[u] * G.ncol + col] = Fzb;
-      }
+      double a = dtr;
+      if (zt)
+        a = (double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz;
+      else if (k == ks)
+        fzs[(size_t)nn[u] * G.ncol + col] = Fzb;
+      const float val = (float)a;
       tro[(size_t)nn[u] * G.S + c] = val;
+      rso[(size_t)nn[u] * G.S + c] = (float)(a - (double)val);
     }
   }
   }
 }
 
 // ---------------------------------------------------------------------------
+// column_finish: the end of an FP32-mixed sub-step for one (column, tracer),
+// shared by k_vd32 and the fused k_step32.
+
+// Advected tracers' column sums from the advection: the FP64 mass of the
+// advected values below the surface (sum of a dz), the FP64 horizontal
+// divergence of the surface cell and the cells above it, and the surface
+// cell's bottom-face flux.
+struct ColSums {
+  double m, dv;
+  float fzb;
+};
+
+// A0, S0: the column's values and Thomas storage from its bottom layer up, row
+// stride sa; an advected tracer (tbdy) holds its advected values below the
+// surface, any other tracer every layer's old value (A0 is overwritten, so is
+// S0).  L0, C0, D0: LU factors, cells and FP64 thicknesses, row stride 32.
+// carry: [ntr][ncol] (null: none).  Adds the values it flags to nwarn and
+// sets bad for a NaN among what it stores.
+template <bool LAST>
+__device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const Work &W,
+                                              const Opt &O, const TrSet &T, const SubStep &ss,
+                                              const TileCol &tc, int col, int n, bool tbdy,
+                                              bool adv, bool vdf, float *A0, float *S0, int sa,
+                                              const float4 *L0, const int *C0, const double *D0,
+                                              const float *tr, float *to, double area, double ia,
+                                              double H, double idt, const ColSums &cs,
+                                              double *carry, bool steady, long long &nwarn,
+                                              bool &bad) {
+  const ColInfo &ci = tc.ci;
+  const int kb = tc.kb, nz = G.nz, c2 = tc.c2;
+  const int nk = tc.ks - kb;  // cells below the surface cell
+  const bool single = (ci.flags & COL_SINGLE) != 0;
+  const bool solve = vdf && !single;
+  const double mn = T.mintr[n], mx = T.maxtr[n];
+  const double dzs_old = (double)W.dz32[ci.s];
+  const double ts_old = (double)tr[ci.s];  // surface value before the sub-step
+  const double dzs = D0[nk * 32];
+  const double carry_in = (carry && steady) ? carry[(size_t)n * G.ncol + col] : 0.0;
+  // the carry goes back as a uniform shift of the column's values
+  const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
+  // FP64 mass bookkeeping per unit area: what the step computed (mx*) and
+  // what is stored (ms*), compensated sums
+  double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
+  if (H > 0.0) f32::neumaier_add(mxs, mxc, carry_in * ia);
+  long long nw = 0;
+  double vs = ts_old;  // the surface value
+  if (!tbdy) {
+    for (int j = 0; j < nk; ++j)
+      f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * sa], D0[j * 32]));
+    vs = (double)A0[nk * sa];
+    f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+    for (int j = nk + 1; j < nz - kb; ++j) {
+      to[C0[j * 32]] = A0[j * sa];
+      bad |= isnan(A0[j * sa]);
+    }
+  } else {
+    // tr_bounds clip and range check (:3278-3293) of the cells below the
+    // surface; a < mn and a > mx of a float a, exactly, as float compares
+    const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
+    const bool clip = mn <= kClipEps;
+    f32::neumaier_add(mxs, mxc, cs.m);
+    for (int j = 0; j < nk; ++j) {
+      float a = A0[j * sa];
+      if (clip && a < mn_up) {
+        f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, D0[j * 32]));
+        a = mnf;
+      }
+      nw += (a < mn_up || a > mx_dn);
+      A0[j * sa] = a;
+    }
+    const double a_below = nk > 0 ? (double)A0[(nk - 1) * sa] : 0.0;
+    // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
+    if (adv) {
+      const double wb = (ci.s == tc.cbot) ? G.botz[c2] : G.gridz[ci.s];
+      const double eta = F.eta[c2], oe = F.oldeta[c2];
+      const double osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
+      const double sub = oe + ss.subeta_f * (eta - oe);
+      double ssum = 0.0, scomp = 0.0;
+      f32::neumaier_add(ssum, scomp, __dmul_rn((double)cs.fzb, area));
+      f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
+      f32::neumaier_add(ssum, scomp, -cs.dv);
+      const double dzn = sub - wb;
+      const double svol = dzn * area;
+      const double st = ssum + scomp;
+      const double sv = (svol == 0.0 || (st < 0.0 && dzn <= O.hmin)) ? 0.0 : st / svol;
+      vs = (G.botz[c2] > 0.0 && dzs_old < O.hmin) ? ts_old : sv;
+    }
+    if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
+    if (mn <= kClipEps && vs < mn) vs = mn;
+    if (vs < mn || vs > mx) ++nw;
+    bad |= isnan(vs);
+    f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+    const float vs32 = (float)vs;
+    for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
+  }
+  if (!solve) {
+    // the values as they are, plus the carry's shift (tr_bounds has run)
+    for (int j = 0; j < nk; ++j) {
+      const float fin = (float)((double)A0[j * sa] + dl);
+      to[C0[j * 32]] = fin;
+      bad |= isnan(fin);
+      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
+    }
+    const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
+    const float fin = (vdf && single) ? (float)(vs + dl + F.dt * (0.0 - 0.0) / h)
+                                      : (float)(vs + dl);
+    to[ci.s] = fin;
+    bad |= isnan(fin);
+    f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+  } else {
+    A0[nk * sa] = (float)vs;
+    // FP32 forward sweep
+    float fwd = 0.f;  // the bottom row's cm1 is 0
+    for (int j = 0; j <= nk; ++j) {
+      const float4 lu = L0[j * 32];
+      fwd = (lu.x * A0[j * sa] - lu.y * fwd) * lu.z;
+      S0[j * sa] = fwd;
+    }
+    // back substitution (FP32), x(j) replacing s(j), and one row behind it
+    // the FP64 residual of b - A x for A = dz/dt I + the diffusion operator,
+    //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
+    // (cp1(j) = cm1(j+1); the bottom row has no cm1 term, the top row no cp1
+    // term), which replaces a(j); the diagonal is the FP64 dz / dt, so the
+    // refined solve keeps the column mass the mass diagnostic measures.  The
+    // FP64 copies of x and of the factors are carried from row to row.
+    float x1 = fwd;
+    float4 l1 = L0[nk * 32];
+    double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
+    double dzdt1 = dzs * idt;
+    for (int j = nk - 1; j >= 0; --j) {
+      const float x = S0[j * sa] - l1.w * x1;
+      S0[j * sa] = x;
+      const double xd = (double)x, l1y = (double)l1.y;
+      const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * sa]) + dl;
+      double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
+      if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
+      A0[(j + 1) * sa] = (float)r;
+      x1 = x;
+      xd2 = xd1;
+      xd1 = xd;
+      l2y = l1y;
+      l1 = L0[j * 32];
+      dzdt1 = D0[j * 32] * idt;
+    }
+    {
+      const double a0 = ((nk == 0) ? vs : (double)A0[0]) + dl;
+      double r = dzdt1 * (a0 - xd1) - (double)l1.y * (xd1 - xd1);
+      if (nk > 0) r = r - l2y * (xd2 - xd1);
+      A0[0] = (float)r;
+    }
+    // correction solve (FP32 forward and back) and the update in FP64
+    float u = 0.f;
+    for (int j = 0; j <= nk; ++j) {
+      const float4 lu = L0[j * 32];
+      u = (A0[j * sa] - lu.y * u) * lu.z;
+      A0[j * sa] = u;
+    }
+    float d = A0[nk * sa];
+    {
+      const float fin = (float)((double)S0[nk * sa] + (double)d);
+      to[C0[nk * 32]] = fin;
+      bad |= isnan(fin);
+      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+    }
+    for (int j = nk - 1; j >= 0; --j) {
+      d = A0[j * sa] - L0[(j + 1) * 32].w * d;
+      const float fin = (float)((double)S0[j * sa] + (double)d);
+      to[C0[j * 32]] = fin;
+      bad |= isnan(fin);
+      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
+    }
+  }
+  if (carry && steady) carry[(size_t)n * G.ncol + col] = ((mxs + mxc) - (mss + msc)) * area;
+  nwarn += nw;
+}
+
+// ---------------------------------------------------------------------------
 // k_vd32
 
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
-// LU float4[nd][32], colC int[nd][32], A, S float[nd][nw][32]
+// LU float4[nd][32], thicknesses double[nd][32], colC int[nd][32], A, S
+// float[nd][nw][32]
 inline size_t vd32_smem(int nd, int nw) {
-  return (size_t)nd * 32 * 16 + (size_t)nd * 32 * 4 + (size_t)2 * nd * nw * 32 * 4;
+  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)2 * nd * nw * 32 * 4;
 }
 
 template <bool LAST>
 __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSet T,
                                               SubStep ss, Tile Tl,
                                               const float4 *__restrict__ lu32,
-                                              const float *__restrict__ dz32,
                                               const float *__restrict__ tri,
                                               float *__restrict__ tro,
+                                              const float *__restrict__ rsi,
+                                              double *__restrict__ carry,
                                               const float *__restrict__ fzs, int nw,
                                               int nchunk, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
   // the arrays hold layers kbase .. nz-1 (every column of this launch's
   // tiles starts at or above kbase), row r = layer - kbase
   const int nz = G.nz, nd = nz - kbase;
-  float4 *LU = reinterpret_cast<float4 *>(smem);        // [nd][32]
-  int *colC = reinterpret_cast<int *>(LU + nd * 32);     // [nd][32]
-  float *A = reinterpret_cast<float *>(colC + nd * 32);  // [nd][nw][32]
-  float *Sv = A + nd * nw * 32;                          // [nd][nw][32]
+  float4 *LU = reinterpret_cast<float4 *>(smem);          // [nd][32]
+  double *DZ = reinterpret_cast<double *>(LU + nd * 32);  // [nd][32]
+  int *colC = reinterpret_cast<int *>(DZ + nd * 32);      // [nd][32]
+  float *A = reinterpret_cast<float *>(colC + nd * 32);   // [nd][nw][32]
+  float *Sv = A + nd * nw * 32;                           // [nd][nw][32]
 
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int tile = tile0 + blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
@@ -449,13 +651,13 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
     if (chunk == 0 && wy == 0) atomicOr(W.status, ST_GEOM);
   }
   const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
-  const ColInfo ci = tc.ci;
   const int kmin = __reduce_min_sync(0xffffffffu, act ? kb : nz);
   for (int k = kmin + wy; k < nz; k += nw) {
     const int c = (act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
     const int r = k - kbase;
     colC[r * 32 + lane] = c;
     if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &lu32[c]);
+    if (c && k <= ks) cp_async8(&DZ[r * 32 + lane], &W.dz[c]);
   }
   cp_async_commit();
   cp_async_wait<0>();
@@ -468,168 +670,50 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   const bool tbdy = (tf & TR_TBDY) != 0;
   const bool adv = tbdy && (tf & TR_ADV);
   const bool vdf = LAST && (tf & TR_VDIFF);
-  const bool single = (ci.flags & COL_SINGLE) != 0;
-  const bool solve = vdf && !single;
   const float *tr = tri + (size_t)n * G.S;
   float *to = tro + (size_t)n * G.S;
-  float *Aj = A + wy * 32 + lane;
-  float *Sj = Sv + wy * 32 + lane;
-  // the column's values: advection results (advected tracers) or the old
-  // values (the rest)
+  float *const A0 = A + wy * 32 + lane + (kb - kbase) * sa;
+  float *const S0 = Sv + wy * 32 + lane + (kb - kbase) * sa;
+  const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
+  const int *const C0 = colC + (kb - kbase) * 32 + lane;
+  const double *const D0 = DZ + (kb - kbase) * 32 + lane;
+  // the column's values: advection results and their rounding residuals
+  // (advected tracers, residuals into the Thomas storage until the sweep)
+  // or the old values (the rest)
   {
     const float *src = tbdy ? to : tr;
-    for (int k = kb; k < nz; ++k)
-      cp_async4(&Aj[(k - kbase) * sa], src + colC[(k - kbase) * 32 + lane]);
+    for (int j = 0; j < nz - kb; ++j) cp_async4(&A0[j * sa], src + C0[j * 32]);
+    if (tbdy) {
+      const float *rs = rsi + (size_t)n * G.S;
+      for (int j = 0; j < nz - kb; ++j) cp_async4(&S0[j * sa], rs + C0[j * 32]);
+    }
     cp_async_commit();
   }
-  const double mn = T.mintr[n], mx = T.maxtr[n];
   {  // sediment ghost (tracers.c:827-830)
     const int sed = G.zm1[cbot];
     to[sed] = tbdy ? tr[cbot] : tr[sed];
   }
-  const double dzs_old = (double)dz32[ci.s];
-  const double ts_old = (double)tr[ci.s];  // surface value before the sub-step
-  const double area = G.cellarea[c2];
-  double Fzb_s = 0.0, wb = 0.0, osub = 0.0, sub = 0.0;
-  if (adv) {
-    Fzb_s = (double)fzs[(size_t)n * G.ncol + col];
-    wb = (ci.s == cbot) ? G.botz[c2] : G.gridz[ci.s];
-    const double eta = F.eta[c2], oe = F.oldeta[c2];
-    osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
-    sub = oe + ss.subeta_f * (eta - oe);
-  }
+  const double area = G.cellarea[c2], ia = 1.0 / area;
+  const bool steady = F.eta[c2] == F.oldeta[c2];
+  // the water depth the carry is spread over
+  const int nk = ks - kb;
+  double H = 0.0;
+  for (int j = 0; j <= nk; ++j) H += D0[j * 32];
+  ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.f};
   cp_async_wait<0>();
-
-  // the column in shared memory, from its bottom layer up: value (A),
-  // Thomas storage (S), LU factors {dzdt, cm1, 1/div, ud} (L), cell (C)
-  float *const A0 = Aj + (kb - kbase) * sa;
-  float *const S0 = Sj + (kb - kbase) * sa;
-  const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
-  const int *const C0 = colC + (kb - kbase) * 32 + lane;
-  const int nk = ks - kb;  // cells below the surface cell
+  if (tbdy) {
+    // the FP64 advected values are stored + residual
+    double m = 0.0, mc = 0.0, dv = 0.0;
+    for (int j = 0; j < nk; ++j)
+      f32::neumaier_add(m, mc, __dmul_rn((double)A0[j * sa] + (double)S0[j * sa], D0[j * 32]));
+    for (int j = nk; j < nz - kb; ++j) dv += (double)A0[j * sa] + (double)S0[j * sa];
+    cs.m = m + mc;
+    cs.dv = dv;
+  }
   long long nwarn = 0;
   bool bad = false;  // a NaN among the values this thread stores
-  float fwd = 0.f;  // Thomas forward carry (the bottom row's cm1 is 0)
-  if (!tbdy) {
-    for (int j = 0; j < nz - kb; ++j) {
-      to[C0[j * 32]] = A0[j * sa];
-      bad |= isnan(A0[j * sa]);
-    }
-    if (vdf && single) {
-      const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-      to[ci.s] = (float)((double)A0[nk * sa] + F.dt * (0.0 - 0.0) / h);
-    } else if (solve) {
-      for (int j = 0; j <= nk; ++j) {
-        const float4 lu = L0[j * 32];
-        fwd = (lu.x * A0[j * sa] - lu.y * fwd) * lu.z;
-        S0[j * sa] = fwd;
-      }
-    }
-  } else {
-    // tr_bounds clip and range check (:3278-3293) of the cells below the
-    // surface; a < mn and a > mx of a float a, exactly, as float compares
-    const double a_below = nk > 0 ? (double)A0[(nk - 1) * sa] : 0.0;
-    const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
-    const bool clip = mn <= kClipEps;
-    if (solve) {
-      for (int j = 0; j < nk; ++j) {
-        float a = A0[j * sa];
-        if (clip && a < mn_up) a = mnf;
-        nwarn += (a < mn_up || a > mx_dn);
-        bad |= isnan(a);
-        A0[j * sa] = a;
-        const float4 lu = L0[j * 32];
-        fwd = (lu.x * a - lu.y * fwd) * lu.z;
-        S0[j * sa] = fwd;
-      }
-    } else {
-      for (int j = 0; j < nk; ++j) {
-        float a = A0[j * sa];
-        if (clip && a < mn_up) a = mnf;
-        nwarn += (a < mn_up || a > mx_dn);
-        bad |= isnan(a);
-        to[C0[j * 32]] = a;
-      }
-    }
-    // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
-    double vs = ts_old;
-    if (adv) {
-      double ssum = 0.0, scomp = 0.0;
-      f32::neumaier_add(ssum, scomp, __dmul_rn(Fzb_s, area));
-      f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
-      for (int j = nk; j < nz - kb; ++j) f32::neumaier_add(ssum, scomp, -(double)A0[j * sa]);
-      const double dzs = sub - wb;
-      const double svol = dzs * area;
-      const double st = ssum + scomp;
-      const double sv = (svol == 0.0 || (st < 0.0 && dzs <= O.hmin)) ? 0.0 : st / svol;
-      vs = (G.botz[c2] > 0.0 && dzs_old < O.hmin) ? ts_old : sv;
-    }
-    if ((ci.flags & COL_THIN) && (vs < mn || vs > mx)) vs = a_below;
-    if (mn <= kClipEps && vs < mn) vs = mn;
-    if (vs < mn || vs > mx) ++nwarn;
-    bad |= isnan(vs);
-    const float vs32 = (float)vs;
-    for (int j = nk; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
-    if (vdf && single) {
-      const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-      to[ci.s] = (float)(vs + F.dt * (0.0 - 0.0) / h);
-    } else if (solve) {
-      const float4 lu = L0[nk * 32];
-      A0[nk * sa] = vs32;
-      S0[nk * sa] = (lu.x * vs32 - lu.y * fwd) * lu.z;
-    }
-  }
-  if (solve) {
-    // back substitution (FP32), x(j) replacing s(j), and in the same pass
-    // down the column the FP64 residual of the row above,
-    //   r(j) = dzdt (a - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
-    // (the difference form of b - A x for A = dzdt I + the diffusion
-    // operator, cp1(j) = cm1(j+1)), which replaces a(j); the bottom row has
-    // no cm1 term (x(-1) = x(0)), the top row no cp1 term.  The correction
-    // solve runs on r in FP32 and the update x + d is added in FP64.  The
-    // FP64 copies of x and of the factors are carried from row to row, so
-    // each value is converted once.
-    float x1 = S0[nk * sa];      // x(j + 1)
-    float4 l1 = L0[nk * 32];     // factors of row j + 1
-    double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;  // x(j + 1), x(j + 2), cm1(j + 2)
-    for (int j = nk - 1; j >= 0; --j) {
-      const float x = S0[j * sa] - l1.w * x1;
-      S0[j * sa] = x;
-      const double xd = (double)x, l1y = (double)l1.y;
-      double r = (double)l1.x * ((double)A0[(j + 1) * sa] - xd1) - l1y * (xd - xd1);
-      if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
-      A0[(j + 1) * sa] = (float)r;
-      x1 = x;
-      xd2 = xd1;
-      xd1 = xd;
-      l2y = l1y;
-      l1 = L0[j * 32];
-    }
-    {
-      double r = (double)l1.x * ((double)A0[0] - xd1) - (double)l1.y * (xd1 - xd1);
-      if (nk > 0) r = r - l2y * (xd2 - xd1);
-      A0[0] = (float)r;
-    }
-    // correction solve (FP32 forward and back) and update in FP64
-    float u = 0.f;
-    for (int j = 0; j <= nk; ++j) {
-      const float4 lu = L0[j * 32];
-      u = (A0[j * sa] - lu.y * u) * lu.z;
-      A0[j * sa] = u;
-    }
-    float d = A0[nk * sa];
-    {
-      const float fin = (float)((double)S0[nk * sa] + (double)d);
-      to[C0[nk * 32]] = fin;
-      bad |= isnan(fin);
-    }
-    for (int j = nk - 1; j >= 0; --j) {
-      d = A0[j * sa] - L0[(j + 1) * 32].w * d;
-      const float fin = (float)((double)S0[j * sa] + (double)d);
-      to[C0[j * 32]] = fin;
-      bad |= isnan(fin);
-    }
-  }
+  column_finish<LAST>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0, D0, tr,
+                      to, area, ia, H, 1.0 / F.dt, cs, carry, steady, nwarn, bad);
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
 }

@@ -141,11 +141,14 @@ def test_fused_and_split_kernels_agree(kw):
     assert np.all(np.abs(a[:, c] - b[:, c]).max(axis=1) <= TOL * np.abs(ref[:, c]).max(axis=1))
 
 
+@pytest.mark.parametrize("kernels", ["split", "fused"])
 @pytest.mark.parametrize("name,steps", [("basin64", 100), ("small", 50)])
-def test_fp32mixed_conserves_mass(name, steps):
+def test_fp32mixed_conserves_mass(name, steps, kernels):
     """FP32 storage loses mass at every rounding; the per-column FP64 carry
-    of the fused kernel gives it back, so the stored values plus the carry
-    conserve each tracer's mass to 1e-12 relative, as the FP64 path does."""
+    gives it back (the two-kernel sub-step from the advection kernel's
+    rounding residuals, the fused one from its FP64 accumulators), so the
+    stored values plus the carry conserve each tracer's mass to 1e-12
+    relative, as the FP64 path does."""
     case = synth.make(name)
-    _, m0, m1 = run_kernels(case, steps, "fused")
+    _, m0, m1 = run_kernels(case, steps, kernels)
     assert np.all(np.abs(m1 - m0) <= 1e-12 * np.abs(m0)), np.abs(m1 - m0) / np.abs(m0)
