@@ -15,7 +15,7 @@ cudaError_t attr(K k, int bytes = 227 * 1024) {
 template <bool Q, bool U, int M>
 void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &W, const TrSet &T,
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
-         const float *tin, float *tout, float *rnd, float *fzs, int hd) {
+         const float *tin, float *tout, float *rnd, double *fzs, int hd) {
   k_adv32<Q, U, M><<<grid, kAdv32Block, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
                                                                   tin, tout, rnd, fzs, hd);
 }
@@ -23,7 +23,7 @@ template <bool Q, bool U>
 void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F3,
               const Work &W, const TrSet &T, const SubStep &ss, const Tile &Tl,
               const f32::Face2 *fx2, const f32::Face2 *fy2, const float *tin, float *tout,
-              float *rnd, float *fzs, int hd) {
+              float *rnd, double *fzs, int hd) {
   if (mode == 1)
     adv<Q, U, 1>(grid, st, G, F3, W, T, ss, Tl, fx2, fy2, tin, tout, rnd, fzs, hd);
   else if (mode == 2)
@@ -51,7 +51,7 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
-                    double *carry, float *fzs, int vd_nw, int any_hd, int adv_flags,
+                    double *carry, double *fzs, int vd_nw, int any_hd, int adv_flags,
                     cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {

@@ -61,7 +61,7 @@ struct Fused {
 // union of the phase-B column arrays float [2][nwb][nd][32] with the phase-A
 // contributions double
 // [8][ngrp][32] followed by its stencil double buffer float [2][13][256],
-// the accumulators double [ntb][32] x 2 and float [ntb][32], and the surface
+// the accumulators double [ntb][32] x 3, and the surface
 // layer of each lane
 constexpr int kStencil = 13;  // values of a cell's advection stencil
 __host__ __device__ inline size_t fused_red(int ngrp) {
@@ -74,7 +74,7 @@ __host__ __device__ inline size_t fused_union(int nd, int nwb, int ngrp) {
 }
 inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
   return (size_t)nd * 32 * (16 + 8) + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
-         (size_t)ntb * 32 * (8 + 8 + 4) + 32 * 4;
+         (size_t)ntb * 32 * (8 + 8 + 8) + 32 * 4;
 }
 
 
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   float *pf = reinterpret_cast<float *>(uni + fused_red(ngrp));   // [2][13][256]
   double *accM = reinterpret_cast<double *>(uni + fused_union(nd, nwb, ngrp));  // [ntb][32]
   double *accD = accM + ntb * 32;                                 // [ntb][32]
-  float *accF = reinterpret_cast<float *>(accD + ntb * 32);       // [ntb][32]
+  double *accF = accD + ntb * 32;                                 // [ntb][32]
   int *sks = reinterpret_cast<int *>(accF + ntb * 32);            // [32]
 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   for (int i = threadIdx.x; i < ntb * 32; i += kFusedThreads) {
     accM[i] = 0.0;
     accD[i] = 0.0;
-    accF[i] = 0.f;
+    accF[i] = 0.0;
   }
   if (w == 0) sks[lane] = tc.act ? ks : -1;
   __syncthreads();
@@ -189,12 +189,13 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
         const bool top = (nzv.z == c);
         const float dzp1 = W.dz32[nzv.z];
-        zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
+        zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu),
+              __dmul_rn(F3.w64[c], dtu));
         if (zt) {  // the bottom face of the cell above, folded alike
           const bool top1 = (nzv.w == nzv.z);
           const float dzp2 = W.dz32[nzv.w];
-          zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1,
-                     __fmul_rn(F3.w[nzv.z], fdtu));
+          zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, __fmul_rn(F3.w[nzv.z], fdtu),
+                __dmul_rn(F3.w64[nzv.z], dtu));
         }
       }
       dz0d = W.dz[c];
@@ -242,23 +243,23 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const float tp1 = v[7 * kFusedThreads], tp2 = v[8 * kFusedThreads];
         const float txm1 = v[9 * kFusedThreads], txm2 = v[10 * kFusedThreads];
         const float txp1 = v[11 * kFusedThreads], txp2 = v[12 * kFusedThreads];
-        const float Fw = hor ? face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1) : 0.f;
-        const float Fs = hor ? face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1) : 0.f;
-        float Fe = (hor && needE) ? face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2) : 0.f;
-        float Fn = (hor && needN) ? face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2) : 0.f;
-        const float Fb = vz ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
-        const float Ft = (vz && zt) ? face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
-                                    : 0.f;
-        const float e = __shfl_down_sync(FULL, Fw, 1);
-        const float nb = __shfl_down_sync(FULL, Fs, 8);
+        const double Fw = hor ? face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1) : 0.0;
+        const double Fs = hor ? face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1) : 0.0;
+        double Fe = (hor && needE) ? face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2) : 0.0;
+        double Fn = (hor && needN) ? face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2) : 0.0;
+        const double Fb = vz ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.0;
+        const double Ft = (vz && zt) ? face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
+                                     : 0.0;
+        const double e = __shfl_down_sync(FULL, Fw, 1);
+        const double nb = __shfl_down_sync(FULL, Fs, 8);
         if (sxp1) Fe = e;
         if (syp1) Fn = nb;
         double contrib = 0.0;
         if (on && n < ntc) {
           // FP64 flux divergence (tracers.c:888-892)
-          const double dtr = (((double)Fe - (double)Fw) + ((double)Fn - (double)Fs)) * dtu;
+          const double dtr = ((Fe - Fw) + (Fn - Fs)) * dtu;
           if (zt) {
-            const double a = (double)t0 - (dtr * ia + ((double)Ft - (double)Fb)) * idz;
+            const double a = (double)t0 - (dtr * ia + (Ft - Fb)) * idz;
             const float a32 = (float)a;
             tro[(size_t)n * G.S + c] = a32;
             nstat |= isnan(a32) ? ST_NAN : 0;
@@ -330,10 +331,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         to[sed] = tbdy ? tr[cbot] : tr[sed];
       }
       const ColSums cs{accM[slot * 32 + lane], accD[slot * 32 + lane],
-                       adv ? accF[slot * 32 + lane] : 0.f};
+                       adv ? accF[slot * 32 + lane] : 0.0};
       bool bad = false;
       cp_async_wait<0>();
-      column_finish<LAST>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, 32, L0, C0, D0,
+      column_finish<LAST, false>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, 32, L0, C0, D0,
                           tr, to, area, ia, H, idt, cs, Fu.carry, steady, nwarn, bad);
       if (bad) nstat |= ST_NAN;
     }

@@ -72,9 +72,8 @@ struct shoc_tr_gpu {
   Flow32 F3{};
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
   Tile tl{};                          // static tables of the column-tile kernels
-  float *fzs = nullptr;               // [ntr][ncol] surface-cell bottom-face flux
   float *rnd = nullptr;               // [ntr][S] FP32 rounding residual of k_adv32's values
-  double *fzs64 = nullptr;            // the same, FP64 path
+  double *fzs64 = nullptr;            // [ntr][ncol] surface-cell bottom-face flux
   int adv_flags = 0;                  // 1 / 2: every advected tracer without / with hdiff
   double *cols = nullptr;             // column-solve entry points: their device arrays
   int *halo_send = nullptr, *halo_recv = nullptr;  // halo exchange plan (device cell lists)
@@ -1212,8 +1211,6 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u1 = fp;
     TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u2 = fp;
     TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.w = fp;
-    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u1flux3d = fp;
-    TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.u2flux3d = fp;
     if (h->any_hdiff) {
       TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.khx = fp;
       TRY(dupload<float>(h, &fp, nullptr, S)); h->F3.khy = fp;
@@ -1229,12 +1226,10 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     }
     TRY(dupload(h, &h->fx2, ax.data(), S2));
     TRY(dupload(h, &h->fy2, ay.data(), S2));
-    TRY(dupload<float>(h, &h->fzs, nullptr, (size_t)ntr * ncol));
     // the FP64 mass each column's stored values owe it
     TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
-  } else {
-    TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   }
+  TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
   if (f32p) {
     // the fused sub-step kernel (SHOC_TR_GPU_KERNELS=fused; the two-kernel
@@ -1276,6 +1271,11 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<double>(h, (double **)&F.u1flux3d, nullptr, S));
   TRY(dupload<double>(h, (double **)&F.u2flux3d, nullptr, S));
   TRY(dupload<double>(h, (double **)&F.Kz, nullptr, S));
+  if (f32p) {  // the FP32-mixed kernels take the FP64 volume fluxes
+    h->F3.u1flux3d = F.u1flux3d;
+    h->F3.u2flux3d = F.u2flux3d;
+    h->F3.w64 = F.w;
+  }
   if (h->any_hdiff) {
     TRY(dupload<double>(h, (double **)&F.dzu1, nullptr, S));
     TRY(dupload<double>(h, (double **)&F.dzu2, nullptr, S));
@@ -1502,7 +1502,7 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
         const Tile tl = vd_classes(h, tw);
         tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
                        h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->rnd,
-                       h->fu.carry, h->fzs, tw,
+                       h->fu.carry, h->fzs64, tw,
                        h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
         if (prof) {  // pairs share events; sync destroys each event once
           h->ev.push_back({0, ev[0], ev[2]});
@@ -1858,9 +1858,7 @@ int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
     k_to_f32<<<592, 256, 0, s>>>(h->F.u1, (float *)h->F3.u1, n);
     k_to_f32<<<592, 256, 0, s>>>(h->F.u2, (float *)h->F3.u2, n);
     k_to_f32<<<592, 256, 0, s>>>(h->F.w, (float *)h->F3.w, n);
-    k_to_f32<<<592, 256, 0, s>>>(h->F.u1flux3d, (float *)h->F3.u1flux3d, n);
-    k_to_f32<<<592, 256, 0, s>>>(h->F.u2flux3d, (float *)h->F3.u2flux3d, n);
-    h->launches += 5;
+    h->launches += 3;
     if (h->any_hdiff) {
       k_khfac<<<592, 256, 0, s>>>(h->G, h->F, (float *)h->F3.khx, (float *)h->F3.khy);
       h->launches++;

@@ -97,7 +97,8 @@ struct Work {
 
 // FP32 copies of the flow fields (FP32-mixed path), made by set_flow.
 struct Flow32 {
-  const float *u1, *u2, *w, *u1flux3d, *u2flux3d;
+  const float *u1, *u2, *w;  // FP32 copies for the Courant numbers
+  const double *u1flux3d, *u2flux3d, *w64;  // the FP64 arrays of Flow: volume fluxes
   const float *khx, *khy;  // dzu1 h2au1 u1kh / h1au1 and the e2 analogue
 };
 

@@ -22,7 +22,7 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
-                    double *carry, float *fzs, int vd_nw, int any_hd, int adv_flags,
+                    double *carry, double *fzs, int vd_nw, int any_hd, int adv_flags,
                     cudaEvent_t *ev);
 
 // allow every k_step32 instance `bytes` of dynamic shared memory

@@ -20,26 +20,33 @@ __device__ __forceinline__ bool staged_column(const ColInfo &ci, int cbot) {
 }
 
 // ===========================================================================
-// FP32-mixed policy: FP32 tracers, face values and Thomas sweeps; FP64 flux
-// divergence, surface column-mass sum (Neumaier), implicit-solve residual and
-// one refinement step.
+// FP32-mixed policy: FP32 tracers, face values and Thomas sweeps; FP64
+// face fluxes (FP32 face value times the FP64 volume flux), flux divergence
+// and cell update, surface column-mass sum (Neumaier), implicit-solve
+// residual and one refinement step, and the columns' FP64 mass carry.
 
 namespace f32 {
 
 // QUICKEST (quickest(), tracers.c:1870-1884) is, for a given sign of the
 // Courant number, linear in the upwind-side value tu (tm2 for cr > 0, tp1 for
-// cr < 0) and the two values beside the face:
-//   F = wa tu + w1 tm1 + w2 t0
-// with the tracer-independent weights folded once per cell from
-// a = d - cr/2, b = (1 - cr^2)/6 and the upwind curvature factors A, B:
-//   cr > 0: wa = -b B, w1 = 1 - a + 2b, w2 = a - b A
-//   cr < 0: wa = -b A, w1 = 1 - a - b B, w2 = a + 2b
-//   cr = 0: wa = 0,    w1 = 1 - d,      w2 = d
-// Van Leer keeps wa = (1 -+ cr)/2 and its flux-limiter form.  Then ULTIMATE
-// (ircr = 1/|cr|), times the volume flux U, minus K (t0 - tm1) for horizontal
-// diffusion.  A face that carries nothing has all weights, U and K zero.
+// cr < 0) and the two values beside the face.  With a = d - cr/2,
+// b = (1 - cr^2)/6 and the upwind curvature factors A + B = 2 (db (hm + h0),
+// df (h0 + hp)), the curvature is a sum of differences, so the face value is
+//   F = tm1 + wg (t0 - tm1) + wa (tu - tc)
+// (tc = tm1 for cr > 0, t0 for cr < 0) with the tracer-independent weights
+//   cr > 0: wg = a - b A,  wa = -b B
+//   cr < 0: wg = a + b B,  wa = -b A
+//   cr = 0: wg = d,        wa = 0
+// folded once per cell.  The weights multiply differences, so their FP32
+// rounding (the same every step while the flow is steady) moves the face
+// value by a fraction of the differences, not of the value itself.  Van Leer
+// keeps wa = (1 -+ cr)/2 and its flux-limiter form.  Then ULTIMATE
+// (ircr = 1/|cr|); the face value times the FP64 volume flux U, minus
+// K (t0 - tm1) for horizontal diffusion, is the FP64 flux.  A face that
+// carries nothing has all weights, U and K zero.
 struct Face {
-  float wa, w1, w2, ircr, U, K;
+  float wg, wa, ircr, K;
+  double U;
   int bits;
 };
 constexpr int FB_POS = 1, FB_NEG = 2, FB_ULT = 4;
@@ -51,8 +58,9 @@ struct Face2 {
 };
 
 __device__ __forceinline__ void face_zero(Face &f) {
-  f.wa = f.w1 = f.w2 = 0.f;
-  f.ircr = f.U = f.K = 0.f;
+  f.wg = f.wa = 0.f;
+  f.ircr = f.K = 0.f;
+  f.U = 0.0;
   f.bits = 0;
 }
 
@@ -62,46 +70,45 @@ __device__ __forceinline__ void face_zero(Face &f) {
 // (north, top) face computed by the cell itself equals its neighbour's own
 // west (south, bottom) face, and no mass is made between them.
 __device__ __forceinline__ void set_face(Face &f, bool quick, float cr, float d, float Ap,
-                                         float Bp, float Am, float Bm, float U, bool ult,
+                                         float Bp, float Am, float Bm, double U, bool ult,
                                          float K) {
   f.bits = (cr > 0.f ? FB_POS : 0) | (cr < 0.f ? FB_NEG : 0) | ((ult && cr != 0.f) ? FB_ULT : 0);
   if (quick) {
     const float a = __fmaf_rn(-0.5f, cr, d);
     const float b = __fmul_rn(__fmaf_rn(-cr, cr, 1.f), 1.f / 6.f);
     if (cr > 0.f) {
+      f.wg = __fmaf_rn(-b, Ap, a);
       f.wa = __fmul_rn(-b, Bp);
-      f.w1 = __fmaf_rn(2.f, b, __fsub_rn(1.f, a));
-      f.w2 = __fmaf_rn(-b, Ap, a);
     } else if (cr < 0.f) {
+      f.wg = __fmaf_rn(b, Bm, a);
       f.wa = __fmul_rn(-b, Am);
-      f.w1 = __fmaf_rn(-b, Bm, __fsub_rn(1.f, a));
-      f.w2 = __fmaf_rn(2.f, b, a);
     } else {
+      f.wg = d;
       f.wa = 0.f;
-      f.w1 = __fsub_rn(1.f, d);
-      f.w2 = d;
     }
   } else {
     f.wa = cr > 0.f ? __fmul_rn(0.5f, __fsub_rn(1.f, cr)) : __fmul_rn(0.5f, __fadd_rn(1.f, cr));
-    f.w1 = f.w2 = 0.f;
+    f.wg = 0.f;
   }
   f.ircr = cr != 0.f ? __frcp_rn(fabsf(cr)) : 0.f;
   f.U = U;
   f.K = K;
 }
 
-// One face flux, every rounding explicit: QUICKEST or Van Leer from the
-// values tm2..tp1 at i-2..i+1 of the face's cell, then ULTIMATE, times the
-// volume flux, minus the horizontal-diffusion term.
+// One face flux, every rounding explicit: the QUICKEST or Van Leer face value
+// from the values tm2..tp1 at i-2..i+1 of the face's cell (FP32), then
+// ULTIMATE, times the FP64 volume flux, minus the horizontal-diffusion term.
 template <bool QUICK, bool ULT>
-__device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm2, float tm1,
-                                      float t0, float tp1) {
-  float F = 0.f;
+__device__ __forceinline__ double face(const Face &f, bool adv, bool hd, float tm2, float tm1,
+                                       float t0, float tp1) {
+  double flux = 0.0;
   if (adv) {
     const bool pos = (f.bits & FB_POS) != 0;
     const float tu = pos ? tm2 : tp1;
+    float F;
     if (QUICK) {
-      F = __fmaf_rn(f.wa, tu, __fmaf_rn(f.w1, tm1, __fmul_rn(f.w2, t0)));
+      const float tc = pos ? tm1 : t0;
+      F = __fmaf_rn(f.wa, __fsub_rn(tu, tc), __fmaf_rn(f.wg, __fsub_rn(t0, tm1), tm1));
     } else {
       const bool neg = (f.bits & FB_NEG) != 0;
       const float p = pos ? __fsub_rn(tm1, tm2) : __fsub_rn(t0, tm1);
@@ -135,10 +142,10 @@ __device__ __forceinline__ float face(const Face &f, bool adv, bool hd, float tm
       // one straight-line block the compiler can interleave
       F = (f.bits & FB_ULT) ? G : F;
     }
-    F = __fmul_rn(F, f.U);
+    flux = __dmul_rn((double)F, f.U);
   }
-  if (hd) F = __fmaf_rn(-f.K, __fsub_rn(t0, tm1), F);
-  return F;
+  if (hd) flux = __dsub_rn(flux, (double)__fmul_rn(f.K, __fsub_rn(t0, tm1)));
+  return flux;
 }
 
 // Neumaier compensated sum; the explicitly rounded operations keep the

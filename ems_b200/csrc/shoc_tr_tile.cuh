@@ -131,7 +131,7 @@ namespace f32 {
 // Face coefficients of one horizontal face at a cell with the given flags
 // (cr = u dt / h, rounded by the caller as __fmul_rn(__fmul_rn(u, dt), 1/h)).
 __device__ __forceinline__ void hface(Face &f, bool wet, bool eb, bool quick, bool ult,
-                                      float cr, float U, float K, const Face2 &m) {
+                                      float cr, double U, float K, const Face2 &m) {
   if (!wet) {  // a ghost: the face carries nothing
     face_zero(f);
     return;
@@ -146,17 +146,18 @@ __device__ __forceinline__ void hface(Face &f, bool wet, bool eb, bool quick, bo
 
 // Vertical face at the bottom of a cell from the thicknesses of the two cells
 // below it (dzm2, dzm1), the cell (dz0) and the one above (dzp1; the
-// surface-layer cell maps onto itself, top != 0), and w * dtu; IEEE
-// divisions, so the cell below folds its top face to the same bits.
+// surface-layer cell maps onto itself, top != 0), and w * dtu (wv in FP32
+// for the Courant number, U in FP64 for the flux); IEEE divisions, so the
+// cell below folds its top face to the same bits.
 __device__ __forceinline__ void zface(Face &f, bool quick, bool ult, float dzm2, float dzm1,
-                                      float dz0, float dzp1, bool top, float wv) {
+                                      float dz0, float dzp1, bool top, float wv, double U) {
   const float w9m = __fmul_rn(0.5f, __fadd_rn(dzm1, dzm2));
   const float w90 = __fmul_rn(0.5f, __fadd_rn(dz0, dzm1));
   const float w9p = top ? w90 : __fmul_rn(0.5f, __fadd_rn(dzp1, dz0));
   const float cz = __fdiv_rn(wv, w90);
   const float db = __fdiv_rn(2.f, __fadd_rn(w9m, w90)), df = __fdiv_rn(2.f, __fadd_rn(w90, w9p));
   set_face(f, quick, cz, __fdiv_rn(dzm1, __fadd_rn(dzm1, dz0)), __fmul_rn(db, w9m),
-           __fmul_rn(db, w90), __fmul_rn(df, w90), __fmul_rn(df, w9p), wv, ult, 0.f);
+           __fmul_rn(db, w90), __fmul_rn(df, w90), __fmul_rn(df, w9p), U, ult, 0.f);
 }
 
 }  // namespace f32
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
                                                      const float *__restrict__ tri,
                                                      float *__restrict__ tro,
                                                      float *__restrict__ rso,
-                                                     float *__restrict__ fzs, int any_hd) {
+                                                     double *__restrict__ fzs, int any_hd) {
   using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ int sTr[kMaxTracers], sTf[kMaxTracers];
@@ -271,11 +272,13 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       const float dzm1 = W.dz32[nzv.x], dzm2 = W.dz32[nzv.y];
       const bool top = (nzv.z == c);
       const float dzp1 = W.dz32[nzv.z];
-      zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu));
+      zface(fzb, QUICK, ULT, dzm2, dzm1, dz0, dzp1, top, __fmul_rn(F3.w[c], fdtu),
+            __dmul_rn(F3.w64[c], dtu));
       if (k < ks) {  // the bottom face of the cell above
         const bool top1 = (nzv.w == nzv.z);
         const float dzp2 = W.dz32[nzv.w];
-        zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, __fmul_rn(F3.w[nzv.z], fdtu));
+        zface(fzt, QUICK, ULT, dzm1, dz0, dzp1, dzp2, top1, __fmul_rn(F3.w[nzv.z], fdtu),
+              __dmul_rn(F3.w64[nzv.z], dtu));
       }
     }
     idz = 1.0 / W.dz[c];  // the FP64 thickness: the update conserves mass to FP64 round-off
@@ -338,20 +341,20 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         const float tp1 = v[7 * kAdv32Block], tp2 = v[8 * kAdv32Block];
         const float txm1 = v[9 * kAdv32Block], txm2 = v[10 * kAdv32Block];
         const float txp1 = v[11 * kAdv32Block], txp2 = v[12 * kAdv32Block];
-        const float Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
-        const float Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
-        const float Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
-        const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
-        const float Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
-        const float Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.f;
+        const double Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
+        const double Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
+        const double Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
+        const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
+        const double Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
+        const double Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.0;
         const int n = sTr[s];
         if (!on || n >= ntc) continue;
         // FP64 flux divergence (tracers.c:888-892)
-        const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+        const double dtr = ((Fxe - Fxw) + (Fyn - Fys)) * dtu;
         double a = dtr;
         if (zt) {
-          const float Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
-          a = (double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz;
+          const double Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
+          a = (double)t0 - (dtr * ia + (Fzt - Fzb)) * idz;
         } else if (zf) {
           fzs[(size_t)n * G.ncol + col] = Fzb;
         }
@@ -394,7 +397,7 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       const float t0 = v[u][0];
       const float u1v = __shfl_up_sync(FULL, t0, 1), u2v = __shfl_up_sync(FULL, t0, 2);
       const float d1v = __shfl_down_sync(FULL, t0, 1), d2v = __shfl_down_sync(FULL, t0, 2);
-      float Fxw = 0.f, Fxe = 0.f, Fys = 0.f, Fyn = 0.f, Fzb = 0.f, Fzt = 0.f;
+      double Fxw = 0.0, Fxe = 0.0, Fys = 0.0, Fyn = 0.0, Fzb = 0.0, Fzt = 0.0;
       if (on && (adv || hd)) {
         const float txm1 = sxm1 ? u1v : v[u][9];
         const float txm2 = sxm2 ? u2v : v[u][10];
@@ -413,14 +416,14 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
           if (zt) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, v[u][8]);
         }
       }
-      const float Fnext = __shfl_down_sync(FULL, Fxw, 1);
+      const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
       if (!on || nn[u] >= ntc) continue;
       if (sxp1) Fxe = Fnext;
       // FP64 flux divergence (tracers.c:888-892)
-      const double dtr = (((double)Fxe - (double)Fxw) + ((double)Fyn - (double)Fys)) * dtu;
+      const double dtr = ((Fxe - Fxw) + (Fyn - Fys)) * dtu;
       double a = dtr;
       if (zt)
-        a = (double)t0 - (dtr * ia + ((double)Fzt - (double)Fzb)) * idz;
+        a = (double)t0 - (dtr * ia + (Fzt - Fzb)) * idz;
       else if (k == ks)
         fzs[(size_t)nn[u] * G.ncol + col] = Fzb;
       const float val = (float)a;
@@ -440,24 +443,28 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
 // divergence of the surface cell and the cells above it, and the surface
 // cell's bottom-face flux.
 struct ColSums {
-  double m, dv;
-  float fzb;
+  double m, dv, fzb;
 };
 
 // A0, S0: the column's values and Thomas storage from its bottom layer up, row
 // stride sa; an advected tracer (tbdy) holds its advected values below the
 // surface, any other tracer every layer's old value (A0 is overwritten, so is
 // S0).  L0, C0, D0: LU factors, cells and FP64 thicknesses, row stride 32.
+// RES: an advected tracer's A0 holds every layer's stored advection result
+// and S0 its rounding residual (k_vd32), and the column sums cs.m and cs.dv
+// are taken from them; else they come in cs (k_step32).
 // carry: [ntr][ncol] (null: none).  Adds the values it flags to nwarn and
-// sets bad for a NaN among what it stores.
-template <bool LAST>
+// sets bad for a NaN among what it stores.  The mass bookkeeping sums are
+// plain FP64 sums of at most nz terms: their rounding (a few 1e-16 of the
+// column mass, of either sign) is what the carry may miss per step.
+template <bool LAST, bool RES>
 __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const Work &W,
                                               const Opt &O, const TrSet &T, const SubStep &ss,
                                               const TileCol &tc, int col, int n, bool tbdy,
                                               bool adv, bool vdf, float *A0, float *S0, int sa,
                                               const float4 *L0, const int *C0, const double *D0,
                                               const float *tr, float *to, double area, double ia,
-                                              double H, double idt, const ColSums &cs,
+                                              double H, double idt, ColSums cs,
                                               double *carry, bool steady, long long &nwarn,
                                               bool &bad) {
   const ColInfo &ci = tc.ci;
@@ -472,17 +479,15 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   const double carry_in = (carry && steady) ? carry[(size_t)n * G.ncol + col] : 0.0;
   // the carry goes back as a uniform shift of the column's values
   const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
-  // FP64 mass bookkeeping per unit area: what the step computed (mx*) and
-  // what is stored (ms*), compensated sums
-  double mxs = 0.0, mxc = 0.0, mss = 0.0, msc = 0.0;
-  if (H > 0.0) f32::neumaier_add(mxs, mxc, carry_in * ia);
+  // FP64 mass bookkeeping per unit area: what the step computed (mxs) and
+  // what is stored (mss)
+  double mxs = H > 0.0 ? carry_in * ia : 0.0, mss = 0.0;
   long long nw = 0;
   double vs = ts_old;  // the surface value
   if (!tbdy) {
-    for (int j = 0; j < nk; ++j)
-      f32::neumaier_add(mxs, mxc, __dmul_rn((double)A0[j * sa], D0[j * 32]));
+    for (int j = 0; j < nk; ++j) mxs += (double)A0[j * sa] * D0[j * 32];
     vs = (double)A0[nk * sa];
-    f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+    mxs += vs * dzs;
     for (int j = nk + 1; j < nz - kb; ++j) {
       to[C0[j * 32]] = A0[j * sa];
       bad |= isnan(A0[j * sa]);
@@ -492,11 +497,19 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     // surface; a < mn and a > mx of a float a, exactly, as float compares
     const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
     const bool clip = mn <= kClipEps;
-    f32::neumaier_add(mxs, mxc, cs.m);
+    if (RES) {
+      // the FP64 advected values are stored + residual
+      double m = 0.0, dv = 0.0;
+      for (int j = 0; j < nk; ++j) m += ((double)A0[j * sa] + (double)S0[j * sa]) * D0[j * 32];
+      for (int j = nk; j < nz - kb; ++j) dv += (double)A0[j * sa] + (double)S0[j * sa];
+      cs.m = m;
+      cs.dv = dv;
+    }
+    mxs += cs.m;
     for (int j = 0; j < nk; ++j) {
       float a = A0[j * sa];
       if (clip && a < mn_up) {
-        f32::neumaier_add(mxs, mxc, __dmul_rn((double)mnf - (double)a, D0[j * 32]));
+        mxs += ((double)mnf - (double)a) * D0[j * 32];
         a = mnf;
       }
       nw += (a < mn_up || a > mx_dn);
@@ -510,7 +523,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       const double osub = ss.first ? oe : oe + ss.osub_f * (eta - oe);
       const double sub = oe + ss.subeta_f * (eta - oe);
       double ssum = 0.0, scomp = 0.0;
-      f32::neumaier_add(ssum, scomp, __dmul_rn((double)cs.fzb, area));
+      f32::neumaier_add(ssum, scomp, __dmul_rn(cs.fzb, area));
       f32::neumaier_add(ssum, scomp, __dmul_rn(__dmul_rn(ts_old, area), osub - wb));
       f32::neumaier_add(ssum, scomp, -cs.dv);
       const double dzn = sub - wb;
@@ -523,7 +536,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     if (mn <= kClipEps && vs < mn) vs = mn;
     if (vs < mn || vs > mx) ++nw;
     bad |= isnan(vs);
-    f32::neumaier_add(mxs, mxc, __dmul_rn(vs, dzs));
+    mxs += vs * dzs;
     const float vs32 = (float)vs;
     for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
   }
@@ -533,14 +546,14 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       const float fin = (float)((double)A0[j * sa] + dl);
       to[C0[j * 32]] = fin;
       bad |= isnan(fin);
-      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
+      mss += (double)fin * D0[j * 32];
     }
     const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
     const float fin = (vdf && single) ? (float)(vs + dl + F.dt * (0.0 - 0.0) / h)
                                       : (float)(vs + dl);
     to[ci.s] = fin;
     bad |= isnan(fin);
-    f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+    mss += (double)fin * dzs;
   } else {
     A0[nk * sa] = (float)vs;
     // FP32 forward sweep
@@ -594,17 +607,17 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       const float fin = (float)((double)S0[nk * sa] + (double)d);
       to[C0[nk * 32]] = fin;
       bad |= isnan(fin);
-      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, dzs));
+      mss += (double)fin * dzs;
     }
     for (int j = nk - 1; j >= 0; --j) {
       d = A0[j * sa] - L0[(j + 1) * 32].w * d;
       const float fin = (float)((double)S0[j * sa] + (double)d);
       to[C0[j * 32]] = fin;
       bad |= isnan(fin);
-      f32::neumaier_add(mss, msc, __dmul_rn((double)fin, D0[j * 32]));
+      mss += (double)fin * D0[j * 32];
     }
   }
-  if (carry && steady) carry[(size_t)n * G.ncol + col] = ((mxs + mxc) - (mss + msc)) * area;
+  if (carry && steady) carry[(size_t)n * G.ncol + col] = (mxs - mss) * area;
   nwarn += nw;
 }
 
@@ -626,7 +639,7 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
                                               float *__restrict__ tro,
                                               const float *__restrict__ rsi,
                                               double *__restrict__ carry,
-                                              const float *__restrict__ fzs, int nw,
+                                              const double *__restrict__ fzs, int nw,
                                               int nchunk, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
   // the arrays hold layers kbase .. nz-1 (every column of this launch's
@@ -699,21 +712,12 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   const int nk = ks - kb;
   double H = 0.0;
   for (int j = 0; j <= nk; ++j) H += D0[j * 32];
-  ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.f};
+  const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
   cp_async_wait<0>();
-  if (tbdy) {
-    // the FP64 advected values are stored + residual
-    double m = 0.0, mc = 0.0, dv = 0.0;
-    for (int j = 0; j < nk; ++j)
-      f32::neumaier_add(m, mc, __dmul_rn((double)A0[j * sa] + (double)S0[j * sa], D0[j * 32]));
-    for (int j = nk; j < nz - kb; ++j) dv += (double)A0[j * sa] + (double)S0[j * sa];
-    cs.m = m + mc;
-    cs.dv = dv;
-  }
   long long nwarn = 0;
   bool bad = false;  // a NaN among the values this thread stores
-  column_finish<LAST>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0, D0, tr,
-                      to, area, ia, H, 1.0 / F.dt, cs, carry, steady, nwarn, bad);
+  column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
+                            D0, tr, to, area, ia, H, 1.0 / F.dt, cs, carry, steady, nwarn, bad);
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
 }
