@@ -80,6 +80,13 @@ struct shoc_tr_gpu {
   int *colown = nullptr;              // columns counted in the sub-step minimum (null: all)
   double dmin_set = 0.0;              // sub-step minimum imposed by the caller (0: own)
   int nhalo_send = 0, nhalo_recv = 0;
+  struct Preamble {                   // transport-mode flow preamble (k_faces, k_wvel)
+    bool on = false, ok = false;      // enabled; the window's face lists support it
+    int n1 = 0, n2 = 0;               // e1 and e2 face columns
+    int2 *fc = nullptr;               // [n1 + n2] {2D cell, bottom face cell}
+    double *bz = nullptr;             // [n1 + n2] the faces' floors (botzu1 / botzu2)
+    double *detadt = nullptr;         // [S2] surface velocity (wtop)
+  } pre;
   Fused fu{};                         // FP32-mixed: the columns' mass carry; k_step32's tiles
   bool fused = false;                 // FP32-mixed sub-steps run k_step32
   size_t fused_bytes = 0;             // its dynamic shared memory
@@ -470,6 +477,118 @@ __device__ __forceinline__ void neumaier(double &s, double &comp, double v) {
   double u = s + v;
   comp += (fabs(s) >= fabs(v)) ? (s - u) + v : (v - u) + s;
   s = u;
+}
+
+// ---------------------------------------------------------------------------
+// Transport-mode flow preamble (transport_step, model/hd/tracers/
+// transport.c:436-462): what SHOC's transport mode computes from the
+// velocities and the surface before the tracer step, on the device.  A z-level
+// window, linear free surface (wtop = detadt), no point sources (waterss = 0),
+// conserve = CONS_W, mdx = mdy = 1 and no one-cell-deep face list (the
+// momentum step builds that list; transport mode does not run it).
+
+// set_dz_at_u1 / set_dz_at_u2 (model/hd/momentum/vel3d.c:720-853, :2718-2850,
+// z coordinates) and set_flux_3d (vel3d.c:4041-4175, VEL3D) of one face
+// column per thread, e1 faces first: the face's surface is the higher of the
+// two elevations beside it (at least the face's floor botzu), its surface cell
+// the first cell down from the surface layer whose bottom is at or below it,
+// its thicknesses from there to the bottom face cell (the layers above copy
+// the surface cell's), the volume flux u dzu h2au1 (h1au2) at and below the
+// surface and zero above.  The arrays start zeroed (the reference's memsets).
+// fc: {2D cell, bottom face cell} per face column, bz: its floor.
+__global__ void k_faces(Geo G, Flow F, int n1, int n, const int2 *fc, const double *bz,
+                        double *dzu1, double *dzu2, double *f1, double *f2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const bool e1 = i < n1;
+  const int c2 = fc[i].x, cb = fc[i].y;
+  const int nb = e1 ? G.xm1[c2] : G.ym1[c2];
+  const double *u = e1 ? F.u1 : F.u2;
+  const double hf = e1 ? G.h2au1[c2] : G.h1au2[c2];
+  double *dzu = e1 ? dzu1 : dzu2, *flux = e1 ? f1 : f2;
+  const double floor = bz[i];
+  double top = F.eta[c2] > F.eta[nb] ? F.eta[c2] : F.eta[nb];
+  top = top > floor ? top : floor;
+  int c = c2, zm = G.zm1[c];
+  while (c != zm && G.gridz[c] > top) {
+    c = zm;
+    zm = G.zm1[c];
+  }
+  const int sur = c;
+  double t = top;
+  while (c != cb) {
+    const double bot = G.gridz[c];
+    const double d = t - bot;
+    dzu[c] = d;
+    flux[c] = u[c] * d * hf;
+    t = bot;
+    c = G.zm1[c];
+  }
+  {
+    const double d = t - floor;
+    dzu[cb] = d;
+    flux[cb] = u[cb] * d * hf;
+  }
+  const double ds = dzu[sur];
+  c = sur;
+  while (c != c2) {
+    c = G.zp1[c];
+    dzu[c] = ds;
+  }
+}
+
+// vel_w_update (vel3d.c:4609-4760, z coordinates, CONS_W) of one water column
+// per thread, before k_set_dz: the column's old surface cell (the previous
+// step's new one) and new surface cell, and whether the column is processed,
+// as set_dz decides them (tracers.c:5739-5800); then w from continuity from
+// the bottom (wbot = 0) up to the old surface, wtop = detadt in the cells the
+// surface moved through, and set_w_dry (vel3d.c:5116-5135): wtop in every
+// cell above the new surface cell, in every column.  w starts zeroed (the
+// reference's memset).
+__global__ void k_wvel(Geo G, Flow F, Work W, Opt O, const double *detadt, double *w) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= G.ncol) return;
+  const int top = G.col_top[col], bot = G.col_bot[col];
+  const int sur = W.nsur_t[col];
+  int nsur = top, zm = G.zm1[nsur];
+  const double etat = F.eta[top];
+  while (nsur != zm && G.gridz[nsur] >= etat) {
+    nsur = zm;
+    zm = G.zm1[nsur];
+  }
+  const int s = sur > nsur ? sur : nsur;
+  const int c2 = G.m2d[s];
+  const double tz = F.eta[c2] < F.oldeta[c2] ? F.eta[c2] : F.oldeta[c2];
+  const double bz = SHOC_TR_DRY_FRAC * O.hmin + G.botz[c2];
+  if (tz > bz && s != G.zm1[s]) {
+    const int cs = G.m2d[bot];
+    const double area = G.cellarea[cs];
+    int c = bot;
+    const double wb = 0.0;  // wbot (vel_w_bounds, z coordinates)
+    w[c] = wb;
+    double fcbot = wb * area;
+    while (c > sur) {
+      const int xp = G.xp1[c], yp = G.yp1[c], zp = G.zp1[c];
+      const double fctop = fcbot + F.u1flux3d[c] - F.u1flux3d[xp] + F.u2flux3d[c] -
+                           F.u2flux3d[yp] + 0.0;  // + waterss
+      w[zp] = fctop / area;
+      fcbot = fctop;
+      c = zp;
+    }
+    while (c > nsur) {
+      const int zp = G.zp1[c];
+      w[zp] = detadt[cs];  // wtop (vel_w_bounds, linear surface)
+      c = zp;
+    }
+  }
+  // set_w_dry
+  const int cs = G.m2d[nsur];
+  int c = nsur, zp = G.zp1[c];
+  while (c != zp) {
+    w[zp] = detadt[cs];
+    c = zp;
+    zp = G.zp1[c];
+  }
 }
 
 __global__ void k_to_f32(const double *a, float *b, size_t n) {
@@ -961,6 +1080,39 @@ int check_geom(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr) {
 // ---------------------------------------------------------------------------
 // C-ABI
 
+// The e1 (e2) face columns of a window as SHOC lists them in w2_e1, bot_e1
+// and botzu1 (w2_e2, bot_e2, botzu2): the surface-layer cells of w3_e1, each
+// column's deepest w3_e1 cell (the faces are wet from the surface layer
+// down to it) and the higher of the floors on the two sides of the face
+// (hd_init.c:1443).  bm: the backward map (xm1 or ym1).  False where w3_e1 is
+// not one run from the surface layer down in every face column.
+bool face_columns(const shoc_tr_geom *g, int ne, const int *w3, const int *bm,
+                  std::vector<int2> &fc, std::vector<double> &bz) {
+  const int S = g->sgsiz;
+  if (ne > 0 && !w3) return false;
+  std::vector<uint8_t> in(S, 0);
+  for (int i = 1; i <= ne; i++) {
+    const int c = w3[i];
+    if (c <= 0 || c >= S || in[c]) return false;
+    in[c] = 1;
+  }
+  long long covered = 0;
+  for (int i = 1; i <= ne; i++) {
+    const int c2 = w3[i];
+    if (g->zp1[c2] != c2) continue;  // below the surface layer
+    int c = c2, cb = c2;
+    while (g->zm1[c] != c && in[c]) {
+      cb = c;
+      covered++;
+      c = g->zm1[c];
+    }
+    fc.push_back(make_int2(c2, cb));
+    const double a = g->botz[bm[c2]], b = g->botz[c2];
+    bz.push_back(a > b ? a : b);
+  }
+  return covered == ne;
+}
+
 extern "C" {
 
 const char *shoc_tr_gpu_strerror(int st) {
@@ -1231,6 +1383,20 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   }
   TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
+  {  // face columns of the transport-mode preamble
+    std::vector<int2> fc;
+    std::vector<double> bz;
+    bool ok = face_columns(g, g->v3_e1, g->w3_e1, g->xm1, fc, bz);
+    const int n1 = (int)fc.size();
+    ok = ok && face_columns(g, g->v3_e2, g->w3_e2, g->ym1, fc, bz);
+    h->pre.ok = ok;
+    if (ok && !fc.empty()) {
+      h->pre.n1 = n1;
+      h->pre.n2 = (int)fc.size() - n1;
+      TRY(dupload(h, &h->pre.fc, fc.data(), fc.size()));
+      TRY(dupload(h, &h->pre.bz, bz.data(), bz.size()));
+    }
+  }
   if (f32p) {
     // the fused sub-step kernel (SHOC_TR_GPU_KERNELS=fused; the two-kernel
     // sub-step is the default, measured faster): every advected tracer's
@@ -1365,13 +1531,47 @@ void launch_lateral(shoc_tr_gpu *h, int cur, const TrSet &T) {
   h->launches++;
 }
 
-// Step set-up: counters, lateral boundaries (when `lateral`) and k_set_dz.
-// k_set_dz reads no tracer, so the lateral copies may follow it instead.
+// The transport-mode flow preamble: dzu1, dzu2, u1flux3d, u2flux3d and w
+// from the velocities, the surface and detadt (k_faces, k_wvel), and the
+// FP32-mixed path's copies of what changed.
+int launch_preamble(shoc_tr_gpu *h) {
+  cudaStream_t st = h->stream;
+  const size_t S = (size_t)h->S;
+  double *f1 = (double *)h->F.u1flux3d, *f2 = (double *)h->F.u2flux3d, *w = (double *)h->F.w;
+  double *d1 = (double *)h->F.dzu1, *d2 = (double *)h->F.dzu2;
+  for (double *p : {f1, f2, w, d1, d2}) CK(cudaMemsetAsync(p, 0, S * sizeof(double), st));
+  const int n = h->pre.n1 + h->pre.n2;
+  if (n > 0) {
+    k_faces<<<(n + 127) / 128, 128, 0, st>>>(h->G, h->F, h->pre.n1, n, h->pre.fc, h->pre.bz, d1,
+                                             d2, f1, f2);
+    h->launches++;
+  }
+  k_wvel<<<(h->ncol + 127) / 128, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->pre.detadt, w);
+  h->launches++;
+  if (h->esize == sizeof(float)) {
+    k_to_f32<<<592, 256, 0, st>>>(h->F.w, (float *)h->F3.w, S);
+    h->launches++;
+    if (h->any_hdiff) {
+      k_khfac<<<592, 256, 0, st>>>(h->G, h->F, (float *)h->F3.khx, (float *)h->F3.khy);
+      h->launches++;
+    }
+  }
+  CK(cudaGetLastError());
+  return 0;
+}
+
+// Step set-up: counters, lateral boundaries (when `lateral`), the flow
+// preamble (when on) and k_set_dz.  k_set_dz reads no tracer, so the lateral
+// copies may follow it instead.
 int launch_part_a(shoc_tr_gpu *h, int cur, bool lateral = true) {
   cudaStream_t st = h->stream;
   k_reset<<<1, 32, 0, st>>>(h->W, h->d_counts);
   h->launches++;
   if (lateral) launch_lateral(h, cur, h->T);
+  if (h->pre.on) {
+    const int rc = launch_preamble(h);
+    if (rc) return rc;
+  }
   int nb = (h->ncol + 127) / 128;
   k_set_dz<<<nb, 128, 0, st>>>(h->G, h->F, h->W, h->O, h->tl, h->any_vdiff ? 1 : 0, h->d_counts,
                                h->staged ? 1 : 0, h->esize == sizeof(float) ? 1 : 0, h->colown,
@@ -1834,22 +2034,33 @@ int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
   DeviceScope dev_(h->device);
   const size_t S = (size_t)h->S * sizeof(double), S2 = (size_t)h->S2 * sizeof(double);
   cudaStream_t s = h->stream;
+  // with the flow preamble on, w, u1flux3d, u2flux3d, dzu1 and dzu2 are
+  // computed by every step and not read from the state (they may be null)
+  const bool pre = h->pre.on;
   const struct {
     const double *dst;
     const double *src;
     size_t n;
-  } cp[] = {{h->F.u1, st->u1, S},         {h->F.u2, st->u2, S},
-            {h->F.w, st->w, S},           {h->F.u1flux3d, st->u1flux3d, S},
-            {h->F.u2flux3d, st->u2flux3d, S}, {h->F.Kz, st->Kz, S},
-            {h->F.eta, st->eta, S2},      {h->F.oldeta, st->oldeta, S2}};
+    bool need;
+  } cp[] = {{h->F.u1, st->u1, S, true},
+            {h->F.u2, st->u2, S, true},
+            {h->F.w, st->w, S, !pre},
+            {h->F.u1flux3d, st->u1flux3d, S, !pre},
+            {h->F.u2flux3d, st->u2flux3d, S, !pre},
+            {h->F.Kz, st->Kz, S, true},
+            {h->F.eta, st->eta, S2, true},
+            {h->F.oldeta, st->oldeta, S2, true}};
   for (auto &x : cp) {
+    if (!x.need) continue;
     if (!x.src) return SHOC_TR_EARG;
     CK(cudaMemcpyAsync((void *)x.dst, x.src, x.n, cudaMemcpyHostToDevice, s));
   }
   if (h->any_hdiff) {
-    if (!st->dzu1 || !st->dzu2 || !st->u1kh || !st->u2kh) return SHOC_TR_EARG;
-    CK(cudaMemcpyAsync((void *)h->F.dzu1, st->dzu1, S, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync((void *)h->F.dzu2, st->dzu2, S, cudaMemcpyHostToDevice, s));
+    if ((!pre && (!st->dzu1 || !st->dzu2)) || !st->u1kh || !st->u2kh) return SHOC_TR_EARG;
+    if (!pre) {
+      CK(cudaMemcpyAsync((void *)h->F.dzu1, st->dzu1, S, cudaMemcpyHostToDevice, s));
+      CK(cudaMemcpyAsync((void *)h->F.dzu2, st->dzu2, S, cudaMemcpyHostToDevice, s));
+    }
     CK(cudaMemcpyAsync((void *)h->F.u1kh, st->u1kh, S, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync((void *)h->F.u2kh, st->u2kh, S, cudaMemcpyHostToDevice, s));
   }
@@ -1857,9 +2068,12 @@ int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st) {
     const size_t n = (size_t)h->S;
     k_to_f32<<<592, 256, 0, s>>>(h->F.u1, (float *)h->F3.u1, n);
     k_to_f32<<<592, 256, 0, s>>>(h->F.u2, (float *)h->F3.u2, n);
-    k_to_f32<<<592, 256, 0, s>>>(h->F.w, (float *)h->F3.w, n);
-    h->launches += 3;
-    if (h->any_hdiff) {
+    h->launches += 2;
+    if (!pre) {
+      k_to_f32<<<592, 256, 0, s>>>(h->F.w, (float *)h->F3.w, n);
+      h->launches++;
+    }
+    if (h->any_hdiff && !pre) {
       k_khfac<<<592, 256, 0, s>>>(h->G, h->F, (float *)h->F3.khx, (float *)h->F3.khy);
       h->launches++;
     }
@@ -1896,6 +2110,58 @@ int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t) {
                        cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   return 0;
+}
+
+int shoc_tr_gpu_set_preamble(shoc_tr_gpu *h, int on) {
+  if (!h) return SHOC_TR_EARG;
+  if (on && !h->pre.ok) return SHOC_TR_EUNSUPPORTED;
+  DeviceScope dev_(h->device);
+  if (on) {
+    int rc = 0;
+    if (!rc && !h->F.dzu1) rc = dupload<double>(h, (double **)&h->F.dzu1, nullptr, (size_t)h->S);
+    if (!rc && !h->F.dzu2) rc = dupload<double>(h, (double **)&h->F.dzu2, nullptr, (size_t)h->S);
+    if (!rc && !h->pre.detadt) rc = dupload<double>(h, &h->pre.detadt, nullptr, (size_t)h->S2);
+    if (rc) return rc;
+  }
+  if (h->pre.on != (on != 0)) {
+    h->pre.on = on != 0;
+    for (int i = 0; i < 2; i++)  // the captured steps hold the old part A
+      if (h->graph[i]) {
+        cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+      }
+    h->probe_left = std::max(h->probe_left, 1);  // w, and so the sub-steps, change
+  }
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_set_detadt(shoc_tr_gpu *h, const double *detadt) {
+  if (!h || !detadt) return SHOC_TR_EARG;
+  if (!h->pre.detadt) return SHOC_TR_EARG;  // the preamble was never enabled
+  DeviceScope dev_(h->device);
+  CK(cudaMemcpyAsync(h->pre.detadt, detadt, (size_t)h->S2 * sizeof(double),
+                     cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_get_flow(shoc_tr_gpu *h, double *u1flux3d, double *u2flux3d, double *w,
+                         double *dzu1, double *dzu2) {
+  if (!h) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  const size_t S = (size_t)h->S * sizeof(double);
+  const struct {
+    double *dst;
+    const double *src;
+  } cp[] = {{u1flux3d, h->F.u1flux3d}, {u2flux3d, h->F.u2flux3d}, {w, h->F.w},
+            {dzu1, h->F.dzu1}, {dzu2, h->F.dzu2}};
+  for (auto &x : cp) {
+    if (!x.dst) continue;
+    if (!x.src) return SHOC_TR_EARG;  // dzu1 / dzu2: neither uploaded nor computed
+    CK(cudaMemcpyAsync(x.dst, x.src, S, cudaMemcpyDeviceToHost, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  return SHOC_TR_OK;
 }
 
 // ---- checkpoint / resume: a versioned raw image of the resident state ----

@@ -29,7 +29,8 @@ EXPORTS = (
     "shoc_tr_gpu_substep_min", "shoc_tr_gpu_set_substep_min", "shoc_tr_gpu_host_register", "shoc_tr_gpu_host_unregister",
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
-    "shoc_tr_gpu_strerror",
+    "shoc_tr_gpu_strerror", "shoc_tr_gpu_set_preamble", "shoc_tr_gpu_set_detadt",
+    "shoc_tr_gpu_get_flow",
 )
 
 _lib = None
@@ -84,6 +85,9 @@ def lib(path=None):
                                                C.POINTER(C.c_int)]
     L.shoc_tr_gpu_launch_count.argtypes = [H]
     L.shoc_tr_gpu_launch_count.restype = C.c_longlong
+    L.shoc_tr_gpu_set_preamble.argtypes = [H, C.c_int]
+    L.shoc_tr_gpu_set_detadt.argtypes = [H, _abi.DP]
+    L.shoc_tr_gpu_get_flow.argtypes = [H] + [_abi.DP] * 5
     L.shoc_tr_gpu_strerror.argtypes = [C.c_int]
     L.shoc_tr_gpu_strerror.restype = C.c_char_p
     for name in EXPORTS:
@@ -197,6 +201,29 @@ class TracerStep:
 
     def run(self, nsteps):
         _check("run", self.L.shoc_tr_gpu_run(self.h, int(nsteps)))
+
+    def set_preamble(self, on=True, detadt=None):
+        """Transport-mode flow preamble on the device (shoc_tr_gpu_set_preamble),
+        with the surface velocity detadt [sgsizS] (default 0)."""
+        _check("set_preamble", self.L.shoc_tr_gpu_set_preamble(self.h, 1 if on else 0))
+        if on:
+            d = np.zeros(self.case.win.sgsizS) if detadt is None else detadt
+            d = np.ascontiguousarray(d, np.float64)
+            _check("set_detadt", self.L.shoc_tr_gpu_set_detadt(self.h, _abi.dptr(d)))
+
+    def get_flow(self):
+        """dict of the device's u1flux3d, u2flux3d, w, dzu1, dzu2 [sgsiz]
+        (dzu1 / dzu2 only where the handle holds them)."""
+        S = self.case.win.sgsiz
+        out = {k: np.zeros(S) for k in ("u1flux3d", "u2flux3d", "w")}
+        _check("get_flow", self.L.shoc_tr_gpu_get_flow(
+            self.h, _abi.dptr(out["u1flux3d"]), _abi.dptr(out["u2flux3d"]), _abi.dptr(out["w"]),
+            None, None))
+        d1, d2 = np.zeros(S), np.zeros(S)
+        if self.L.shoc_tr_gpu_get_flow(self.h, None, None, None, _abi.dptr(d1),
+                                       _abi.dptr(d2)) == 0:
+            out["dzu1"], out["dzu2"] = d1, d2
+        return out
 
     def sync(self):
         d = _abi.Diag()

@@ -92,6 +92,25 @@ int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc);
  * sur_t / nsur_t. */
 int shoc_tr_gpu_set_flow(shoc_tr_gpu *h, const shoc_tr_state *st);
 int shoc_tr_gpu_get_surface(shoc_tr_gpu *h, int *sur_t, int *nsur_t);
+/* Transport-mode flow preamble.  With on != 0, every step (shoc_tr_gpu_run
+ * and shoc_tr_gpu_step) first computes on the device what SHOC's transport
+ * mode computes before the tracer step (transport_step, model/hd/tracers/
+ * transport.c:436-462): dzu1 / dzu2 (set_dz_at_u1 / set_dz_at_u2, model/hd/
+ * momentum/vel3d.c:720, :2718), u1flux3d / u2flux3d (set_flux_3d,
+ * vel3d.c:4041, VEL3D) from the state's u1, u2 and eta, and w from
+ * continuity (vel_w_update, vel3d.c:4609, CONS_W) with wtop = detadt.  Then
+ * the state's w, u1flux3d, u2flux3d, dzu1 and dzu2 are neither read nor
+ * needed (they may be NULL).  Covers z-level windows without open
+ * boundaries, a linear free surface, no point sources of water and
+ * mdx = mdy = 1; SHOC_TR_EUNSUPPORTED where the window's w3_e1 / w3_e2 are
+ * not one run of faces from the surface layer down per face column.
+ * set_detadt copies the surface velocity detadt [sgsizS] (used by every
+ * following step; call it after set_preamble(h, 1)); get_flow copies the
+ * device's current fields back (any pointer may be NULL). */
+int shoc_tr_gpu_set_preamble(shoc_tr_gpu *h, int on);
+int shoc_tr_gpu_set_detadt(shoc_tr_gpu *h, const double *detadt);
+int shoc_tr_gpu_get_flow(shoc_tr_gpu *h, double *u1flux3d, double *u2flux3d, double *w,
+                         double *dzu1, double *dzu2);
 /* Enqueues nsteps steps on the handle's stream (CUDA-graph replays once the
  * sub-step schedule is known).  May synchronise once after set_flow to learn
  * the sub-step count. */

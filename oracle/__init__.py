@@ -8,6 +8,9 @@ against or timed beside -- never as part of the product path.
   run_ref(case, nsteps, ...)     the reference's own tracers.c, compiled
                                  unmodified (oracle/_ref, built by
                                  oracle/build.py where the reference exists)
+  ref_preamble(case, detadt)     the reference's transport-mode flow preamble
+                                 (vel3d.c compiled unmodified)
+  preamble(case, detadt)         its restatement (oracle/flow_preamble.py)
 """
 import ctypes as C
 import os
@@ -24,6 +27,18 @@ def _load(name):
     if name in _libs:
         return _libs[name]
     from . import build
+    if name == "ref_vel":
+        path = os.path.join(HERE, "_ref", "libshoc_ref_vel.so")
+        if not os.path.exists(path):
+            build.ref_vel_lib()
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        L.ref_preamble.argtypes = [C.POINTER(_abi.Geom), C.POINTER(_abi.State),
+                                   C.POINTER(_abi.Opts)] + [_abi.DP] * 6
+        L.ref_preamble.restype = C.c_int
+        _libs[name] = L
+        return L
     if name == "oracle":
         path = build.oracle_lib()
         L = C.CDLL(path)
@@ -128,6 +143,38 @@ def ref_vdiff_cols(case, var, dzcell, Cd, Cm1, Cp1, fb, ft, scale, dt, Splus=Non
     P = _abi.dptr
     return _ref_call("ref_vdiff_cols", case, sur, nsur, P(var), P(dzcell), P(Cd), P(Cm1),
                      P(Cp1), P(fb), P(ft), P(Splus), P(Sminus), P(scale), C.c_double(dt))
+
+
+def ref_preamble(case, detadt, sur=None, nsur=None):
+    """The reference's set_dz_at_u1 / _u2, set_flux_3d (VEL3D), set_dz and
+    vel_w_update on case's window, velocities and surface (transport.c:
+    436-462), wtop = detadt [sgsizS]; returns dict of dzu1, dzu2, u1flux3d,
+    u2flux3d, w (each [sgsiz])."""
+    L = _load("ref_vel")
+    if L is None:
+        raise FileNotFoundError("reference build oracle/_ref/libshoc_ref_vel.so not available")
+    sur = case.sur_t.copy() if sur is None else sur
+    nsur = case.nsur_t.copy() if nsur is None else nsur
+    keep = []
+    tr = case.tr.copy()
+    st = case.make_state(tr, sur, nsur, keep)
+    op = case.make_opts(keep)
+    S = case.win.sgsiz
+    out = {k: np.zeros(S) for k in ("dzu1", "dzu2", "u1flux3d", "u2flux3d", "w")}
+    det = np.ascontiguousarray(detadt, np.float64)
+    P = _abi.dptr
+    rc = L.ref_preamble(C.byref(case.win.geom), C.byref(st), C.byref(op), P(det),
+                        P(out["dzu1"]), P(out["dzu2"]), P(out["u1flux3d"]), P(out["u2flux3d"]),
+                        P(out["w"]))
+    if rc:
+        raise RuntimeError("ref_preamble: status %d" % rc)
+    return out
+
+
+def preamble(case, detadt, sur=None, nsur=None):
+    """The restatement of the same preamble (oracle/flow_preamble.py)."""
+    from . import flow_preamble
+    return flow_preamble.preamble(case, detadt, sur, nsur)
 
 
 def set_strip(owned2d=None, dmin=0.0):

@@ -12,6 +12,12 @@
   oracle/_ref/libshoc_shim.so       include/shoc_tr_shim.h (the SHOC-side binding)
                                     compiled against the reference's headers,
                                     linked with the product library
+  oracle/_ref/libshoc_ref_vel.so    the reference's transport-mode preamble:
+                                    model/hd/momentum/vel3d.c with tracers.c and
+                                    MY2-5.c, unmodified, driven by
+                                    oracle/ref/ref_preamble.c (no-op link stubs
+                                    for vel3d.c's other callees in
+                                    oracle/ref/vel_stubs.c)
 
 The reference libraries are built only where the reference source tree is
 present: the directory named by the REF_ROOT environment variable or the
@@ -99,6 +105,29 @@ def ref_libs(force=False):
     return outs
 
 
+def ref_vel_lib(force=False):
+    """set_dz_at_u1 / _u2, set_flux_3d, set_dz and vel_w_update compiled from
+    the reference (only where its sources exist)."""
+    out = os.path.join(REF_OUT, "libshoc_ref_vel.so")
+    if not ref_available():
+        return out if os.path.exists(out) else None
+    R = REF_ROOT
+    inc = ["-I", os.path.join(HERE, "ref", "stub"), "-I", os.path.join(ROOT, "include"),
+           "-I", os.path.join(R, "lib", "include"), "-I", os.path.join(R, "model", "hd", "include")]
+    for sub in ("sediments", "tracerstats", "waves", "ecology", "da"):
+        inc += ["-I", os.path.join(R, "model", "lib", sub, "include")]
+    srcs = [os.path.join(R, "model", "hd", "tracers", "tracers.c"),
+            os.path.join(R, "model", "hd", "closure", "MY2-5.c"),
+            os.path.join(R, "model", "hd", "momentum", "vel3d.c"),
+            os.path.join(HERE, "ref", "ref_harness.c"), os.path.join(HERE, "ref", "ref_preamble.c"),
+            os.path.join(HERE, "ref", "vel_stubs.c")]
+    deps = srcs + [os.path.join(ROOT, "include", "shoc_tr.h")]
+    if force or _stale(out, deps):
+        os.makedirs(REF_OUT, exist_ok=True)
+        _run(["gcc", "-w"] + CFLAGS + ["-DREF_WITH_VEL3D"] + inc + ["-o", out] + srcs + ["-lm"])
+    return out
+
+
 def shim_lib(force=False):
     """include/shoc_tr_shim.h compiled against the reference's headers and
     linked with the product library it binds (oracle/_ref/libshoc_shim.so);
@@ -127,9 +156,9 @@ def shim_lib(force=False):
 def build_all(force=False):
     out = [oracle_lib(force), grid_lib(force)]
     out += ref_libs(force)
-    shim = shim_lib(force)
-    if shim:
-        out.append(shim)
+    for extra in (shim_lib(force), ref_vel_lib(force)):
+        if extra:
+            out.append(extra)
     return out
 
 
