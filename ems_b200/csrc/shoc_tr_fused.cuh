@@ -2,11 +2,12 @@
 // sub-step: advection and horizontal diffusion (advect_diffuse, tracers.c:
 // 849-925), tr_bounds (:3217-3324), surf_conc (:3047-3207) and, on the last
 // sub-step, the implicit vertical diffusion (vert_diffuse_3d /
-// implicit_vdiff_tr, :3893-3953, :4067-4214) of a tile of 8 x 4 water columns
+// implicit_vdiff_tr, :3893-3953, :4067-4214) of a tile of 32 water columns
 // over all its layers and tracers, with an FP64 per-column mass carry.
 //
-// A block owns one tile (lane = column: lane = 8 * iy + ix for the columns at
-// (i0 + ix, j0 + iy)) and runs two phases:
+// A block owns one tile of tx x (32 / tx) columns (tx = 8, 16 or 32, a
+// launch parameter the autotuner chooses; lane = tx * iy + ix for the column
+// at (i0 + ix, j0 + iy)) and runs two phases:
 //
 //  A  advection, layer chunk by layer chunk from the top down: warp w holds
 //     layer k0 - w of the chunk, so a thread holds one cell and folds its
@@ -50,6 +51,7 @@ struct Fused {
   const int *tcol;    // [ntile][32] column of each lane of each tile (-1: none)
   const int *tkmin;   // [ntile] lowest layer of the tile's columns
   int ntile;
+  int tx;             // tile width along i (8, 16 or 32)
   double *carry;      // [ntr][ncol] FP64 mass the stored values owe each column
   int nwb;            // warps of phase B (tracers in flight per tile)
   int ngrp;           // advected tracers per phase-A reduction pass
@@ -153,9 +155,10 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       fl = Tl.fl[c];
     }
     // east / north neighbours that are the cells of the lanes at ix + 1 / iy + 1
-    const int cE = __shfl_down_sync(FULL, c, 1), cN = __shfl_down_sync(FULL, c, 8);
-    const bool sxp1 = on && (lane & 7) != 7 && cE != 0 && n1.y == cE;
-    const bool syp1 = on && lane < 24 && cN != 0 && n1.w == cN;
+    const int tx = Fu.tx;
+    const int cE = __shfl_down_sync(FULL, c, 1), cN = __shfl_down_sync(FULL, c, tx);
+    const bool sxp1 = on && (lane & (tx - 1)) != tx - 1 && cE != 0 && n1.y == cE;
+    const bool syp1 = on && lane < 32 - tx && cN != 0 && n1.w == cN;
     const bool zf = on && k <= ks, zt = on && k < ks;
     Face fw, fs, fn, fe, fzb, fzt;
     f32::face_zero(fw);
@@ -254,7 +257,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
         const double Ft = (vz && zt) ? face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2)
                                      : 0.0;
         const double e = __shfl_down_sync(FULL, Fw, 1);
-        const double nb = __shfl_down_sync(FULL, Fs, 8);
+        const double nb = __shfl_down_sync(FULL, Fs, tx);
         if (sxp1) Fe = e;
         if (syp1) Fn = nb;
         double contrib = 0.0;

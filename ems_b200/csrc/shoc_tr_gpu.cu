@@ -30,7 +30,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <string>
 #include <vector>
+
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "shoc_tr_gpu.h"
 #include "shoc_tr_kernels.cuh"
@@ -90,6 +94,11 @@ struct shoc_tr_gpu {
   Fused fu{};                         // FP32-mixed: the columns' mass carry; k_step32's tiles
   bool fused = false;                 // FP32-mixed sub-steps run k_step32
   size_t fused_bytes = 0;             // its dynamic shared memory
+  struct FusedTiles {                 // k_step32 tiles of width 8, 16, 32
+    const int *tcol = nullptr, *tkmin = nullptr;
+    int ntile = 0;
+  } ftile[3];
+  int fnwb_max = 0;                   // phase-B warps k_step32 may have (0: no k_step32)
   std::vector<int> vd_depth;          // layers of the k_vd32 tiles, in their (sorted) order
   bool staged = false;                // column-tile fast path
   int cur = 0;
@@ -962,11 +971,13 @@ int build_tile_tables(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<u
   return 0;
 }
 
-// Tiles of the fused FP32-mixed kernel: 8 x 4 water columns (lane = 8 * iy
-// + ix for the column at (8 * ti + ix, 4 * tj + iy)), in row-major tile order
-// so that blocks running at the same time hold neighbouring tiles; a tile's
-// lowest layer bounds its layer loop.
-int build_fused_tiles(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<int> &col_kb) {
+// Tiles of the fused FP32-mixed kernel: tx x ty water columns, ty = 32 / tx
+// (lane = tx * iy + ix for the column at (tx * ti + ix, ty * tj + iy)), in
+// row-major tile order so that blocks running at the same time hold
+// neighbouring tiles; a tile's lowest layer bounds its layer loop.
+int build_fused_tiles(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<int> &col_kb,
+                      int tx, shoc_tr_gpu::FusedTiles &out) {
+  const int ty = 32 / tx;
   const int ncol = h->ncol;
   int imax = 0, jmax = 0;
   for (int col = 0; col < ncol; col++) {
@@ -975,14 +986,14 @@ int build_fused_tiles(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<i
     imax = std::max(imax, g->s2i[top]);
     jmax = std::max(jmax, g->s2j[top]);
   }
-  const long long nti = imax / 8 + 1, ntj = jmax / 4 + 1;
+  const long long nti = imax / tx + 1, ntj = jmax / ty + 1;
   std::vector<int> tid((size_t)(nti * ntj), -1);
   std::vector<int> tcol, tkmin;
   std::vector<int> order(ncol);
   for (int col = 0; col < ncol; col++) order[col] = col;
   auto key = [&](int col) {
     const int top = g->w2_t[col + 1];
-    return (long long)(g->s2j[top] / 4) * nti + g->s2i[top] / 8;
+    return (long long)(g->s2j[top] / ty) * nti + g->s2i[top] / tx;
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
   for (int col : order) {
@@ -994,19 +1005,79 @@ int build_fused_tiles(shoc_tr_gpu *h, const shoc_tr_geom *g, const std::vector<i
       tkmin.push_back(h->nz);
       tcol.insert(tcol.end(), 32, -1);
     }
-    const int lane = (j % 4) * 8 + i % 8;
+    const int lane = (j % ty) * tx + i % tx;
     if (tcol[(size_t)t * 32 + lane] >= 0) return SHOC_TR_EGEOM;  // two columns at one (i, j)
     tcol[(size_t)t * 32 + lane] = col;
     tkmin[t] = std::min(tkmin[t], col_kb[col]);
   }
-  h->fu.ntile = (int)tkmin.size();
+  out.ntile = (int)tkmin.size();
   int *ip;
   int rc;
   if ((rc = dupload(h, &ip, tcol.data(), tcol.size()))) return rc;
-  h->fu.tcol = ip;
+  out.tcol = ip;
   if ((rc = dupload(h, &ip, tkmin.data(), tkmin.size()))) return rc;
-  h->fu.tkmin = ip;
+  out.tkmin = ip;
   return 0;
+}
+
+// k_step32's shared memory with nwb phase-B warps, and its reduction group:
+// as many advected tracers per phase-A reduction pass as fit the space the
+// phase-B arrays leave.
+size_t fused_config(const shoc_tr_gpu *h, int nwb, int *ngrp) {
+  const int ntb = h->T.ntb;
+  const size_t room = (size_t)2 * nwb * h->nz * 32 * 4;
+  const size_t buf = (size_t)2 * kStencil * kFusedThreads * 4;
+  const int gmax = room > buf ? (int)((room - buf) / fused_red(1)) : 1;
+  *ngrp = std::max(1, std::min(std::max(ntb, 1), gmax));
+  return fused_smem(h->nz, nwb, ntb, *ngrp);
+}
+
+int tile_index(int tx) { return tx == 8 ? 0 : tx == 16 ? 1 : tx == 32 ? 2 : -1; }
+
+void drop_graphs(shoc_tr_gpu *h) {
+  for (int i = 0; i < 2; i++)
+    if (h->graph[i]) {
+      cudaGraphExecDestroy(h->graph[i]);
+      h->graph[i] = nullptr;
+    }
+}
+
+// The launch configuration of the transport kernels (validated; takes
+// effect at the next step).
+int apply_tuning(shoc_tr_gpu *h, const shoc_tr_tuning &t) {
+  const bool f32 = h->esize == sizeof(float);
+  if (t.tracers_per_block < 1 || t.tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
+  if (vd_smem(h, h->nz, t.tracers_per_block) > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
+  if (t.fused) {
+    const int ti = tile_index(t.tile_x);
+    if (!f32 || !h->fnwb_max || ti < 0 || !h->ftile[ti].tcol) return SHOC_TR_EUNSUPPORTED;
+    if (t.phase_b_warps < 1 || t.phase_b_warps > h->fnwb_max) return SHOC_TR_EUNSUPPORTED;
+  } else if (f32 && !h->rnd) {
+    const int rc = dalloc(h, &h->rnd, (size_t)h->ntr * h->S);
+    if (rc) return rc;
+  }
+  h->tw = t.tracers_per_block;
+  h->fused = t.fused != 0;
+  if (h->fused) {
+    const auto &ft = h->ftile[tile_index(t.tile_x)];
+    h->fu.tcol = ft.tcol;
+    h->fu.tkmin = ft.tkmin;
+    h->fu.ntile = ft.ntile;
+    h->fu.tx = t.tile_x;
+    h->fu.nwb = t.phase_b_warps;
+    h->fused_bytes = fused_config(h, t.phase_b_warps, &h->fu.ngrp);
+  }
+  drop_graphs(h);
+  return SHOC_TR_OK;
+}
+
+shoc_tr_tuning current_tuning(const shoc_tr_gpu *h) {
+  shoc_tr_tuning t;
+  t.fused = h->fused ? 1 : 0;
+  t.tracers_per_block = h->tw;
+  t.tile_x = h->fused ? h->fu.tx : 8;
+  t.phase_b_warps = h->fused ? h->fu.nwb : h->fnwb_max;
+  return t;
 }
 
 int map_status(int st) {
@@ -1382,6 +1453,17 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     TRY(dupload<double>(h, &h->fu.carry, nullptr, (size_t)ntr * ncol));
   }
   TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
+  // tiling: tracers per block
+  int tw = 8;
+  {
+    // tracers per column-kernel block: two blocks per SM at full depth,
+    // balanced chunks
+    while (tw > 1 && vd_smem(h, g->nz, tw) > 113 * 1024) tw--;
+    int nch = (h->nslot + tw - 1) / std::max(tw, 1);
+    if (nch > 0) tw = (h->nslot + nch - 1) / nch;
+    if (tw < 1) tw = 1;
+  }
+  h->tw = tw;
   TRY(build_tile_tables(h, g, cflag, col_bot, col_kb));
   {  // face columns of the transport-mode preamble
     std::vector<int2> fc;
@@ -1398,36 +1480,31 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     }
   }
   if (f32p) {
-    // the fused sub-step kernel (SHOC_TR_GPU_KERNELS=fused; the two-kernel
-    // sub-step is the default, measured faster): every advected tracer's
-    // accumulators and the column arrays of as many phase-B warps as keep
-    // two blocks per SM
-    const char *env = getenv("SHOC_TR_GPU_KERNELS");
-    const bool want = env && strcmp(env, "fused") == 0;
-    // (phase-B warps, tracers per reduction pass): the most phase-B warps
-    // that keep two blocks per SM, the reduction groups fitting the space
-    // the phase-B arrays leave
-    const int ntb = o->ntbdy;
-    int nwb = 0, ngrp = 0;
-    for (int c = kFusedWarps; c >= 1 && !nwb; c--) {
-      const size_t room = (size_t)2 * c * g->nz * 32 * 4;
-      const size_t buf = (size_t)2 * kStencil * kFusedThreads * 4;
-      const int gmax = room > buf ? (int)((room - buf) / fused_red(1)) : 1;
-      const int gq = std::max(1, std::min(std::max(ntb, 1), gmax));
-      if (fused_smem(g->nz, c, ntb, gq) <= 113 * 1024) {
-        nwb = c;
-        ngrp = gq;
+    // the fused sub-step kernel k_step32: every advected tracer's
+    // accumulators and the column arrays of up to as many phase-B warps as
+    // keep two blocks per SM; tiles of every width the autotuner may choose
+    if (o->ntbdy <= kFusedMaxTracers) {
+      for (int c = kFusedWarps; c >= 1 && !h->fnwb_max; c--) {
+        int gq;
+        if (fused_config(h, c, &gq) <= 113 * 1024) h->fnwb_max = c;
       }
     }
-    if (want && nwb && ntb <= kFusedMaxTracers) {
-      TRY(build_fused_tiles(h, g, col_kb));
-      h->fu.nwb = nwb;
-      h->fu.ngrp = ngrp;
-      h->fused_bytes = fused_smem(g->nz, nwb, ntb, ngrp);
-      h->fused = true;
-      if (fused32_set_smem_attr((int)h->fused_bytes) != cudaSuccess) TRY(SHOC_TR_ECUDA);
+    if (h->fnwb_max) {
+      int gq;
+      if (fused32_set_smem_attr((int)fused_config(h, h->fnwb_max, &gq)) != cudaSuccess)
+        TRY(SHOC_TR_ECUDA);
+      for (int tx : {8, 16, 32}) TRY(build_fused_tiles(h, g, col_kb, tx, h->ftile[tile_index(tx)]));
     }
-    if (!h->fused) TRY(dupload<float>(h, &h->rnd, nullptr, (size_t)ntr * S));
+    // the two-kernel sub-step is the default (measured faster);
+    // SHOC_TR_GPU_KERNELS=fused starts with k_step32 (8 x 4 tiles)
+    const char *env = getenv("SHOC_TR_GPU_KERNELS");
+    shoc_tr_tuning t0 = current_tuning(h);
+    if (env && strcmp(env, "fused") == 0 && h->fnwb_max) {
+      t0.fused = 1;
+      t0.tile_x = 8;
+      t0.phase_b_warps = h->fnwb_max;
+    }
+    TRY(apply_tuning(h, t0));
   }
   // flow fields
   Flow &F = h->F;
@@ -1457,17 +1534,6 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   h->h_status = (int *)((char *)pin + 8);
   h->h_nwarn = (unsigned long long *)((char *)pin + 16);
   h->h_counts = (int *)((char *)pin + 24);
-  // tiling: tracers per block
-  int tw = 8;
-  {
-    // tracers per column-kernel block: two blocks per SM at full depth,
-    // balanced chunks
-    while (tw > 1 && vd_smem(h, g->nz, tw) > 113 * 1024) tw--;
-    int nch = (h->nslot + tw - 1) / std::max(tw, 1);
-    if (nch > 0) tw = (h->nslot + nch - 1) / nch;
-    if (tw < 1) tw = 1;
-  }
-  h->tw = tw;
   if (cudaFuncSetAttribute(k_vd64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024) != cudaSuccess ||
       cudaFuncSetAttribute(k_vd64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2741,47 +2807,228 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
   if (!h) return SHOC_TR_EARG;
   DeviceScope dev_(h->device);
   if (cols_per_block != 0 && cols_per_block != 32) return SHOC_TR_EUNSUPPORTED;
-  if (tracers_per_block > 0) {
-    if (tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
-    if (vd_smem(h, h->nz, tracers_per_block) > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
-    h->tw = tracers_per_block;
-    for (int i = 0; i < 2; i++)
-      if (h->graph[i]) {
-        cudaGraphExecDestroy(h->graph[i]);
-        h->graph[i] = nullptr;
-      }
+  if (tracers_per_block <= 0) return SHOC_TR_OK;
+  shoc_tr_tuning t = current_tuning(h);
+  t.tracers_per_block = tracers_per_block;
+  return apply_tuning(h, t);
+}
+
+int shoc_tr_gpu_get_tuning(shoc_tr_gpu *h, shoc_tr_tuning *t) {
+  if (!h || !t) return SHOC_TR_EARG;
+  *t = current_tuning(h);
+  return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t) {
+  if (!h || !t) return SHOC_TR_EARG;
+  DeviceScope dev_(h->device);
+  return apply_tuning(h, *t);
+}
+
+}  // extern "C"
+
+// ---- autotuner ----
+namespace {
+
+// The autotuner's cache: one line per GPU model and window configuration,
+//   <key> <fused> <tracers_per_block> <tile_x> <phase_b_warps> <ms>
+// in the file SHOC_TR_TUNE_CACHE names (default
+// $HOME/.cache/shoc_tr_gpu/tuning.txt; "off": none).
+std::string tune_cache_path() {
+  const char *e = getenv("SHOC_TR_TUNE_CACHE");
+  if (e) return strcmp(e, "off") == 0 ? std::string() : std::string(e);
+  const char *home = getenv("HOME");
+  if (!home || !*home) return std::string();
+  return std::string(home) + "/.cache/shoc_tr_gpu/tuning.txt";
+}
+
+std::string tune_key(const shoc_tr_gpu *h) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, h->device) != cudaSuccess) return std::string();
+  std::string name = p.name;
+  for (char &c : name)
+    if (c == ' ' || c == '\t') c = '_';
+  char buf[512];
+  snprintf(buf, sizeof buf, "v1|%s|sm%d%d|S%d|C%d|Z%d|N%d|B%d|P%d|A%d|U%d|F%d|H%d|V%d",
+           name.c_str(), p.major, p.minor, h->S, h->ncol, h->nz, h->ntr, h->T.ntb, h->precision,
+           h->O.trasc, h->O.ultimate, h->adv_flags, h->any_hdiff ? 1 : 0, h->any_vdiff ? 1 : 0);
+  return std::string(buf);
+}
+
+bool tune_cache_get(const std::string &path, const std::string &key, shoc_tr_tuning *t) {
+  if (path.empty() || key.empty()) return false;
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return false;
+  char line[1024];
+  bool found = false;
+  while (fgets(line, sizeof line, f)) {
+    char k[600];
+    shoc_tr_tuning v;
+    double ms;
+    if (sscanf(line, "%599s %d %d %d %d %lf", k, &v.fused, &v.tracers_per_block, &v.tile_x,
+               &v.phase_b_warps, &ms) == 6 &&
+        key == k) {
+      *t = v;
+      found = true;  // the last line for a key wins
+    }
   }
+  fclose(f);
+  return found;
+}
+
+void tune_cache_put(const std::string &path, const std::string &key, const shoc_tr_tuning &t,
+                    double ms) {
+  if (path.empty() || key.empty()) return;
+  // the directory, one level at a time
+  for (size_t i = 1; i < path.size(); i++)
+    if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+  std::vector<std::string> keep;
+  if (FILE *f = fopen(path.c_str(), "r")) {
+    char line[1024];
+    while (fgets(line, sizeof line, f)) {
+      char k[600];
+      if (sscanf(line, "%599s", k) == 1 && key != k) keep.push_back(line);
+    }
+    fclose(f);
+  }
+  const std::string tmp = path + ".tmp" + std::to_string((long long)getpid());
+  FILE *f = fopen(tmp.c_str(), "w");
+  if (!f) return;
+  for (auto &l : keep) fputs(l.c_str(), f);
+  fprintf(f, "%s %d %d %d %d %.6f\n", key.c_str(), t.fused, t.tracers_per_block, t.tile_x,
+          t.phase_b_warps, ms);
+  fclose(f);
+  rename(tmp.c_str(), path.c_str());
+}
+
+// Device copy of the resident state (both tracer buffers, mass carry,
+// surface vectors) the trial steps start from.
+struct Snapshot {
+  void *tr = nullptr;
+  double *carry = nullptr;
+  int *sur = nullptr, *nsur = nullptr;
+  int cur = 0;
+};
+
+int snap_take(shoc_tr_gpu *h, Snapshot &s) {
+  const size_t tb = (size_t)h->ntr * h->S * h->esize;
+  const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
+  const size_t ib = (size_t)h->ncol * sizeof(int);
+  CK(cudaMallocAsync(&s.tr, tb ? 2 * tb : 1, h->stream));
+  if (h->fu.carry) CK(cudaMallocAsync((void **)&s.carry, cb ? cb : 1, h->stream));
+  CK(cudaMallocAsync((void **)&s.sur, 2 * ib, h->stream));
+  s.nsur = s.sur + h->ncol;
+  s.cur = h->cur;
+  for (int b = 0; b < 2; b++)
+    CK(cudaMemcpyAsync((char *)s.tr + b * tb, h->tr[b], tb, cudaMemcpyDeviceToDevice, h->stream));
+  if (s.carry) CK(cudaMemcpyAsync(s.carry, h->fu.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(s.sur, h->W.sur_t, ib, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(s.nsur, h->W.nsur_t, ib, cudaMemcpyDeviceToDevice, h->stream));
   return 0;
 }
 
-int shoc_tr_gpu_autotune(shoc_tr_gpu *h, int steps, int *tracers_per_block) {
+int snap_restore(shoc_tr_gpu *h, const Snapshot &s) {
+  const size_t tb = (size_t)h->ntr * h->S * h->esize;
+  const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
+  const size_t ib = (size_t)h->ncol * sizeof(int);
+  h->cur = s.cur;
+  for (int b = 0; b < 2; b++)
+    CK(cudaMemcpyAsync(h->tr[b], (const char *)s.tr + b * tb, tb, cudaMemcpyDeviceToDevice,
+                       h->stream));
+  if (s.carry) CK(cudaMemcpyAsync(h->fu.carry, s.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->W.sur_t, s.sur, ib, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->W.nsur_t, s.nsur, ib, cudaMemcpyDeviceToDevice, h->stream));
+  return 0;
+}
+
+void snap_free(shoc_tr_gpu *h, Snapshot &s) {
+  if (s.tr) cudaFreeAsync(s.tr, h->stream);
+  if (s.carry) cudaFreeAsync(s.carry, h->stream);
+  if (s.sur) cudaFreeAsync(s.sur, h->stream);
+  cudaStreamSynchronize(h->stream);
+  s = Snapshot();
+}
+
+}  // namespace
+
+extern "C" {
+
+int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tuning *best,
+                            int *from_cache) {
   if (!h || steps < 1) return SHOC_TR_EARG;
-  static const int cand[] = {2, 3, 4, 5, 6, 8};
+  DeviceScope dev_(h->device);
+  if (from_cache) *from_cache = 0;
+  const std::string path = use_cache ? tune_cache_path() : std::string();
+  const std::string key = use_cache ? tune_key(h) : std::string();
+  shoc_tr_tuning t;
+  if (use_cache && tune_cache_get(path, key, &t) && apply_tuning(h, t) == SHOC_TR_OK) {
+    if (best) *best = t;
+    if (from_cache) *from_cache = 1;
+    return SHOC_TR_OK;
+  }
+  // candidates: tracers per column-kernel block for the two-kernel sub-step;
+  // tile widths and phase-B warps for the fused one (FP32-mixed, where it fits)
+  std::vector<shoc_tr_tuning> cand;
+  shoc_tr_tuning base = current_tuning(h);
+  for (int tw : {2, 3, 4, 5, 6, 8}) {
+    shoc_tr_tuning c = base;
+    c.fused = 0;
+    c.tracers_per_block = tw;
+    cand.push_back(c);
+  }
+  if (h->esize == sizeof(float) && h->fnwb_max) {
+    std::vector<int> nwbs = {h->fnwb_max};
+    if (h->fnwb_max / 2 >= 1 && h->fnwb_max / 2 != h->fnwb_max) nwbs.push_back(h->fnwb_max / 2);
+    for (int tx : {8, 16, 32})
+      for (int nwb : nwbs) {
+        shoc_tr_tuning c = base;
+        c.fused = 1;
+        c.tile_x = tx;
+        c.phase_b_warps = nwb;
+        cand.push_back(c);
+      }
+  }
+  Snapshot snap;
+  int rc = snap_take(h, snap);
+  if (rc) {
+    snap_free(h, snap);
+    return rc;
+  }
   const bool prof0 = h->profile;
-  int best_tw = h->tw;
-  double best = 1e300;
-  for (int c : cand) {
-    if (shoc_tr_gpu_set_tiling(h, 0, c) != SHOC_TR_OK) continue;
+  shoc_tr_tuning win = base;
+  double best_ms = 1e300;
+  for (const auto &c : cand) {
+    if (apply_tuning(h, c) != SHOC_TR_OK) continue;
     shoc_tr_gpu_profile(h, 1);
-    int rc = shoc_tr_gpu_run(h, steps);
+    rc = shoc_tr_gpu_run(h, steps);
     if (!rc) rc = shoc_tr_gpu_sync(h, nullptr);
-    if (rc) {
-      shoc_tr_gpu_set_tiling(h, 0, best_tw);
-      h->profile = prof0;
-      return rc;
-    }
     double ms = 0.0;
     int n = 0;
     shoc_tr_gpu_kernel_time(h, &ms, &n);
-    if (n > 0 && ms < best) {
-      best = ms;
-      best_tw = c;
+    if (!rc) rc = snap_restore(h, snap);
+    if (rc) break;
+    if (n > 0 && ms < best_ms) {
+      best_ms = ms;
+      win = c;
     }
   }
-  shoc_tr_gpu_set_tiling(h, 0, best_tw);
+  if (!rc) rc = snap_restore(h, snap);
+  snap_free(h, snap);
+  h->profile = prof0;
   shoc_tr_gpu_profile(h, prof0 ? 1 : 0);
-  if (tracers_per_block) *tracers_per_block = best_tw;
+  const int rc2 = apply_tuning(h, win);
+  if (rc) return rc;
+  if (rc2) return rc2;
+  if (use_cache && best_ms < 1e300) tune_cache_put(path, key, win, best_ms);
+  if (best) *best = win;
   return SHOC_TR_OK;
+}
+
+int shoc_tr_gpu_autotune(shoc_tr_gpu *h, int steps, int *tracers_per_block) {
+  shoc_tr_tuning t;
+  const int rc = shoc_tr_gpu_autotune_ex(h, steps, 0, &t, nullptr);
+  if (!rc && tracers_per_block) *tracers_per_block = t.tracers_per_block;
+  return rc;
 }
 
 int shoc_tr_gpu_profile(shoc_tr_gpu *h, int enable) {

@@ -30,8 +30,18 @@ EXPORTS = (
     "shoc_tr_gpu_stream", "shoc_tr_gpu_set_tiling", "shoc_tr_gpu_autotune", "shoc_tr_gpu_profile",
     "shoc_tr_gpu_kernel_time", "shoc_tr_gpu_kernel_time_part", "shoc_tr_gpu_launch_count",
     "shoc_tr_gpu_strerror", "shoc_tr_gpu_set_preamble", "shoc_tr_gpu_set_detadt",
-    "shoc_tr_gpu_get_flow",
+    "shoc_tr_gpu_get_flow", "shoc_tr_gpu_get_tuning", "shoc_tr_gpu_set_tuning",
+    "shoc_tr_gpu_autotune_ex",
 )
+
+
+class Tuning(C.Structure):
+    """shoc_tr_tuning: the transport kernels' launch configuration."""
+    _fields_ = [("fused", C.c_int), ("tracers_per_block", C.c_int), ("tile_x", C.c_int),
+                ("phase_b_warps", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 _lib = None
 
@@ -85,6 +95,10 @@ def lib(path=None):
                                                C.POINTER(C.c_int)]
     L.shoc_tr_gpu_launch_count.argtypes = [H]
     L.shoc_tr_gpu_launch_count.restype = C.c_longlong
+    L.shoc_tr_gpu_get_tuning.argtypes = [H, C.POINTER(Tuning)]
+    L.shoc_tr_gpu_set_tuning.argtypes = [H, C.POINTER(Tuning)]
+    L.shoc_tr_gpu_autotune_ex.argtypes = [H, C.c_int, C.c_int, C.POINTER(Tuning),
+                                          C.POINTER(C.c_int)]
     L.shoc_tr_gpu_set_preamble.argtypes = [H, C.c_int]
     L.shoc_tr_gpu_set_detadt.argtypes = [H, _abi.DP]
     L.shoc_tr_gpu_get_flow.argtypes = [H] + [_abi.DP] * 5
@@ -358,11 +372,33 @@ class TracerStep:
         _check("set_tiling", self.L.shoc_tr_gpu_set_tiling(self.h, cols, tracers))
 
     def autotune(self, steps=2):
-        """Pick the tracers per block with the fastest transport (runs
-        `steps` real steps per candidate); returns the choice."""
+        """Pick the fastest launch configuration (`steps` trial steps per
+        candidate from the current state, which is put back); returns the
+        tracers per block (shoc_tr_gpu_autotune, no cache)."""
         tw = C.c_int()
         _check("autotune", self.L.shoc_tr_gpu_autotune(self.h, int(steps), C.byref(tw)))
         return tw.value
+
+    def autotune_ex(self, steps=2, use_cache=True):
+        """shoc_tr_gpu_autotune_ex: (tuning dict, from_cache)."""
+        t, fc = Tuning(), C.c_int()
+        _check("autotune_ex", self.L.shoc_tr_gpu_autotune_ex(
+            self.h, int(steps), 1 if use_cache else 0, C.byref(t), C.byref(fc)))
+        return t.as_dict(), bool(fc.value)
+
+    def get_tuning(self):
+        t = Tuning()
+        _check("get_tuning", self.L.shoc_tr_gpu_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Change fields of the current tuning (fused, tracers_per_block,
+        tile_x, phase_b_warps)."""
+        t = Tuning()
+        _check("get_tuning", self.L.shoc_tr_gpu_get_tuning(self.h, C.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        _check("set_tuning", self.L.shoc_tr_gpu_set_tuning(self.h, C.byref(t)))
 
     def profile(self, on=True):
         _check("profile", self.L.shoc_tr_gpu_profile(self.h, 1 if on else 0))

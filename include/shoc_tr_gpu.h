@@ -239,16 +239,45 @@ int shoc_tr_gpu_set_substep_min(shoc_tr_gpu *h, double dmin);
 /* cudaStream_t of the handle, for event timing by the caller. */
 void *shoc_tr_gpu_stream(shoc_tr_gpu *h);
 
-/* Launch tuning: columns per block (multiple of 32) and tracers per block.
- * 0 keeps the current value.  Takes effect at the next step. */
+/* Launch tuning: columns per block (32; 0 keeps it) and tracers per block
+ * of the column kernel (0 keeps it).  Takes effect at the next step. */
 int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_block);
 
-/* Autotuner: runs `steps` steps (real steps: the tracers advance exactly as
- * with shoc_tr_gpu_run, and the results do not depend on the tiling) with
- * each candidate number of tracers per block, times the transport kernels
- * with CUDA events, and keeps the fastest; returns it in *tracers_per_block
- * (may be NULL).  Call after the flow is set.  No reference counterpart
+/* The transport kernels' launch configuration.  No reference counterpart
  * (launch tuning of this library). */
+typedef struct {
+  int fused;             /* FP32-mixed: 1 one fused launch per sub-step (k_step32),
+                            0 the advection + column kernel pair */
+  int tracers_per_block; /* column kernel (k_vd32 / k_vd64): tracers per block, 1..8 */
+  int tile_x;            /* k_step32: tile width along i (8, 16, 32; 32 / tile_x
+                            columns along j) */
+  int phase_b_warps;     /* k_step32: warps of its column phase */
+} shoc_tr_tuning;
+/* set_tuning validates (SHOC_TR_EUNSUPPORTED for a configuration the window
+ * or the shared memory does not allow) and takes effect at the next step.
+ * Results are bitwise independent of tracers_per_block, tile_x and
+ * phase_b_warps; the FP32-mixed fused and two-kernel sub-steps agree to FP32
+ * rounding. */
+int shoc_tr_gpu_get_tuning(shoc_tr_gpu *h, shoc_tr_tuning *t);
+int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t);
+
+/* Autotuner: from the current state, runs `steps` trial steps with each
+ * candidate configuration, times the transport kernels with CUDA events,
+ * puts the state back (a device copy taken before the trials: the tracers,
+ * surface vectors and mass carry are as they were) and keeps the fastest.
+ * Candidates: 2..8 tracers per block of the column kernel; for FP32-mixed
+ * also the fused sub-step with tile widths 8, 16, 32 and the most and half
+ * the most phase-B warps its shared memory allows.  With use_cache != 0 the
+ * choice is looked up in and saved to a file keyed by the GPU model and the
+ * window's configuration (sizes, tracers, precision, scheme, diffusion),
+ * named by the environment variable SHOC_TR_TUNE_CACHE (default
+ * $HOME/.cache/shoc_tr_gpu/tuning.txt, "off" for none): a cached choice is
+ * applied without trial steps and *from_cache set to 1.  best / from_cache
+ * may be NULL.  Call after the flow is set and any earlier step synced.
+ * shoc_tr_gpu_autotune is autotune_ex without the cache, returning the
+ * tracers per block. */
+int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tuning *best,
+                            int *from_cache);
 int shoc_tr_gpu_autotune(shoc_tr_gpu *h, int steps, int *tracers_per_block);
 
 /* Time of the transport of a step's last sub-step (the transport kernels

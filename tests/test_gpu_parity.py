@@ -141,25 +141,59 @@ def test_substep_limit_raises():
 
 
 @pytest.mark.parametrize("prec", [gpu.FP64, gpu.FP32_MIXED])
-def test_autotune_keeps_results(prec):
-    """The autotuner's trial steps are real steps: 6 candidates x 1 step plus
-    2 more steps give the same tracers as 8 plain steps, bit for bit."""
+def test_autotune_keeps_state(prec, tmp_path, monkeypatch):
+    """The autotuner's trial steps start from a device copy of the state and
+    the state is put back: 3 steps after autotuning equal 3 plain steps with
+    the chosen configuration, bit for bit.  The choice is cached per GPU and
+    configuration: a second handle gets it without trial steps."""
+    monkeypatch.setenv("SHOC_TR_TUNE_CACHE", str(tmp_path / "tuning.txt"))
     case = synth.make("small", seed=48)
-    ref = gpu.TracerStep(case, precision=prec)
-    ref.start()
-    ref.run(8)
-    ref.sync()
-    a = ref.download()
-    ref.close()
     t = gpu.TracerStep(case, precision=prec)
     t.start()
-    tw = t.autotune(1)
-    assert tw in (2, 3, 4, 5, 6, 8)
     t.run(2)
+    t.sync()
+    best, cached = t.autotune_ex(1)
+    assert not cached and best["tracers_per_block"] in (2, 3, 4, 5, 6, 8)
+    assert prec == gpu.FP32_MIXED or not best["fused"]
+    t.run(3)
     t.sync()
     b = t.download()
     t.close()
+    ref = gpu.TracerStep(case, precision=prec)
+    ref.start()
+    ref.set_tuning(**best)
+    ref.run(5)
+    ref.sync()
+    a = ref.download()
+    ref.close()
     np.testing.assert_array_equal(a[:, 1:], b[:, 1:])
+    u = gpu.TracerStep(case, precision=prec)
+    u.start()
+    best2, cached2 = u.autotune_ex(1)
+    u.close()
+    assert cached2 and best2 == best
+
+
+@pytest.mark.parametrize("tx", [8, 16, 32])
+def test_fused_tile_shapes_agree(tx):
+    """FP32-mixed fused sub-step: every tile width and phase-B warp count
+    gives the same tracers bit for bit (tiles only regroup columns)."""
+    case = synth.make("small", seed=49)
+    out = []
+    for tile_x, nwb in ((8, None), (tx, 1)):
+        t = gpu.TracerStep(case, precision=gpu.FP32_MIXED)
+        t.start()
+        kw = dict(fused=1, tile_x=tile_x)
+        if nwb:
+            kw["phase_b_warps"] = nwb
+        else:
+            kw["phase_b_warps"] = t.get_tuning()["phase_b_warps"] or 1
+        t.set_tuning(**kw)
+        t.run(4)
+        t.sync()
+        out.append(t.download())
+        t.close()
+    np.testing.assert_array_equal(out[0], out[1])
 
 
 @pytest.mark.parametrize("name", sorted(SCHEME_CASES))
