@@ -153,8 +153,9 @@ def ref_preamble(case, detadt, sur=None, nsur=None):
     L = _load("ref_vel")
     if L is None:
         raise FileNotFoundError("reference build oracle/_ref/libshoc_ref_vel.so not available")
-    sur = case.sur_t.copy() if sur is None else sur
-    nsur = case.nsur_t.copy() if nsur is None else nsur
+    # the reference's set_dz moves the surface vectors it is given: copies
+    sur = np.array(case.sur_t if sur is None else sur, np.int32)
+    nsur = np.array(case.nsur_t if nsur is None else nsur, np.int32)
     keep = []
     tr = case.tr.copy()
     st = case.make_state(tr, sur, nsur, keep)
