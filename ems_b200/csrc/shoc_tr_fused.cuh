@@ -308,12 +308,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int *const C0 = colC + (kb - kbase) * 32 + lane;
     const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
     const int nk = ks - kb;  // cells below the surface cell
-    // the water depth the carry is spread over, and 1 / dt for the FP64
-    // diagonal of the residual (dz / dt exactly, so the refined solve keeps
-    // the same column mass as the mass diagnostic measures)
-    double H = 0.0;
-    for (int j = 0; j <= nk; ++j) H += D0[j * 32];
-    const double idt = 1.0 / F.dt;
+    const double idt = 1.0 / F.dt;  // the residual's diagonal is dz / dt in FP64
     long long nwarn = 0;
     for (int slot = w; slot < T.nslot; slot += nwb) {
       const int n = T.slot_tr[slot];
@@ -342,7 +337,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       bool bad = false;
       cp_async_wait<0>();
       column_finish<LAST, false>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, 32, L0,
-                                 C0, D0, M0, tr, to, area, ia, H, idt, cs, Fu.carry, steady,
+                                 C0, D0, M0, tr, to, area, ia, idt, cs, Fu.carry, steady,
                                  nwarn, bad);
       if (bad) nstat |= ST_NAN;
     }

@@ -465,8 +465,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
                                               bool adv, bool vdf, float *A0, float *S0, int sa,
                                               const float4 *L0, const int *C0, const double *D0,
                                               const double *M0, const float *tr, float *to,
-                                              double area, double ia,
-                                              double H, double idt, ColSums cs,
+                                              double area, double ia, double idt, ColSums cs,
                                               double *carry, bool steady, long long &nwarn,
                                               bool &bad) {
   const ColInfo &ci = tc.ci;
@@ -478,45 +477,55 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   const double dzs_old = (double)W.dz32[ci.s];
   const double ts_old = (double)tr[ci.s];  // surface value before the sub-step
   const double dzs = D0[nk * 32];
-  const double carry_in = (carry && steady) ? carry[(size_t)n * G.ncol + col] : 0.0;
-  // the carry goes back as a uniform shift of the column's values
-  const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
   // FP64 mass bookkeeping per unit area: what the step computed (mxs) and
   // what is stored (mss)
-  double mxs = H > 0.0 ? carry_in * ia : 0.0, mss = 0.0;
+  double mxs = 0.0, mss = 0.0;
   long long nw = 0;
   double vs = ts_old;  // the surface value
+  double H = dzs;      // the water depth the carry is spread over
+  // tr_bounds clip and range check (:3278-3293) of the cells below the
+  // surface (advected tracers); a < mn and a > mx of a float a, exactly, as
+  // float compares
+  const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
+  const bool clip = tbdy && mn <= kClipEps;
+  if (RES && tbdy) {  // the divergence at and above the surface: stored + residual
+    double dv = 0.0;
+    for (int j = nk; j < nz - kb; ++j) dv += (double)A0[j * sa] + (double)S0[j * sa];
+    cs.dv = dv;
+  }
   if (!tbdy) {
-    for (int j = 0; j < nk; ++j) mxs += (double)A0[j * sa] * D0[j * 32];
     vs = (double)A0[nk * sa];
-    mxs += vs * dzs;
     for (int j = nk + 1; j < nz - kb; ++j) {
       to[C0[j * 32]] = A0[j * sa];
       bad |= isnan(A0[j * sa]);
     }
-  } else {
-    // tr_bounds clip and range check (:3278-3293) of the cells below the
-    // surface; a < mn and a > mx of a float a, exactly, as float compares
-    const float mnf = (float)mn, mn_up = __double2float_ru(mn), mx_dn = __double2float_rd(mx);
-    const bool clip = mn <= kClipEps;
-    if (RES) {
-      // the FP64 advected values are stored + residual
-      double m = 0.0, dv = 0.0;
-      for (int j = 0; j < nk; ++j) m += ((double)A0[j * sa] + (double)S0[j * sa]) * D0[j * 32];
-      for (int j = nk; j < nz - kb; ++j) dv += (double)A0[j * sa] + (double)S0[j * sa];
-      cs.m = m;
-      cs.dv = dv;
+  }
+  // one pass up the column below the surface: the computed mass (an
+  // advected tracer's FP64 values are stored + residual, or come in cs.m),
+  // the clip, the depth and, with a solve, the FP32 forward sweep
+  float fwd = 0.f;  // the bottom row's cm1 is 0
+  double m = 0.0;
+  for (int j = 0; j < nk; ++j) {
+    float a = A0[j * sa];
+    const double dz = D0[j * 32];
+    H += dz;
+    if (!tbdy || RES) m += (tbdy ? (double)a + (double)S0[j * sa] : (double)a) * dz;
+    if (clip && a < mn_up) {
+      mxs += ((double)mnf - (double)a) * dz;
+      a = mnf;
     }
-    mxs += cs.m;
-    for (int j = 0; j < nk; ++j) {
-      float a = A0[j * sa];
-      if (clip && a < mn_up) {
-        mxs += ((double)mnf - (double)a) * D0[j * 32];
-        a = mnf;
-      }
+    if (tbdy) {
       nw += (a < mn_up || a > mx_dn);
       A0[j * sa] = a;
     }
+    if (solve) {
+      const float4 lu = L0[j * 32];
+      fwd = (lu.x * a - lu.y * fwd) * lu.z;
+      S0[j * sa] = fwd;
+    }
+  }
+  mxs += (tbdy && !RES) ? cs.m : m;
+  if (tbdy) {
     const double a_below = nk > 0 ? (double)A0[(nk - 1) * sa] : 0.0;
     // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
     if (adv) {
@@ -538,10 +547,14 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     if (mn <= kClipEps && vs < mn) vs = mn;
     if (vs < mn || vs > mx) ++nw;
     bad |= isnan(vs);
-    mxs += vs * dzs;
     const float vs32 = (float)vs;
     for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
   }
+  mxs += vs * dzs;
+  const double carry_in = (carry && steady) ? carry[(size_t)n * G.ncol + col] : 0.0;
+  // the carry goes back as a uniform shift of the column's values
+  const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
+  if (H > 0.0) mxs += carry_in * ia;
   if (!solve) {
     // the values as they are, plus the carry's shift (tr_bounds has run)
     for (int j = 0; j < nk; ++j) {
@@ -557,13 +570,12 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     bad |= isnan(fin);
     mss += (double)fin * dzs;
   } else {
-    A0[nk * sa] = (float)vs;
-    // FP32 forward sweep
-    float fwd = 0.f;  // the bottom row's cm1 is 0
-    for (int j = 0; j <= nk; ++j) {
-      const float4 lu = L0[j * 32];
-      fwd = (lu.x * A0[j * sa] - lu.y * fwd) * lu.z;
-      S0[j * sa] = fwd;
+    // the surface row of the forward sweep
+    {
+      const float4 lu = L0[nk * 32];
+      A0[nk * sa] = (float)vs;
+      fwd = (lu.x * (float)vs - lu.y * fwd) * lu.z;
+      S0[nk * sa] = fwd;
     }
     // back substitution (FP32), x(j) replacing s(j), and one row behind it
     // the FP64 residual of b - A x for A = dz/dt I + the diffusion operator,
@@ -719,16 +731,12 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   }
   const double area = G.cellarea[c2], ia = 1.0 / area;
   const bool steady = F.eta[c2] == F.oldeta[c2];
-  // the water depth the carry is spread over
-  const int nk = ks - kb;
-  double H = 0.0;
-  for (int j = 0; j <= nk; ++j) H += D0[j * 32];
   const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
   cp_async_wait<0>();
   long long nwarn = 0;
   bool bad = false;  // a NaN among the values this thread stores
   column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
-                            D0, M0, tr, to, area, ia, H, 1.0 / F.dt, cs, carry, steady, nwarn,
+                            D0, M0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn,
                             bad);
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
