@@ -15,7 +15,10 @@ FP64 mass drift of both over the run.
 Multi-GPU (torchrun, one process per GPU): every rank steps its own
 independent basin (a differently seeded copy of the workload), with no
 collective on the data path -- weak scaling; the timing is the max over
-ranks.  Rank 0 prints one JSON line.
+ranks.  With --workload batch8 the eight basins of the multi-basin
+configuration are shared out instead, largest first to the rank with the
+least work (strong scaling: the job is the same eight basins at every N).
+Rank 0 prints one JSON line.
 
 The reference arm (--impl reference) times the reference's own
 model/hd/tracers/tracers.c (compiled unmodified into oracle/_ref, OpenMP
@@ -135,6 +138,16 @@ def dist_init():
     return world, rank, local, pg
 
 
+def sum_over_ranks(pg, x, device):
+    """Sum of one number over the ranks (the whole job's work)."""
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
 def max_over_ranks(pg, x, device):
     if pg is None:
         return x
@@ -178,10 +191,11 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def workload_case(args, seed, sample=False):
-    """The arm's window (sample: the bounded CPU sample of it)."""
+def workload_case(args, seed, sample=False, which=None):
+    """The arm's window (sample: the bounded CPU sample of it; which: the
+    basins of a multi-basin workload this rank steps)."""
     from ems_b200 import synth
-    kw = {}
+    kw = {} if which is None else {"which": which}
     if sample:
         if args.workload in ("batch8", "batch8small"):
             # the eight basins at 1/16 of their horizontal size
@@ -330,8 +344,16 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     mixed = args.precision == "fp32mixed"
-    case = workload_case(args, seed=2048 + rank)
+    shared = args.workload in ("batch8", "batch8small") and world > 1
+    if shared:
+        # the eight basins shared out over the ranks (strong scaling)
+        which = synth.batch_partition(synth.BATCH8, world)[rank]
+        case = workload_case(args, seed=2048, which=which)
+    else:
+        which = None
+        case = workload_case(args, seed=2048 + rank)
     units = case.cell_tracers()
+    job_units = sum_over_ranks(pg, units, dev)  # every rank's work
     host_gb = case.ntr * case.win.sgsiz * 8 / 1e9  # one FP64 copy of all tracers
 
     # the headline arm (timed with clocks sampled), then the plain FP64 arm on
@@ -358,7 +380,7 @@ def main():
             err = max(per)
             rms = float(np.nanmax(d["rms_rel"][0]))
         err = max_over_ranks(pg, err, dev)
-        fp64 = {"value": units * world / (ref["ms_step"] / 1000.0),
+        fp64 = {"value": job_units / (ref["ms_step"] / 1000.0),
                 "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
                 "kernels_ms": {"k_adv64": ref["parts"][1], "k_vd64": ref["parts"][2]},
                 "mass_rel_drift": ref["mass_drift"],
@@ -368,7 +390,7 @@ def main():
                 "steps_compared": arm["nsteps"]}
         ref["step"].close()
 
-    value = units * world / (arm["ms_step"] / 1000.0)
+    value = job_units / (arm["ms_step"] / 1000.0)
     hbm, peak_kind = peaks()
     f64b = not mixed
     # the dominant transport kernel and its roofline
@@ -427,7 +449,8 @@ def main():
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": arm["ms_step"],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "higher_is_better": True, "scaling": "strong" if shared else "weak",
+        "vs_baseline": None,
         "dtype": "f32-mixed" if mixed else "f64", "data": "synthetic",
         "config": {
             "workload": args.workload + ("@" + args.size if args.size else ""), "nx": case.win.nx, "ny": case.win.ny,
@@ -438,13 +461,15 @@ def main():
             "substeps": arm["diag"].nsub, "seed": case.seed,
             "l2": "inputs larger than L2 (%.1f GB of tracers and fields per step)" % (
                 step_bytes / 1e9),
-            "parallelism": "independent basin per GPU" if world > 1 else "single GPU",
+            "parallelism": ("basins shared out over GPUs: %s" % synth.batch_partition(
+                synth.BATCH8, world) if shared else
+                "independent basin per GPU" if world > 1 else "single GPU"),
         },
         "fp64": fp64,
         "mass_rel_drift": arm["mass_drift"],
         "mass_rel_drift_rank_max": arm["mass_drift_rank_max"],
         "clocks": arm["clocks"],
-        "e2e": {"value": units / e2e_s if e2e_s == e2e_s else None, "unit": UNIT,
+        "e2e": {"value": job_units / e2e_s if e2e_s == e2e_s else None, "unit": UNIT,
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "path": "shoc_tr_gpu_step on page-locked host arrays (copies inside the timing)"},
         "gpu_launches": arm["launches"],

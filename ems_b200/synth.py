@@ -443,28 +443,50 @@ BATCH8 = ((128, 128, 20, 4), (256, 256, 26, 8), (384, 256, 31, 12), (512, 512, 3
           (2048, 1024, 60, 32))
 
 
-def build_batch(name, basins, *, seed, scale=1.0, gap=3, nz=60, depth=250.0, **kw):
+def batch_partition(basins, parts):
+    """Basins (indices) of each of `parts` ranks: largest first (cells x
+    tracers), each to the rank with the least work so far."""
+    order = sorted(range(len(basins)), key=lambda b: -np.prod(basins[b], dtype=np.float64))
+    load, out = [0.0] * parts, [[] for _ in range(parts)]
+    for b in order:
+        r = int(np.argmin(load))
+        out[r].append(b)
+        load[r] += float(np.prod(basins[b], dtype=np.float64))
+    return [sorted(o) for o in out]
+
+
+def build_batch(name, basins, *, seed, scale=1.0, gap=3, nz=60, depth=250.0, which=None, **kw):
     """One window holding independent basins side by side, separated by
     `gap` land columns, each with its own seeded bathymetry (its own deepest
     layer count and 30 % land) and tracer count (shoc_tr_opts.ntr2d).  The
     streamfunction vanishes at every coast, so no water or tracer crosses
-    between basins and each steps as it would alone."""
+    between basins and each steps as it would alone.  which: the indices of
+    the basins to build (default all), each with the bathymetry and land it
+    has in the whole batch (the seeded draws of the others are made and
+    dropped)."""
     rng = np.random.default_rng(seed)
     layers = uniform_layers(nz, depth)
     dims = [(max(8, int(round(bx * scale))), max(8, int(round(by * scale))), L, T)
             for bx, by, L, T in basins]
+    keep = list(range(len(dims))) if which is None else sorted(which)
+    # the bathymetry and land draws of every basin, in order
+    draws = []
+    for bx, by, L, T in dims:
+        f = _smooth(rng, by, bx)
+        g = _smooth(rng, by, bx, nmodes=10, kmax=6.0)
+        draws.append((f, g))
+    dims = [dims[b] for b in keep]
+    draws = [draws[b] for b in keep]
     nx = sum(d[0] for d in dims) + gap * (len(dims) + 1)
     ny = max(d[1] for d in dims) + 2 * gap
     bathy = np.full((ny, nx), layers[-2])
     land = np.ones((ny, nx), np.uint8)
     tr_of = np.zeros((ny, nx), np.int32)
     x0 = gap
-    for bx, by, L, T in dims:
-        f = _smooth(rng, by, bx)
+    for (bx, by, L, T), (f, g) in zip(dims, draws):
         dmax = depth * L / nz
         b = -(2.0 + (dmax - 2.0) * f)
         b = np.maximum(b, layers[0])
-        g = _smooth(rng, by, bx, nmodes=10, kmax=6.0)
         ld = (g < np.quantile(g, 0.3)).astype(np.uint8)
         bathy[gap:gap + by, x0:x0 + bx] = _snap_bathy(b, layers)
         land[gap:gap + by, x0:x0 + bx] = ld

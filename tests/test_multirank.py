@@ -40,7 +40,9 @@ def _worker(rank, world, port, q):
                                                  size="", steps=1, warmup=0), r, w)
     # whole-job mass: per-rank masses gathered and summed in rank order
     m = bench.mass_over_ranks(pg, [0.1 * (r + 1), 2.0 * (r + 1)], "cpu")
-    q.put((r, w, t, case.nwet, float(case.tr.sum()), ref is None, m.tolist()))
+    # the whole job's work: every rank's units summed
+    u = bench.sum_over_ranks(pg, 10.0 * (r + 1), "cpu")
+    q.put((r, w, t, case.nwet, float(case.tr.sum()), ref is None, m.tolist(), u))
     pg.barrier()
     pg.destroy_process_group()
 
@@ -56,12 +58,13 @@ def test_two_gloo_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    (r0, w0, t0, n0, s0, none0, m0), (r1, w1, t1, n1, s1, none1, m1) = out
+    (r0, w0, t0, n0, s0, none0, m0, u0), (r1, w1, t1, n1, s1, none1, m1, u1) = out
     assert (r0, r1, w0, w1) == (0, 1, 2, 2)
     assert t0 == t1 == 11.0            # max over ranks
     assert s0 != s1                    # each rank its own seeded basin
     assert none1 and (none0 is False)  # only rank 0 runs the reference arm
     assert m0 == m1 == [0.1 + 0.2, 6.0]   # the same bits on every rank
+    assert u0 == u1 == 30.0
 
 
 def test_compensated_sum_of_rank_masses():
@@ -71,3 +74,22 @@ def test_compensated_sum_of_rank_masses():
     import bench
     got = bench.compensated_sum([[1e16, 3.0], [1.0, 4.0], [-1e16, 5.0]])
     assert got.tolist() == [1.0, 12.0]
+
+
+def test_batch_basins_shared_out():
+    """--workload batch8 over N ranks: every basin on exactly one rank,
+    largest first to the least-loaded rank; a rank's subset keeps each
+    basin's bathymetry and land as in the whole batch."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    from ems_b200 import synth
+    for n in (1, 2, 3, 4, 8):
+        parts = synth.batch_partition(synth.BATCH8, n)
+        got = sorted(b for p in parts for b in p)
+        assert got == list(range(8))
+        loads = [sum(float(np.prod(synth.BATCH8[b])) for b in p) for p in parts]
+        assert max(loads) <= max(float(np.prod(b)) for b in synth.BATCH8) + min(loads) + 1e-9
+    whole = synth.make("batch8small", seed=5)
+    sub = synth.make("batch8small", seed=5, which=[1, 6])
+    assert sub.basins == [whole.basins[1], whole.basins[6]]
+    assert sub.cell_tracers() < whole.cell_tracers()
