@@ -12,6 +12,10 @@ reference's tracers.c on the parity cases, so it stands in for the FP64
 oracle at sizes the CPU cannot run for many steps.
 
   python -m ems_b200.accuracy --workload stiff2048 --steps 1000 --every 100
+
+--worst also reports, per tracer, where its largest difference is (layer,
+column, the column's bottom layer, the cell's velocities and Kz): the two
+paths' tracers are copied to the host once, at the end.
 """
 import argparse
 import json
@@ -22,9 +26,29 @@ import numpy as np
 from . import gpu, synth
 
 
-def compare(case, steps, every, device=0, log=None):
+def worst_cells(case, x64, x32):
+    """Per tracer: the wet cell of the largest |x32 - x64| and what is there."""
+    win = case.win
+    c = win.wet_cells()
+    col = {int(v): i for i, v in enumerate(win.w2_t[1:win.geom.b2_t + 1], 1)}
+    out = []
+    for n in range(case.ntr):
+        e = np.abs(x32[n, c] - x64[n, c])
+        i = int(np.argmax(e))
+        cell = int(c[i])
+        cc = col[int(win.m2d[cell])]
+        out.append({"tracer": n, "max_rel": float(e[i] / np.abs(x64[n, c]).max()),
+                    "k": int(win.s2k[cell]), "i": int(win.s2i[cell]), "j": int(win.s2j[cell]),
+                    "k_bottom": int(win.s2k[win.bot_t[cc]]), "x64": float(x64[n, cell]),
+                    "u1": float(case.u1[cell]), "u2": float(case.u2[cell]),
+                    "w": float(case.w[cell]), "Kz": float(case.Kz[cell])})
+    return out
+
+
+def compare(case, steps, every, device=0, log=None, worst=None):
     """Per-tracer errors of FP32-mixed vs FP64 after every `every` steps
-    (compared on the device, shoc_tr_gpu_compare: no tracer leaves HBM)."""
+    (compared on the device, shoc_tr_gpu_compare: no tracer leaves HBM).
+    worst: a list that receives worst_cells() after the last step."""
     s64 = gpu.TracerStep(case, precision=gpu.FP64, device=device)
     s32 = gpu.TracerStep(case, precision=gpu.FP32_MIXED, device=device)
     s64.start()
@@ -52,6 +76,8 @@ def compare(case, steps, every, device=0, log=None):
             log("step %d: max rel %.3g, RMS rel %.3g, mass drift fp64 %.3g, fp32-mixed %.3g" % (
                 done, mx.max(), rms.max(), max(row["mass_drift_fp64"]),
                 max(row["mass_drift_fp32mixed"])))
+    if worst is not None:
+        worst.extend(worst_cells(case, s64.download(), s32.download()))
     s64.close()
     s32.close()
     return rows
@@ -65,16 +91,23 @@ def main():
     p.add_argument("--seed", type=int, default=2048)
     p.add_argument("--size", default="", help="NXxNY: the workload at another size")
     p.add_argument("--json", default="")
+    p.add_argument("--worst", action="store_true",
+                   help="report where each tracer's largest difference is")
     a = p.parse_args()
     kw = {}
     if a.size:
         kw["nx"], kw["ny"] = (int(v) for v in a.size.split("x"))
     case = synth.make(a.workload, seed=a.seed, **kw)
     t0 = time.time()
-    rows = compare(case, a.steps, a.every, log=lambda s: print(s, flush=True))
+    worst = [] if a.worst else None
+    rows = compare(case, a.steps, a.every, log=lambda s: print(s, flush=True), worst=worst)
     out = {"workload": a.workload + ("@" + a.size if a.size else ""), "seed": a.seed,
            "steps": a.steps, "tracers": case.ntr, "wet_cells": case.nwet,
            "seconds": time.time() - t0, "checkpoints": rows}
+    if worst is not None:
+        out["worst"] = worst
+        for w in worst:
+            print("worst", json.dumps(w))
     if a.json:
         with open(a.json, "w") as f:
             json.dump(out, f)
