@@ -70,18 +70,17 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                              fzs, any_hd);
   }
   if (ev) cudaEventRecord(ev[1], st);
-  const int nchunk = (T.nslot + vd_nw - 1) / vd_nw;
   const dim3 blk(32, vd_nw);
   for (int i = 0; i < Tl.nclass; i++) {
     const int t0 = Tl.ctile[i], nt = Tl.ctile[i + 1] - t0, kbase = Tl.cbase[i];
     if (nt <= 0) continue;
     const size_t smem = vd32_smem(G.nz - kbase, vd_nw);
     if (last)
-      k_vd32<true><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd,
-                                                   carry, fzs, vd_nw, nchunk, t0, kbase);
+      k_vd32<true><<<nt, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd, carry,
+                                          fzs, vd_nw, t0, kbase);
     else
-      k_vd32<false><<<nt * nchunk, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout,
-                                                    rnd, carry, fzs, vd_nw, nchunk, t0, kbase);
+      k_vd32<false><<<nt, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd, carry,
+                                           fzs, vd_nw, t0, kbase);
   }
   if (ev) cudaEventRecord(ev[2], st);
 }

@@ -1046,7 +1046,8 @@ void drop_graphs(shoc_tr_gpu *h) {
 // effect at the next step).
 int apply_tuning(shoc_tr_gpu *h, const shoc_tr_tuning &t) {
   const bool f32 = h->esize == sizeof(float);
-  if (t.tracers_per_block < 1 || t.tracers_per_block > 8) return SHOC_TR_EUNSUPPORTED;
+  if (t.tracers_per_block < 1 || t.tracers_per_block > (f32 ? kVd32MaxWarps : 8))
+    return SHOC_TR_EUNSUPPORTED;
   if (vd_smem(h, h->nz, t.tracers_per_block) > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
   if (t.fused) {
     const int ti = tile_index(t.tile_x);
@@ -1455,9 +1456,26 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   // tiling: tracers per block
   int tw = 8;
-  {
-    // tracers per column-kernel block: two blocks per SM at full depth,
-    // balanced chunks
+  if (f32p) {
+    // k_vd32 warps per block: the most warps per SM at full depth (blocks
+    // per SM x warps per block, as shared memory allows), no more warps than
+    // tracers, then the fewest warps that need the same number of rounds
+    // over the tracers
+    int best = 1, bw = 0;
+    for (int nw = 1; nw <= std::min(kVd32MaxWarps, std::max(h->nslot, 1)); nw++) {
+      const size_t b = vd_smem(h, g->nz, nw);
+      const int per_sm = b <= 227 * 1024 ? (int)std::min<size_t>(8, 233472 / (b + 1024)) : 0;
+      if (per_sm * nw > bw) {
+        bw = per_sm * nw;
+        best = nw;
+      }
+    }
+    tw = best;
+    const int rounds = (h->nslot + tw - 1) / std::max(tw, 1);
+    if (rounds > 0) tw = std::max(1, (h->nslot + rounds - 1) / rounds);
+  } else {
+    // tracers per k_vd64 block: two blocks per SM at full depth, balanced
+    // chunks
     while (tw > 1 && vd_smem(h, g->nz, tw) > 113 * 1024) tw--;
     int nch = (h->nslot + tw - 1) / std::max(tw, 1);
     if (nch > 0) tw = (h->nslot + nch - 1) / nch;
@@ -2970,7 +2988,10 @@ int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tu
   // tile widths and phase-B warps for the fused one (FP32-mixed, where it fits)
   std::vector<shoc_tr_tuning> cand;
   shoc_tr_tuning base = current_tuning(h);
-  for (int tw : {2, 3, 4, 5, 6, 8}) {
+  const std::vector<int> tws = h->esize == sizeof(float)
+                                   ? std::vector<int>{2, 4, 6, 8, 12, 16}
+                                   : std::vector<int>{2, 3, 4, 5, 6, 8};
+  for (int tw : tws) {
     shoc_tr_tuning c = base;
     c.fused = 0;
     c.tracers_per_block = tw;

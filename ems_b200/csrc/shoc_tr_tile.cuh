@@ -642,6 +642,10 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
 // ---------------------------------------------------------------------------
 // k_vd32
 
+// k_vd32: a block is one tile of 32 columns and nw warps (at most
+// kVd32MaxWarps); the tile's tracer-independent column arrays are staged
+// once and each warp steps its share of the tracers through them.
+constexpr int kVd32MaxWarps = 16;
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
 // LU float4[nd][32], thicknesses and sub-diagonals double[nd][32] x 2,
 // colC int[nd][32], A, S float[nd][nw][32]
@@ -650,15 +654,15 @@ inline size_t vd32_smem(int nd, int nw) {
 }
 
 template <bool LAST>
-__global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSet T,
-                                              SubStep ss, Tile Tl,
-                                              const float4 *__restrict__ lu32,
-                                              const float *__restrict__ tri,
-                                              float *__restrict__ tro,
-                                              const float *__restrict__ rsi,
-                                              double *__restrict__ carry,
-                                              const double *__restrict__ fzs, int nw,
-                                              int nchunk, int tile0, int kbase) {
+__global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work W, Opt O,
+                                                             TrSet T, SubStep ss, Tile Tl,
+                                                             const float4 *__restrict__ lu32,
+                                                             const float *__restrict__ tri,
+                                                             float *__restrict__ tro,
+                                                             const float *__restrict__ rsi,
+                                                             double *__restrict__ carry,
+                                                             const double *__restrict__ fzs,
+                                                             int nw, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
   // the arrays hold layers kbase .. nz-1 (every column of this launch's
   // tiles starts at or above kbase), row r = layer - kbase
@@ -671,18 +675,18 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   float *Sv = A + nd * nw * 32;                           // [nd][nw][32]
 
   const int lane = threadIdx.x, wy = threadIdx.y;
-  const int tile = tile0 + blockIdx.x / nchunk, chunk = blockIdx.x % nchunk;
+  const int tile = tile0 + blockIdx.x;
   const int col = Tl.vdcol[tile * 32 + lane];
-  const int slot = chunk * nw + wy;
   const int sa = nw * 32;
 
   const TileCol tc = tile_column(G, W, Tl, col);
   bool act = tc.act;
   if (act && tc.kb < kbase) {  // not in this launch's depth class
     act = false;
-    if (chunk == 0 && wy == 0) atomicOr(W.status, ST_GEOM);
+    if (wy == 0) atomicOr(W.status, ST_GEOM);
   }
   const int kb = tc.kb, ks = tc.ks, cbot = tc.cbot, c2 = tc.c2;
+  // the tile's tracer-independent column arrays, once for every tracer
   const int kmin = __reduce_min_sync(0xffffffffu, act ? kb : nz);
   for (int k = kmin + wy; k < nz; k += nw) {
     const int c = (act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
@@ -697,47 +701,49 @@ __global__ void __launch_bounds__(256) k_vd32(Geo G, Flow F, Work W, Opt O, TrSe
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  if (!act || slot >= T.nslot) return;
+  if (!act) return;
 
-  const int n = T.slot_tr[slot];
-  if (n >= G.colntr[col]) return;  // tracer not carried in this column
-  const int tf = T.trf[n];
-  const bool tbdy = (tf & TR_TBDY) != 0;
-  const bool adv = tbdy && (tf & TR_ADV);
-  const bool vdf = LAST && (tf & TR_VDIFF);
-  const float *tr = tri + (size_t)n * G.S;
-  float *to = tro + (size_t)n * G.S;
   float *const A0 = A + wy * 32 + lane + (kb - kbase) * sa;
   float *const S0 = Sv + wy * 32 + lane + (kb - kbase) * sa;
   const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const double *const D0 = DZ + (kb - kbase) * 32 + lane;
   const double *const M0 = CM + (kb - kbase) * 32 + lane;
-  // the column's values: advection results and their rounding residuals
-  // (advected tracers, residuals into the Thomas storage until the sweep)
-  // or the old values (the rest)
-  {
-    const float *src = tbdy ? to : tr;
-    for (int j = 0; j < nz - kb; ++j) cp_async4(&A0[j * sa], src + C0[j * 32]);
-    if (tbdy) {
-      const float *rs = rsi + (size_t)n * G.S;
-      for (int j = 0; j < nz - kb; ++j) cp_async4(&S0[j * sa], rs + C0[j * 32]);
-    }
-    cp_async_commit();
-  }
-  {  // sediment ghost (tracers.c:827-830)
-    const int sed = G.zm1[cbot];
-    to[sed] = tbdy ? tr[cbot] : tr[sed];
-  }
   const double area = G.cellarea[c2], ia = 1.0 / area;
   const bool steady = F.eta[c2] == F.oldeta[c2];
-  const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
-  cp_async_wait<0>();
+  const int ntc = G.colntr[col];
+  const int sed = G.zm1[cbot];
   long long nwarn = 0;
   bool bad = false;  // a NaN among the values this thread stores
-  column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
-                            D0, M0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn,
-                            bad);
+  // warp wy takes the tracers wy, wy + nw, ... of the column
+  for (int slot = wy; slot < T.nslot; slot += nw) {
+    const int n = T.slot_tr[slot];
+    if (n >= ntc) continue;  // tracer not carried in this column
+    const int tf = T.trf[n];
+    const bool tbdy = (tf & TR_TBDY) != 0;
+    const bool adv = tbdy && (tf & TR_ADV);
+    const bool vdf = LAST && (tf & TR_VDIFF);
+    const float *tr = tri + (size_t)n * G.S;
+    float *to = tro + (size_t)n * G.S;
+    // the column's values: advection results and their rounding residuals
+    // (advected tracers, residuals into the Thomas storage until the sweep)
+    // or the old values (the rest)
+    {
+      const float *src = tbdy ? to : tr;
+      for (int j = 0; j < nz - kb; ++j) cp_async4(&A0[j * sa], src + C0[j * 32]);
+      if (tbdy) {
+        const float *rs = rsi + (size_t)n * G.S;
+        for (int j = 0; j < nz - kb; ++j) cp_async4(&S0[j * sa], rs + C0[j * 32]);
+      }
+      cp_async_commit();
+    }
+    to[sed] = tbdy ? tr[cbot] : tr[sed];  // sediment ghost (tracers.c:827-830)
+    const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
+    cp_async_wait<0>();
+    column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
+                              D0, M0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn,
+                              bad);
+  }
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
 }

@@ -248,7 +248,8 @@ int shoc_tr_gpu_set_tiling(shoc_tr_gpu *h, int cols_per_block, int tracers_per_b
 typedef struct {
   int fused;             /* FP32-mixed: 1 one fused launch per sub-step (k_step32),
                             0 the advection + column kernel pair */
-  int tracers_per_block; /* column kernel (k_vd32 / k_vd64): tracers per block, 1..8 */
+  int tracers_per_block; /* column kernel: tracers per k_vd64 block (1..8), or warps per
+                            k_vd32 block, each stepping its share of the tracers (1..16) */
   int tile_x;            /* k_step32: tile width along i (8, 16, 32; 32 / tile_x
                             columns along j) */
   int phase_b_warps;     /* k_step32: warps of its column phase */
@@ -265,8 +266,8 @@ int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t);
  * candidate configuration, times the transport kernels with CUDA events,
  * puts the state back (a device copy taken before the trials: the tracers,
  * surface vectors and mass carry are as they were) and keeps the fastest.
- * Candidates: 2..8 tracers per block of the column kernel; for FP32-mixed
- * also the fused sub-step with tile widths 8, 16, 32 and the most and half
+ * Candidates: 2..8 tracers per k_vd64 block, or 2..16 warps per k_vd32
+ * block; for FP32-mixed also the fused sub-step with tile widths 8, 16, 32 and the most and half
  * the most phase-B warps its shared memory allows.  With use_cache != 0 the
  * choice is looked up in and saved to a file keyed by the GPU model and the
  * window's configuration (sizes, tracers, precision, scheme, diffusion),
