@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--cpu-sample", default="512x256")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="keep the library's default launch configuration")
     return p.parse_args()
 
 
@@ -288,6 +290,11 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     from ems_b200 import gpu
     step = gpu.TracerStep(case, precision=prec, device=local)
     step.start()
+    tuning, cached = None, None
+    if not args.no_autotune:
+        # the autotuner's trial steps start from a device copy of the state
+        # and put it back (untimed); its choice is cached per GPU and window
+        tuning, cached = step.autotune_ex(2)
     own0 = step.mass()
     m0 = mass_over_ranks(pg, own0, dev)
     stream = torch.cuda.ExternalStream(step.stream(), device=dev)
@@ -323,7 +330,8 @@ def time_arm(case, prec, local, args, pg, dev, clocks=None):
     own = float(np.max(np.abs(own1 - own0) / np.maximum(np.abs(own0), 1e-300)))
     return dict(step=step, ms_step=ms_step, launches=launches, clocks=clk, diag=diag,
                 parts=parts, mass_drift=drift, mass_drift_rank_max=max_over_ranks(pg, own, dev),
-                nsteps=max(args.warmup, 3) + 2 * args.steps)
+                nsteps=max(args.warmup, 3) + 2 * args.steps,
+                tuning=dict(tuning, cached=cached) if tuning else None)
 
 
 def main():
@@ -380,7 +388,7 @@ def main():
             err = max(per)
             rms = float(np.nanmax(d["rms_rel"][0]))
         err = max_over_ranks(pg, err, dev)
-        fp64 = {"value": job_units / (ref["ms_step"] / 1000.0),
+        fp64 = {"value": job_units / (ref["ms_step"] / 1000.0), "tuning": ref["tuning"],
                 "ms_per_step": ref["ms_step"], "transport_ms": ref["parts"][0],
                 "kernels_ms": {"k_adv64": ref["parts"][1], "k_vd64": ref["parts"][2]},
                 "mass_rel_drift": ref["mass_drift"],
@@ -459,6 +467,7 @@ def main():
             "basins": [list(b) for b in getattr(case, "basins", [])] or None,
             "columns": case.win.ncol, "precision": args.precision, "dt": case.dt,
             "substeps": arm["diag"].nsub, "seed": case.seed,
+            "tuning": arm["tuning"],
             "l2": "inputs larger than L2 (%.1f GB of tracers and fields per step)" % (
                 step_bytes / 1e9),
             "parallelism": ("basins shared out over GPUs: %s" % synth.batch_partition(

@@ -59,8 +59,8 @@ struct Fused {
 
 // shared memory of k_step32 (bytes) for columns of at most nd layers, nwb
 // phase-B warps, ntb advected tracers and reduction groups of ngrp tracers:
-// LU float4 [nd][32], thicknesses and sub-diagonals double [nd][32] x 2,
-// cells int [nd][32], a union of the phase-B column arrays float
+// LU float4 [nd][32], thicknesses double [nd][32], cells int [nd][32], a
+// union of the phase-B column arrays float
 // [2][nwb][nd][32] with the phase-A contributions double [8][ngrp][32]
 // followed by its stencil double buffer float [2][13][256], the
 // accumulators double [ntb][32] x 3, and the surface layer of each lane
@@ -74,7 +74,7 @@ __host__ __device__ inline size_t fused_union(int nd, int nwb, int ngrp) {
   return a > r ? a : r;
 }
 inline size_t fused_smem(int nd, int nwb, int ntb, int ngrp) {
-  return (size_t)nd * 32 * (16 + 8 + 8) + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
+  return (size_t)nd * 32 * (16 + 8) + (size_t)nd * 32 * 4 + fused_union(nd, nwb, ngrp) +
          (size_t)ntb * 32 * (8 + 8 + 8) + 32 * 4;
 }
 
@@ -92,8 +92,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
   const int nz = G.nz, nd = nz - kbase, nwb = Fu.nwb, ntb = T.ntb, ngrp = Fu.ngrp;
   float4 *LU = reinterpret_cast<float4 *>(smem);                  // [nd][32]
   double *DZ = reinterpret_cast<double *>(LU + nd * 32);          // [nd][32]
-  double *CM = DZ + nd * 32;                                      // [nd][32]
-  int *colC = reinterpret_cast<int *>(CM + nd * 32);              // [nd][32]
+  int *colC = reinterpret_cast<int *>(DZ + nd * 32);              // [nd][32]
   unsigned char *uni = reinterpret_cast<unsigned char *>(colC + nd * 32);
   float *A = reinterpret_cast<float *>(uni);                      // [nwb][nd][32]
   float *Sv = A + nwb * nd * 32;                                  // [nwb][nd][32]
@@ -118,10 +117,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     const int c = (tc.act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
     const int r = k - kbase;
     colC[r * 32 + lane] = c;
-    if (LAST && c && k <= ks) {
-      cp_async16(&LU[r * 32 + lane], &W.lu32[c]);
-      cp_async8(&CM[r * 32 + lane], &W.vd_cm1[c]);
-    }
+    if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &W.lu32[c]);
     if (c && k <= ks) cp_async8(&DZ[r * 32 + lane], &W.dz[c]);
   }
   cp_async_commit();
@@ -303,7 +299,6 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
     float *const A0 = A + w * nd * 32 + lane + (kb - kbase) * 32;
     float *const S0 = Sv + w * nd * 32 + lane + (kb - kbase) * 32;
     const double *const D0 = DZ + (kb - kbase) * 32 + lane;
-    const double *const M0 = CM + (kb - kbase) * 32 + lane;
     const bool steady = F.eta[c2] == F.oldeta[c2];
     const int *const C0 = colC + (kb - kbase) * 32 + lane;
     const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
@@ -337,7 +332,7 @@ __global__ void __launch_bounds__(kFusedThreads, 2)
       bool bad = false;
       cp_async_wait<0>();
       column_finish<LAST, false>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, 32, L0,
-                                 C0, D0, M0, tr, to, area, ia, idt, cs, Fu.carry, steady,
+                                 C0, D0, tr, to, area, ia, idt, cs, Fu.carry, steady,
                                  nwarn, bad);
       if (bad) nstat |= ST_NAN;
     }

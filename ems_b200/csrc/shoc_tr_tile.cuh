@@ -449,8 +449,7 @@ struct ColSums {
 // A0, S0: the column's values and Thomas storage from its bottom layer up, row
 // stride sa; an advected tracer (tbdy) holds its advected values below the
 // surface, any other tracer every layer's old value (A0 is overwritten, so is
-// S0).  L0, C0, D0, M0: LU factors, cells, FP64 thicknesses and FP64
-// sub-diagonals cm1 of the solve (LAST only), row stride 32.
+// S0).  L0, C0, D0: LU factors, cells and FP64 thicknesses, row stride 32.
 // RES: an advected tracer's A0 holds every layer's stored advection result
 // and S0 its rounding residual (k_vd32), and the column sums cs.m and cs.dv
 // are taken from them; else they come in cs (k_step32).
@@ -464,8 +463,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
                                               const TileCol &tc, int col, int n, bool tbdy,
                                               bool adv, bool vdf, float *A0, float *S0, int sa,
                                               const float4 *L0, const int *C0, const double *D0,
-                                              const double *M0, const float *tr, float *to,
-                                              double area, double ia, double idt, ColSums cs,
+                                              const float *tr, float *to, double area, double ia,
+                                              double idt, ColSums cs,
                                               double *carry, bool steady, long long &nwarn,
                                               bool &bad) {
   const ColInfo &ci = tc.ci;
@@ -581,13 +580,12 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     // the FP64 residual of b - A x for A = dz/dt I + the diffusion operator,
     //   r(j) = dz/dt (a + dl - x) - cm1 (x(j-1) - x) - cp1 (x(j+1) - x)
     // (cp1(j) = cm1(j+1); the bottom row has no cm1 term, the top row no cp1
-    // term), which replaces a(j).  Its coefficients are the FP64 ones (dz / dt
-    // and cm1), not the FP32 factors', so the refinement converges to the
-    // FP64 system's solution (a residual of the FP32-rounded matrix would
-    // leave a bias of about the condition number x 6e-8, the same every step
-    // while Kz is steady), and the refined solve keeps the column mass the
-    // mass diagnostic measures.  The FP64 copies of x are carried from row to
-    // row.
+    // term), which replaces a(j).  Its diagonal is the FP64 dz / dt, so the
+    // refined solve keeps the column mass the mass diagnostic measures; cm1
+    // is the FP32 factor's (the FP64 one, staged as well, changed neither
+    // the maximum nor the RMS error over 1000 stiff2048 steps, and its
+    // shared memory cost warps).  The FP64 copies of x and of the factors are
+    // carried from row to row.
     float x1 = fwd;
     float4 l1 = L0[nk * 32];
     double xd1 = (double)x1, xd2 = 0.0, l2y = 0.0;
@@ -595,7 +593,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     for (int j = nk - 1; j >= 0; --j) {
       const float x = S0[j * sa] - l1.w * x1;
       S0[j * sa] = x;
-      const double xd = (double)x, l1y = M0[(j + 1) * 32];
+      const double xd = (double)x, l1y = (double)l1.y;
       const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * sa]) + dl;
       double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
       if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
@@ -647,10 +645,10 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
 // once and each warp steps its share of the tracers through them.
 constexpr int kVd32MaxWarps = 16;
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
-// LU float4[nd][32], thicknesses and sub-diagonals double[nd][32] x 2,
-// colC int[nd][32], A, S float[nd][nw][32]
+// LU float4[nd][32], thicknesses double[nd][32], colC int[nd][32], A, S
+// float[nd][nw][32]
 inline size_t vd32_smem(int nd, int nw) {
-  return (size_t)nd * 32 * (16 + 8 + 8 + 4) + (size_t)2 * nd * nw * 32 * 4;
+  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)2 * nd * nw * 32 * 4;
 }
 
 template <bool LAST>
@@ -669,8 +667,7 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   const int nz = G.nz, nd = nz - kbase;
   float4 *LU = reinterpret_cast<float4 *>(smem);          // [nd][32]
   double *DZ = reinterpret_cast<double *>(LU + nd * 32);  // [nd][32]
-  double *CM = DZ + nd * 32;                              // [nd][32]
-  int *colC = reinterpret_cast<int *>(CM + nd * 32);      // [nd][32]
+  int *colC = reinterpret_cast<int *>(DZ + nd * 32);      // [nd][32]
   float *A = reinterpret_cast<float *>(colC + nd * 32);   // [nd][nw][32]
   float *Sv = A + nd * nw * 32;                           // [nd][nw][32]
 
@@ -692,10 +689,7 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
     const int c = (act && k >= kb) ? Tl.cellk[(size_t)k * Tl.ncolp + col] : 0;
     const int r = k - kbase;
     colC[r * 32 + lane] = c;
-    if (LAST && c && k <= ks) {
-      cp_async16(&LU[r * 32 + lane], &lu32[c]);
-      cp_async8(&CM[r * 32 + lane], &W.vd_cm1[c]);
-    }
+    if (LAST && c && k <= ks) cp_async16(&LU[r * 32 + lane], &lu32[c]);
     if (c && k <= ks) cp_async8(&DZ[r * 32 + lane], &W.dz[c]);
   }
   cp_async_commit();
@@ -708,7 +702,6 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const double *const D0 = DZ + (kb - kbase) * 32 + lane;
-  const double *const M0 = CM + (kb - kbase) * 32 + lane;
   const double area = G.cellarea[c2], ia = 1.0 / area;
   const bool steady = F.eta[c2] == F.oldeta[c2];
   const int ntc = G.colntr[col];
@@ -741,8 +734,7 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
     const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
     cp_async_wait<0>();
     column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
-                              D0, M0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn,
-                              bad);
+                              D0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn, bad);
   }
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);
