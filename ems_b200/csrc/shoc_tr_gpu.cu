@@ -1456,26 +1456,11 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<double>(h, &h->fzs64, nullptr, (size_t)ntr * ncol));
   // tiling: tracers per block
   int tw = 8;
-  if (f32p) {
-    // k_vd32 warps per block: the most warps per SM at full depth (blocks
-    // per SM x warps per block, as shared memory allows), no more warps than
-    // tracers, then the fewest warps that need the same number of rounds
-    // over the tracers
-    int best = 1, bw = 0;
-    for (int nw = 1; nw <= std::min(kVd32MaxWarps, std::max(h->nslot, 1)); nw++) {
-      const size_t b = vd_smem(h, g->nz, nw);
-      const int per_sm = b <= 227 * 1024 ? (int)std::min<size_t>(8, 233472 / (b + 1024)) : 0;
-      if (per_sm * nw > bw) {
-        bw = per_sm * nw;
-        best = nw;
-      }
-    }
-    tw = best;
-    const int rounds = (h->nslot + tw - 1) / std::max(tw, 1);
-    if (rounds > 0) tw = std::max(1, (h->nslot + rounds - 1) / rounds);
-  } else {
-    // tracers per k_vd64 block: two blocks per SM at full depth, balanced
-    // chunks
+  {
+    // tracers (k_vd64) or warps (k_vd32) per column-kernel block: two
+    // blocks per SM at full depth, balanced rounds over the tracers (on
+    // stiff2048 two blocks of 4 warps beat one block of 12: 9.4 against
+    // 11.5 ms for k_vd32)
     while (tw > 1 && vd_smem(h, g->nz, tw) > 113 * 1024) tw--;
     int nch = (h->nslot + tw - 1) / std::max(tw, 1);
     if (nch > 0) tw = (h->nslot + nch - 1) / nch;
@@ -2989,7 +2974,7 @@ int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tu
   std::vector<shoc_tr_tuning> cand;
   shoc_tr_tuning base = current_tuning(h);
   const std::vector<int> tws = h->esize == sizeof(float)
-                                   ? std::vector<int>{2, 4, 6, 8, 12, 16}
+                                   ? std::vector<int>{2, 3, 4, 5, 6, 8, 12, 16}
                                    : std::vector<int>{2, 3, 4, 5, 6, 8};
   for (int tw : tws) {
     shoc_tr_tuning c = base;
