@@ -36,8 +36,9 @@ void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F
 cudaError_t tile32_set_smem_attr() {
   cudaError_t e = cudaSuccess;
   const int a = (int)kAdvSmem;
-  const cudaError_t r[10] = {
-      attr(k_vd32<true>),              attr(k_vd32<false>),
+  const cudaError_t r[12] = {
+      attr(k_vd32<true, false>),       attr(k_vd32<false, false>),
+      attr(k_vd32<true, true>),        attr(k_vd32<false, true>),
       attr(k_adv32<true, true, 1>, a), attr(k_adv32<true, true, 2>, a),
       attr(k_adv32<true, false, 1>, a), attr(k_adv32<true, false, 2>, a),
       attr(k_adv32<false, true, 1>, a), attr(k_adv32<false, true, 2>, a),
@@ -51,8 +52,8 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
-                    double *carry, double *fzs, int vd_nw, int any_hd, int adv_flags,
-                    cudaEvent_t *ev) {
+                    double *carry, double *fzs, int vd_nw, int vd_pf, int any_hd,
+                    int adv_flags, cudaEvent_t *ev) {
   if (ev) cudaEventRecord(ev[0], st);
   if (T.ntb > 0 && Tl.nwet > 0) {
     const int grid = (Tl.nwet + kAdv32Block - 1) / kAdv32Block;
@@ -74,13 +75,11 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
   for (int i = 0; i < Tl.nclass; i++) {
     const int t0 = Tl.ctile[i], nt = Tl.ctile[i + 1] - t0, kbase = Tl.cbase[i];
     if (nt <= 0) continue;
-    const size_t smem = vd32_smem(G.nz - kbase, vd_nw);
-    if (last)
-      k_vd32<true><<<nt, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd, carry,
-                                          fzs, vd_nw, t0, kbase);
-    else
-      k_vd32<false><<<nt, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd, carry,
-                                           fzs, vd_nw, t0, kbase);
+    const size_t smem = vd32_smem(G.nz - kbase, vd_nw, vd_pf != 0);
+    auto kern = last ? (vd_pf ? k_vd32<true, true> : k_vd32<true, false>)
+                     : (vd_pf ? k_vd32<false, true> : k_vd32<false, false>);
+    kern<<<nt, blk, smem, st>>>(G, F, W, O, T, ss, Tl, W.lu32, tin, tout, rnd, carry, fzs, vd_nw,
+                                t0, kbase);
   }
   if (ev) cudaEventRecord(ev[2], st);
 }

@@ -114,6 +114,7 @@ struct shoc_tr_gpu {
   int graph_nsub = -1;
   // tiling
   int tw = 8;
+  bool vd_pf = false;  // k_vd32 stages the next tracer's column during the solve
   // profiling
   bool profile = false;
   struct ProfEv {
@@ -847,7 +848,7 @@ __global__ void k_halo_unpack(TR *tra, TR *trb, int S, int ntr, const int *cells
 
 // shared memory of the column kernel of the handle's precision
 size_t vd_smem(const shoc_tr_gpu *h, int nd, int nw) {
-  return h->esize == sizeof(float) ? vd32_smem(nd, nw) : vd64_smem(nd, nw);
+  return h->esize == sizeof(float) ? vd32_smem(nd, nw, h->vd_pf) : vd64_smem(nd, nw);
 }
 
 // Static tables of the column-tile kernel: the cell of every column at every
@@ -1048,7 +1049,10 @@ int apply_tuning(shoc_tr_gpu *h, const shoc_tr_tuning &t) {
   const bool f32 = h->esize == sizeof(float);
   if (t.tracers_per_block < 1 || t.tracers_per_block > (f32 ? kVd32MaxWarps : 8))
     return SHOC_TR_EUNSUPPORTED;
-  if (vd_smem(h, h->nz, t.tracers_per_block) > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
+  if (t.prefetch && !f32) return SHOC_TR_EUNSUPPORTED;
+  const size_t vb = f32 ? vd32_smem(h->nz, t.tracers_per_block, t.prefetch != 0)
+                        : vd64_smem(h->nz, t.tracers_per_block);
+  if (vb > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
   if (t.fused) {
     const int ti = tile_index(t.tile_x);
     if (!f32 || !h->fnwb_max || ti < 0 || !h->ftile[ti].tcol) return SHOC_TR_EUNSUPPORTED;
@@ -1058,6 +1062,7 @@ int apply_tuning(shoc_tr_gpu *h, const shoc_tr_tuning &t) {
     if (rc) return rc;
   }
   h->tw = t.tracers_per_block;
+  h->vd_pf = t.prefetch != 0;
   h->fused = t.fused != 0;
   if (h->fused) {
     const auto &ft = h->ftile[tile_index(t.tile_x)];
@@ -1078,6 +1083,7 @@ shoc_tr_tuning current_tuning(const shoc_tr_gpu *h) {
   t.tracers_per_block = h->tw;
   t.tile_x = h->fused ? h->fu.tx : 8;
   t.phase_b_warps = h->fused ? h->fu.nwb : h->fnwb_max;
+  t.prefetch = h->vd_pf ? 1 : 0;
   return t;
 }
 
@@ -1771,7 +1777,7 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
         const Tile tl = vd_classes(h, tw);
         tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
                        h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->rnd,
-                       h->fu.carry, h->fzs64, tw,
+                       h->fu.carry, h->fzs64, tw, h->vd_pf ? 1 : 0,
                        h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
         if (prof) {  // pairs share events; sync destroys each event once
           h->ev.push_back({0, ev[0], ev[2]});
@@ -2834,7 +2840,7 @@ int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t) {
 namespace {
 
 // The autotuner's cache: one line per GPU model and window configuration,
-//   <key> <fused> <tracers_per_block> <tile_x> <phase_b_warps> <ms>
+//   <key> <fused> <tracers_per_block> <tile_x> <phase_b_warps> <prefetch> <ms>
 // in the file SHOC_TR_TUNE_CACHE names (default
 // $HOME/.cache/shoc_tr_gpu/tuning.txt; "off": none).
 std::string tune_cache_path() {
@@ -2852,7 +2858,7 @@ std::string tune_key(const shoc_tr_gpu *h) {
   for (char &c : name)
     if (c == ' ' || c == '\t') c = '_';
   char buf[512];
-  snprintf(buf, sizeof buf, "v1|%s|sm%d%d|S%d|C%d|Z%d|N%d|B%d|P%d|A%d|U%d|F%d|H%d|V%d",
+  snprintf(buf, sizeof buf, "v2|%s|sm%d%d|S%d|C%d|Z%d|N%d|B%d|P%d|A%d|U%d|F%d|H%d|V%d",
            name.c_str(), p.major, p.minor, h->S, h->ncol, h->nz, h->ntr, h->T.ntb, h->precision,
            h->O.trasc, h->O.ultimate, h->adv_flags, h->any_hdiff ? 1 : 0, h->any_vdiff ? 1 : 0);
   return std::string(buf);
@@ -2868,8 +2874,8 @@ bool tune_cache_get(const std::string &path, const std::string &key, shoc_tr_tun
     char k[600];
     shoc_tr_tuning v;
     double ms;
-    if (sscanf(line, "%599s %d %d %d %d %lf", k, &v.fused, &v.tracers_per_block, &v.tile_x,
-               &v.phase_b_warps, &ms) == 6 &&
+    if (sscanf(line, "%599s %d %d %d %d %d %lf", k, &v.fused, &v.tracers_per_block, &v.tile_x,
+               &v.phase_b_warps, &v.prefetch, &ms) == 7 &&
         key == k) {
       *t = v;
       found = true;  // the last line for a key wins
@@ -2898,8 +2904,8 @@ void tune_cache_put(const std::string &path, const std::string &key, const shoc_
   FILE *f = fopen(tmp.c_str(), "w");
   if (!f) return;
   for (auto &l : keep) fputs(l.c_str(), f);
-  fprintf(f, "%s %d %d %d %d %.6f\n", key.c_str(), t.fused, t.tracers_per_block, t.tile_x,
-          t.phase_b_warps, ms);
+  fprintf(f, "%s %d %d %d %d %d %.6f\n", key.c_str(), t.fused, t.tracers_per_block, t.tile_x,
+          t.phase_b_warps, t.prefetch, ms);
   fclose(f);
   rename(tmp.c_str(), path.c_str());
 }
@@ -2976,11 +2982,15 @@ int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tu
   const std::vector<int> tws = h->esize == sizeof(float)
                                    ? std::vector<int>{2, 3, 4, 5, 6, 8, 12, 16}
                                    : std::vector<int>{2, 3, 4, 5, 6, 8};
-  for (int tw : tws) {
-    shoc_tr_tuning c = base;
-    c.fused = 0;
-    c.tracers_per_block = tw;
-    cand.push_back(c);
+  for (int pf : {0, 1}) {
+    if (pf && h->esize != sizeof(float)) continue;
+    for (int tw : tws) {
+      shoc_tr_tuning c = base;
+      c.fused = 0;
+      c.tracers_per_block = tw;
+      c.prefetch = pf;
+      cand.push_back(c);
+    }
   }
   if (h->esize == sizeof(float) && h->fnwb_max) {
     std::vector<int> nwbs = {h->fnwb_max};
@@ -2989,6 +2999,7 @@ int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tu
       for (int nwb : nwbs) {
         shoc_tr_tuning c = base;
         c.fused = 1;
+        c.prefetch = 0;
         c.tile_x = tx;
         c.phase_b_warps = nwb;
         cand.push_back(c);

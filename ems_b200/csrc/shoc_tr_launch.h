@@ -12,7 +12,8 @@ namespace shoc {
 cudaError_t tile32_set_smem_attr();
 
 // one FP32-mixed transport sub-step over the staged columns: k_adv32 then
-// k_vd32 (vd_nw tracers per k_vd32 block); rnd [ntr][S] holds k_adv32's
+// k_vd32 (vd_nw warps per k_vd32 block, vd_pf: staging the next tracer's
+// column while the current one is solved); rnd [ntr][S] holds k_adv32's
 // rounding residuals, carry [ntr][ncol] the columns' FP64 mass carry.
 // adv_flags: 1 every advected
 // tracer has advection and no horizontal diffusion, 2 both, 0 mixed.  With
@@ -22,8 +23,8 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
-                    double *carry, double *fzs, int vd_nw, int any_hd, int adv_flags,
-                    cudaEvent_t *ev);
+                    double *carry, double *fzs, int vd_nw, int vd_pf, int any_hd,
+                    int adv_flags, cudaEvent_t *ev);
 
 // allow every k_step32 instance `bytes` of dynamic shared memory
 cudaError_t fused32_set_smem_attr(int bytes);

@@ -642,16 +642,18 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
 
 // k_vd32: a block is one tile of 32 columns and nw warps (at most
 // kVd32MaxWarps); the tile's tracer-independent column arrays are staged
-// once and each warp steps its share of the tracers through them.
+// once and each warp steps its share of the tracers through them (PF: with
+// the next tracer's column staged while the current one is solved).
 constexpr int kVd32MaxWarps = 16;
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
 // LU float4[nd][32], thicknesses double[nd][32], colC int[nd][32], A, S
-// float[nd][nw][32]
-inline size_t vd32_smem(int nd, int nw) {
-  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)2 * nd * nw * 32 * 4;
+// float[nd][nw][32] (twice with pf: the next tracer's column is staged
+// while the current one is solved)
+inline size_t vd32_smem(int nd, int nw, bool pf = false) {
+  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)(pf ? 4 : 2) * nd * nw * 32 * 4;
 }
 
-template <bool LAST>
+template <bool LAST, bool PF>
 __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work W, Opt O,
                                                              TrSet T, SubStep ss, Tile Tl,
                                                              const float4 *__restrict__ lu32,
@@ -668,8 +670,8 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   float4 *LU = reinterpret_cast<float4 *>(smem);          // [nd][32]
   double *DZ = reinterpret_cast<double *>(LU + nd * 32);  // [nd][32]
   int *colC = reinterpret_cast<int *>(DZ + nd * 32);      // [nd][32]
-  float *A = reinterpret_cast<float *>(colC + nd * 32);   // [nd][nw][32]
-  float *Sv = A + nd * nw * 32;                           // [nd][nw][32]
+  // per buffer (two with PF): A, S float [nd][nw][32]
+  float *const bufs = reinterpret_cast<float *>(colC + nd * 32);
 
   const int lane = threadIdx.x, wy = threadIdx.y;
   const int tile = tile0 + blockIdx.x;
@@ -697,8 +699,9 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   __syncthreads();
   if (!act) return;
 
-  float *const A0 = A + wy * 32 + lane + (kb - kbase) * sa;
-  float *const S0 = Sv + wy * 32 + lane + (kb - kbase) * sa;
+  const size_t off = (size_t)wy * 32 + lane + (size_t)(kb - kbase) * sa;
+  auto A0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + off; };
+  auto S0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + (size_t)nd * sa + off; };
   const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const double *const D0 = DZ + (kb - kbase) * 32 + lane;
@@ -706,35 +709,59 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   const bool steady = F.eta[c2] == F.oldeta[c2];
   const int ntc = G.colntr[col];
   const int sed = G.zm1[cbot];
+  // the column's values of slot s into buffer b, one batch of asynchronous
+  // copies: advection results and their rounding residuals (advected
+  // tracers; the residuals go to the Thomas storage until the sweep) or the
+  // old values (the rest)
+  auto stage = [&](int s, int b) {
+    const int n = T.slot_tr[s];
+    const bool tb = (T.trf[n] & TR_TBDY) != 0;
+    const float *src = (tb ? tro : tri) + (size_t)n * G.S;
+    float *const A0 = A0of(b), *const S0 = S0of(b);
+    for (int j = 0; j < nz - kb; ++j) cp_async4(&A0[j * sa], src + C0[j * 32]);
+    if (tb) {
+      const float *rs = rsi + (size_t)n * G.S;
+      for (int j = 0; j < nz - kb; ++j) cp_async4(&S0[j * sa], rs + C0[j * 32]);
+    }
+    cp_async_commit();
+  };
+  // warp wy takes the tracers wy, wy + nw, ... the column carries
+  auto next = [&](int s) {
+    for (; s < T.nslot; s += nw)
+      if (T.slot_tr[s] < ntc) return s;
+    return T.nslot;
+  };
   long long nwarn = 0;
   bool bad = false;  // a NaN among the values this thread stores
-  // warp wy takes the tracers wy, wy + nw, ... of the column
-  for (int slot = wy; slot < T.nslot; slot += nw) {
+  int slot = next(wy), b = 0;
+  if (PF && slot < T.nslot) stage(slot, 0);
+  while (slot < T.nslot) {
+    const int nxt = next(slot + nw);
+    if (PF) {  // the next tracer's column is copied while this one is solved
+      if (nxt < T.nslot) {
+        stage(nxt, b ^ 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+    } else {
+      stage(slot, 0);
+    }
     const int n = T.slot_tr[slot];
-    if (n >= ntc) continue;  // tracer not carried in this column
     const int tf = T.trf[n];
     const bool tbdy = (tf & TR_TBDY) != 0;
     const bool adv = tbdy && (tf & TR_ADV);
     const bool vdf = LAST && (tf & TR_VDIFF);
     const float *tr = tri + (size_t)n * G.S;
     float *to = tro + (size_t)n * G.S;
-    // the column's values: advection results and their rounding residuals
-    // (advected tracers, residuals into the Thomas storage until the sweep)
-    // or the old values (the rest)
-    {
-      const float *src = tbdy ? to : tr;
-      for (int j = 0; j < nz - kb; ++j) cp_async4(&A0[j * sa], src + C0[j * 32]);
-      if (tbdy) {
-        const float *rs = rsi + (size_t)n * G.S;
-        for (int j = 0; j < nz - kb; ++j) cp_async4(&S0[j * sa], rs + C0[j * 32]);
-      }
-      cp_async_commit();
-    }
     to[sed] = tbdy ? tr[cbot] : tr[sed];  // sediment ghost (tracers.c:827-830)
     const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
-    cp_async_wait<0>();
-    column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0, S0, sa, L0, C0,
-                              D0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady, nwarn, bad);
+    if (!PF) cp_async_wait<0>();
+    column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0of(b), S0of(b),
+                              sa, L0, C0, D0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady,
+                              nwarn, bad);
+    slot = nxt;
+    if (PF) b ^= 1;
   }
   if (bad) atomicOr(W.status, ST_NAN);
   if (nwarn) atomicAdd(W.nwarn, (unsigned long long)nwarn);

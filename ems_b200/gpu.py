@@ -38,7 +38,7 @@ EXPORTS = (
 class Tuning(C.Structure):
     """shoc_tr_tuning: the transport kernels' launch configuration."""
     _fields_ = [("fused", C.c_int), ("tracers_per_block", C.c_int), ("tile_x", C.c_int),
-                ("phase_b_warps", C.c_int)]
+                ("phase_b_warps", C.c_int), ("prefetch", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

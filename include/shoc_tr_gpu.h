@@ -253,6 +253,8 @@ typedef struct {
   int tile_x;            /* k_step32: tile width along i (8, 16, 32; 32 / tile_x
                             columns along j) */
   int phase_b_warps;     /* k_step32: warps of its column phase */
+  int prefetch;          /* k_vd32: 1 stages the next tracer's column while the
+                            current one is solved (twice the per-warp shared memory) */
 } shoc_tr_tuning;
 /* set_tuning validates (SHOC_TR_EUNSUPPORTED for a configuration the window
  * or the shared memory does not allow) and takes effect at the next step.
@@ -267,7 +269,7 @@ int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t);
  * puts the state back (a device copy taken before the trials: the tracers,
  * surface vectors and mass carry are as they were) and keeps the fastest.
  * Candidates: 2..8 tracers per k_vd64 block, or 2..16 warps per k_vd32
- * block; for FP32-mixed also the fused sub-step with tile widths 8, 16, 32 and the most and half
+ * block with and without its prefetch; for FP32-mixed also the fused sub-step with tile widths 8, 16, 32 and the most and half
  * the most phase-B warps its shared memory allows.  With use_cache != 0 the
  * choice is looked up in and saved to a file keyed by the GPU model and the
  * window's configuration (sizes, tracers, precision, scheme, diffusion),

@@ -152,3 +152,24 @@ def test_fp32mixed_conserves_mass(name, steps, kernels):
     case = synth.make(name)
     _, m0, m1 = run_kernels(case, steps, kernels)
     assert np.all(np.abs(m1 - m0) <= 1e-12 * np.abs(m0)), np.abs(m1 - m0) / np.abs(m0)
+
+
+@pytest.mark.parametrize("warps", [2, 5, 16])
+def test_column_kernel_layouts_agree(warps):
+    """k_vd32 with any number of warps per block, with and without staging
+    the next tracer's column during the solve, gives the same tracers bit
+    for bit (each (column, tracer) is solved by one thread either way)."""
+    case = synth.make("small", seed=64)
+    out = []
+    for kw in ({}, dict(tracers_per_block=warps, prefetch=1),
+               dict(tracers_per_block=warps, prefetch=0)):
+        t = gpu.TracerStep(case, precision=gpu.FP32_MIXED)
+        t.start()
+        if kw:
+            t.set_tuning(fused=0, **kw)
+        t.run(5)
+        t.sync()
+        out.append(t.download())
+        t.close()
+    np.testing.assert_array_equal(out[0], out[1])
+    np.testing.assert_array_equal(out[0], out[2])
