@@ -443,12 +443,9 @@ def main():
             e2e_s = (time.perf_counter() - t0) / args.e2e_steps
         del tr_host
     e2e_s = max_over_ranks(pg, e2e_s, dev)
-    # bytes over the host link: the FP32-mixed drop-in moves FP32 tracer
-    # values (the library converts on the host), the FP64 one FP64 values
-    tb = 4 if mixed else 8
-    h2d = (case.ntr * S * tb + (10 if case.diffuse.any() else 6) * S * 8 +
+    h2d = (case.ntr * S * 8 + (10 if case.diffuse.any() else 6) * S * 8 +
            2 * case.win.sgsizS * 8 + 2 * case.win.geom.b2_t * 4)
-    d2h = case.ntr * S * tb + 2 * case.win.geom.b2_t * 4
+    d2h = case.ntr * S * 8 + 2 * case.win.geom.b2_t * 4
 
     cpu = None
     if rank == 0 and not args.no_cpu:
