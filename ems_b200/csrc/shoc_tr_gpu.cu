@@ -29,11 +29,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <condition_variable>
-#include <functional>
 #include <mutex>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include <sys/stat.h>
@@ -57,62 +54,6 @@ struct Sched {
 };
 
 }  // namespace
-
-// Host threads for the drop-in step of an FP32-mixed handle: they convert
-// the caller's FP64 tracers to FP32 into page-locked staging buffers on the
-// way up and back to FP64 on the way down, so only four bytes a value cross
-// the host link.  run(f) calls f(part, nparts) for every part, the caller
-// taking part 0, and returns when all are done.
-struct HostPool {
-  std::vector<std::thread> th;
-  std::mutex mu;
-  std::condition_variable go, done;
-  std::function<void(int, int)> job;
-  long long gen = 0;
-  int left = 0;
-  bool stop = false;
-
-  explicit HostPool(int n) {
-    for (int p = 1; p < n; p++)
-      th.emplace_back([this, p] {
-        long long seen = 0;
-        for (;;) {
-          std::function<void(int, int)> f;
-          {
-            std::unique_lock<std::mutex> lk(mu);
-            go.wait(lk, [&] { return stop || gen != seen; });
-            if (stop) return;
-            seen = gen;
-            f = job;
-          }
-          f(p, (int)th.size() + 1);
-          std::lock_guard<std::mutex> lk(mu);
-          if (--left == 0) done.notify_one();
-        }
-      });
-  }
-  void run(const std::function<void(int, int)> &f) {
-    const int n = (int)th.size() + 1;
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      job = f;
-      left = n - 1;
-      gen++;
-    }
-    go.notify_all();
-    f(0, n);
-    std::unique_lock<std::mutex> lk(mu);
-    done.wait(lk, [&] { return left == 0; });
-  }
-  ~HostPool() {
-    {
-      std::lock_guard<std::mutex> lk(mu);
-      stop = true;
-    }
-    go.notify_all();
-    for (auto &t : th) t.join();
-  }
-};
 
 struct shoc_tr_gpu {
   int device = 0;
@@ -196,13 +137,8 @@ struct shoc_tr_gpu {
   std::vector<int> slot_host;       // slot -> tracer, as T.slot_tr
   cudaStream_t s_up = nullptr, s_dn = nullptr;  // host -> device, device -> host
   std::vector<cudaEvent_t> pev;     // [0] flow sent, then per chunk: sent, stepped
+  double *xout = nullptr;           // FP32-mixed: one tracer of FP64 for the way back
   uint8_t *c3s = nullptr;           // [kItermax + 2][ncol] k_serial cursors between chunks
-  // FP32-mixed drop-in: host conversion threads, page-locked FP32 staging
-  // buffers of one tracer each (rings for the way up and the way down) and
-  // the events that free them
-  HostPool *pool = nullptr;
-  std::vector<float *> stage_up, stage_dn;
-  std::vector<cudaEvent_t> ev_up, ev_dn;
 };
 
 namespace {
@@ -1289,11 +1225,6 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h) {
   for (cudaStream_t x : {h->s_up, h->s_dn})
     if (x) cudaStreamSynchronize(x);
   for (cudaEvent_t x : h->pev) cudaEventDestroy(x);
-  for (cudaEvent_t x : h->ev_up) cudaEventDestroy(x);
-  for (cudaEvent_t x : h->ev_dn) cudaEventDestroy(x);
-  for (float *p : h->stage_up) cudaFreeHost(p);
-  for (float *p : h->stage_dn) cudaFreeHost(p);
-  delete h->pool;
   for (void *p : h->allocs) cudaFree(p);
   if (h->h_dtm) cudaFreeHost(h->h_dtm);
   for (cudaStream_t x : {h->s_up, h->s_dn})
@@ -2017,18 +1948,8 @@ int pipe_init(shoc_tr_gpu *h) {
   CK(cudaStreamCreateWithFlags(&h->s_up, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&h->s_dn, cudaStreamNonBlocking));
   if (h->esize == sizeof(float)) {
-    // two chunks of tracers in flight each way
-    const int ring = 2 * pipe_chunk_slots(h);
-    for (auto *v : {&h->stage_up, &h->stage_dn}) {
-      v->assign(ring, nullptr);
-      for (auto &p : *v) CK(cudaHostAlloc((void **)&p, (size_t)h->S * sizeof(float), 0));
-    }
-    for (auto *v : {&h->ev_up, &h->ev_dn}) {
-      v->assign(ring, nullptr);
-      for (auto &e : *v) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
-    const unsigned hc = std::thread::hardware_concurrency();
-    h->pool = new HostPool((int)std::max(1u, std::min(hc ? hc : 1u, 32u)));
+    int rc = dalloc(h, &h->xout, (size_t)h->S);
+    if (rc) return rc;
   }
   int rc = dalloc(h, &h->c3s, (size_t)(kItermax + 2) * h->ncol);
   if (rc) return rc;
@@ -2044,124 +1965,33 @@ void pipe_drain(shoc_tr_gpu *h) {
   cudaStreamSynchronize(h->stream);
 }
 
-// one FP64 tracer up into both buffers / back from buffer buf
 int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
   cudaStream_t s = h->s_up;
   const size_t S = (size_t)h->S;
-  double *a = (double *)h->tr[cur] + n * S, *b = (double *)h->tr[cur ^ 1] + n * S;
-  CK(cudaMemcpyAsync(a, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(b, a, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (h->esize == sizeof(double)) {
+    double *a = (double *)h->tr[cur] + n * S, *b = (double *)h->tr[cur ^ 1] + n * S;
+    CK(cudaMemcpyAsync(a, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b, a, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  } else {
+    float *a = (float *)h->tr[cur] + n * S, *b = (float *)h->tr[cur ^ 1] + n * S;
+    CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S);
+    h->launches++;
+  }
   return 0;
 }
 
 int down_tracer(shoc_tr_gpu *h, int buf, int n, double *dst) {
+  cudaStream_t s = h->s_dn;
   const size_t S = (size_t)h->S;
-  CK(cudaMemcpyAsync(dst, (double *)h->tr[buf] + n * S, S * sizeof(double),
-                     cudaMemcpyDeviceToHost, h->s_dn));
-  return 0;
-}
-
-// The drop-in step of an FP32-mixed handle.  The device keeps FP32 tracers,
-// so only FP32 values cross the host link: host threads round the caller's
-// FP64 values to FP32 into page-locked staging buffers (the rounding the
-// device would do, IEEE round to nearest) and widen the FP32 results back
-// into the caller's arrays (exact), each tracer in turn while the link
-// carries the others.  Chunk j goes up and is stepped while the host
-// converts chunk j + 1 and the results of chunk j - 1; the sub-step schedule
-// is probed once the first chunk is on its way.
-int step_pipelined_f32(shoc_tr_gpu *h, shoc_tr_state *st) {
-  const size_t S = (size_t)h->S;
-  const int cur = h->cur, csl = pipe_chunk_slots(h);
-  const int nch = (h->nslot + csl - 1) / csl, ring = (int)h->stage_up.size();
-  cudaEvent_t *ev = h->pev.data();  // [0] flow sent, [1 + 2j] chunk j sent, [2 + 2j] stepped
-  CK(cudaEventRecord(ev[0], h->stream));
-  CK(cudaStreamWaitEvent(h->s_up, ev[0], 0));
-  auto convert_up = [&](const double *src, float *dst) {
-    h->pool->run([&](int p, int np) {
-      const size_t a = S * p / np, b = S * (p + 1) / np;
-      for (size_t i = a; i < b; i++) dst[i] = (float)src[i];
-    });
-  };
-  auto convert_dn = [&](const float *src, double *dst) {
-    h->pool->run([&](int p, int np) {
-      const size_t a = S * p / np, b = S * (p + 1) / np;
-      for (size_t i = a; i < b; i++) dst[i] = (double)src[i];
-    });
-  };
-  Sched s;
-  int fin = cur;
-  int rc = 0;
-  for (int j = 0; j <= nch && !rc; j++) {
-    const int s0 = j * csl, ns = std::min(h->nslot - s0, csl);
-    if (j < nch) {
-      // up: convert each tracer of chunk j into a free staging buffer, copy
-      // it to both tracer buffers on the device
-      for (int sl = s0; sl < s0 + ns && !rc; sl++) {
-        const int n = h->slot_host[sl], r = sl % ring;
-        if (cudaEventSynchronize(h->ev_up[r]) != cudaSuccess) rc = SHOC_TR_ECUDA;
-        if (rc) break;
-        convert_up(st->tr_wc[n], h->stage_up[r]);
-        float *a = (float *)h->tr[cur] + n * S, *b = (float *)h->tr[cur ^ 1] + n * S;
-        if (cudaMemcpyAsync(a, h->stage_up[r], S * sizeof(float), cudaMemcpyHostToDevice,
-                            h->s_up) != cudaSuccess ||
-            cudaMemcpyAsync(b, a, S * sizeof(float), cudaMemcpyDeviceToDevice, h->s_up) !=
-                cudaSuccess ||
-            cudaEventRecord(h->ev_up[r], h->s_up) != cudaSuccess)
-          rc = SHOC_TR_ECUDA;
-      }
-      if (rc) break;
-      CK(cudaEventRecord(ev[1 + 2 * j], h->s_up));
-      if (j == 0) {
-        // the schedule from this step's flow, while chunk 0 travels
-        rc = probe_schedule(h, false, s);
-        if (!rc && s.sub.size() > (size_t)kItermax + 2) rc = SHOC_TR_ESUBSTEP;
-        if (rc) break;
-        fin = cur ^ (int)(s.sub.size() & 1);  // the buffer the step ends in
-      }
-      // step chunk j once it is on the device, then start its way back
-      TrSet Tc = h->T;
-      Tc.slot_tr = h->T.slot_tr + s0;
-      Tc.nslot = ns;
-      Tc.ntb = std::max(0, std::min(h->T.ntb - s0, ns));
-      CK(cudaStreamWaitEvent(h->stream, ev[1 + 2 * j], 0));
-      launch_lateral(h, cur, Tc);
-      rc = launch_part_b(h, s, cur, Tc, h->c3s, j > 0);
-      if (rc) break;
-      CK(cudaEventRecord(ev[2 + 2 * j], h->stream));
-      CK(cudaStreamWaitEvent(h->s_dn, ev[2 + 2 * j], 0));
-      for (int sl = s0; sl < s0 + ns; sl++) {
-        const int n = h->slot_host[sl], r = sl % ring;
-        CK(cudaMemcpyAsync(h->stage_dn[r], (const float *)h->tr[fin] + n * S, S * sizeof(float),
-                           cudaMemcpyDeviceToHost, h->s_dn));
-        CK(cudaEventRecord(h->ev_dn[r], h->s_dn));
-      }
-    }
-    if (j > 0) {
-      // down: widen chunk j - 1's results into the caller's arrays
-      const int p0 = (j - 1) * csl, np = std::min(h->nslot - p0, csl);
-      for (int sl = p0; sl < p0 + np && !rc; sl++) {
-        const int n = h->slot_host[sl], r = sl % ring;
-        if (cudaEventSynchronize(h->ev_dn[r]) != cudaSuccess) {
-          rc = SHOC_TR_ECUDA;
-          break;
-        }
-        convert_dn(h->stage_dn[r], st->tr_wc[n]);
-      }
-    }
+  if (h->esize == sizeof(double)) {
+    CK(cudaMemcpyAsync(dst, (double *)h->tr[buf] + n * S, S * sizeof(double),
+                       cudaMemcpyDeviceToHost, s));
+  } else {
+    k_to_f64<<<592, 256, 0, s>>>((float *)h->tr[buf] + n * S, h->xout, S);
+    h->launches++;
+    CK(cudaMemcpyAsync(dst, h->xout, S * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
-  if (rc) {
-    pipe_drain(h);
-    return rc;
-  }
-  if (nch == 0) {  // no tracer to move: the step still runs its set-up
-    rc = probe_schedule(h, false, s);
-    if (rc) return rc;
-    fin = cur ^ (int)(s.sub.size() & 1);
-  }
-  CK(cudaEventRecord(ev[0], h->s_dn));
-  CK(cudaStreamWaitEvent(h->stream, ev[0], 0));
-  h->cur = fin;
-  adopt_schedule(h, s);
   return 0;
 }
 
@@ -2170,7 +2000,6 @@ int step_pipelined(shoc_tr_gpu *h, shoc_tr_state *st) {
   if (rc) return rc;
   rc = shoc_tr_gpu_set_flow(h, st);
   if (rc) return rc;
-  if (h->esize == sizeof(float)) return step_pipelined_f32(h, st);
   const int cur = h->cur, csl = pipe_chunk_slots(h);
   const int nch = (h->nslot + csl - 1) / csl;
   cudaEvent_t *ev = h->pev.data();  // [0] flow sent, [1 + 2j] chunk j sent, [2 + 2j] stepped

@@ -68,14 +68,10 @@ void shoc_tr_gpu_destroy(shoc_tr_gpu *h);
  * shoc_tr_gpu_upload_tracers + shoc_tr_gpu_run(h, 1) +
  * shoc_tr_gpu_download_tracers, bit for bit.  Copies reach the host link's
  * speed only from page-locked memory: see shoc_tr_gpu_host_register.  With
- * SHOC_TR_FP32_MIXED only FP32 values cross the host link: host threads
- * round the caller's FP64 tracers to FP32 (as the device would) into
- * page-locked staging buffers on the way up and widen the results back on
- * the way down, overlapped with the copies; the handle keeps its per-column
- * mass carry (the FP64 mass the FP32-stored values owe each column) from one
- * call to the next: the values it belongs to come back unchanged through the
- * FP64 host arrays, so a run of drop-in steps equals the same steps on
- * resident tracers. */
+ * SHOC_TR_FP32_MIXED the handle keeps its per-column mass carry (the FP64
+ * mass the FP32-stored values owe each column) from one call to the next:
+ * the values it belongs to come back unchanged through the FP64 host arrays,
+ * so a run of drop-in steps equals the same steps on resident tracers. */
 int shoc_tr_gpu_step(shoc_tr_gpu *h, shoc_tr_state *st, shoc_tr_diag *diag);
 
 /* Page-locks (cudaHostRegister) / releases a host array the caller passes to
