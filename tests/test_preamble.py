@@ -116,3 +116,37 @@ def test_steps_with_device_preamble_equal_given_fields(name):
     np.testing.assert_array_equal(tra[:, c], trb[:, c])
     np.testing.assert_array_equal(sa[0], sur)
     np.testing.assert_array_equal(sa[1], nsur)
+
+
+@pytest.mark.gpu
+@pytest.mark.usefixtures("need_gpu")
+@pytest.mark.parametrize("precision", [gpu.FP64, gpu.FP32_MIXED])
+def test_dropin_steps_with_preamble_equal_resident(precision):
+    """The drop-in call on host arrays runs the preamble too: 3 drop-in steps
+    with it on give the resident run's tracers and surfaces bit for bit, and
+    the fields the host state carries for w and the fluxes are not read."""
+    case = _case("small_moving")
+    d = _detadt(case)
+    a = gpu.TracerStep(case, precision=precision)
+    a.start()
+    a.set_preamble(True, d)
+    a.run(3)
+    a.sync()
+    tra = a.download()
+    sa = a.surface()
+    a.close()
+
+    b = gpu.TracerStep(case, precision=precision)
+    b.set_preamble(True, d)
+    tr, sur, nsur = case.copy_state()
+    # garbage in the fields the preamble computes: they must not be read
+    case.w = np.full_like(case.w, np.nan)
+    case.u1flux3d = np.full_like(case.u1flux3d, np.nan)
+    case.u2flux3d = np.full_like(case.u2flux3d, np.nan)
+    for _ in range(3):
+        b.step(tr, sur, nsur)
+    b.close()
+    c = case.win.wet_cells()
+    np.testing.assert_array_equal(tra[:, c], tr[:, c])
+    np.testing.assert_array_equal(sa[0], sur)
+    np.testing.assert_array_equal(sa[1], nsur)
