@@ -53,7 +53,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="stiff2048")
-    p.add_argument("--precision", default="fp32mixed", choices=["fp64", "fp32mixed"])
+    p.add_argument("--precision", default="fp32mixed", choices=["fp64", "fp32mixed", "fp32comp"])
     p.add_argument("--no-fp64", action="store_true",
                    help="skip the plain FP64 arm that the mixed-precision line compares with")
     p.add_argument("--size", default="",
@@ -271,15 +271,17 @@ def run_reference(args, rank, world, sample=False):
                     "d2h_bytes_per_step": 0}}
 
 
-def kernel_bytes(case, kernel, fp64):
+def kernel_bytes(case, kernel, fp64, comp=False):
     """Algorithmic HBM bytes of one launch of a transport kernel: every tracer
-    value read once and written once, plus its per-cell fields (advection:
-    u1flux3d, u2flux3d, w, dz; column kernel: the four LU factors; the fused
-    sub-step kernel: the five fields of a step, u1flux3d, u2flux3d, w, Kz
-    through the LU factors, dz)."""
+    value read once and written once (8 bytes FP64, 4 FP32, 6 FP32 with its
+    16-bit compensation), plus its per-cell fields (advection: u1flux3d,
+    u2flux3d, w, dz; column kernel: the four LU factors; the fused sub-step
+    kernel: the five fields of a step, u1flux3d, u2flux3d, w, Kz through the
+    LU factors, dz)."""
     s = 8 if fp64 else 4
+    st = 6 if comp else s
     fields = 5 if kernel == "k_step32" else 4
-    return case.cell_tracers() * 2 * s + case.nwet * fields * s
+    return case.cell_tracers() * 2 * st + case.nwet * fields * s
 
 
 def time_arm(case, prec, local, args, pg, dev, clocks=None):
@@ -351,7 +353,8 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    mixed = args.precision == "fp32mixed"
+    mixed = args.precision in ("fp32mixed", "fp32comp")
+    comp = args.precision == "fp32comp"
     shared = args.workload in ("batch8", "batch8small") and world > 1
     if shared:
         # the eight basins shared out over the ranks (strong scaling)
@@ -366,7 +369,8 @@ def main():
 
     # the headline arm (timed with clocks sampled), then the plain FP64 arm on
     # the same inputs for the speed-up and the error of the mixed precision
-    arm = time_arm(case, gpu.FP32_MIXED if mixed else gpu.FP64, local, args, pg, dev,
+    arm = time_arm(case, gpu.FP32_COMP if comp else gpu.FP32_MIXED if mixed else gpu.FP64,
+                   local, args, pg, dev,
                    ClockSampler(local))
     step = arm["step"]
     fp64 = None
@@ -410,7 +414,7 @@ def main():
         kern = {"k_adv64": arm["parts"][1], "k_vd64": arm["parts"][2]}
     kname = max(kern, key=kern.get)
     kms = kern[kname]
-    kb = kernel_bytes(case, kname, f64b)
+    kb = kernel_bytes(case, kname, f64b, comp)
     achieved = kb / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
     traffic = None
     try:
@@ -459,7 +463,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": arm["ms_step"],
         "higher_is_better": True, "scaling": "strong" if shared else "weak",
         "vs_baseline": None,
-        "dtype": "f32-mixed" if mixed else "f64", "data": "synthetic",
+        "dtype": "f32-comp" if comp else "f32-mixed" if mixed else "f64", "data": "synthetic",
         "config": {
             "workload": args.workload + ("@" + args.size if args.size else ""), "nx": case.win.nx, "ny": case.win.ny,
             "nz": case.win.nz, "tracers": case.ntr, "wet_cells": case.nwet,

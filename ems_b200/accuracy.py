@@ -1,4 +1,5 @@
-"""Accuracy of the FP32-mixed step against the plain FP64 step.
+"""Accuracy of the FP32-mixed step (or FP32_COMP, --precision fp32comp)
+against the plain FP64 step.
 
 Both precisions step the same window from the same state on the GPU; every
 `every` steps the tracers are compared cell by cell over the wet cells:
@@ -45,12 +46,16 @@ def worst_cells(case, x64, x32):
     return out
 
 
-def compare(case, steps, every, device=0, log=None, worst=None):
-    """Per-tracer errors of FP32-mixed vs FP64 after every `every` steps
-    (compared on the device, shoc_tr_gpu_compare: no tracer leaves HBM).
-    worst: a list that receives worst_cells() after the last step."""
+PRECISIONS = {"fp32mixed": gpu.FP32_MIXED, "fp32comp": gpu.FP32_COMP}
+
+
+def compare(case, steps, every, device=0, log=None, worst=None, precision=gpu.FP32_MIXED):
+    """Per-tracer errors of FP32-mixed (or FP32_COMP) vs FP64 after every
+    `every` steps (compared on the device, shoc_tr_gpu_compare: no tracer
+    leaves HBM).  worst: a list that receives worst_cells() after the last
+    step."""
     s64 = gpu.TracerStep(case, precision=gpu.FP64, device=device)
-    s32 = gpu.TracerStep(case, precision=gpu.FP32_MIXED, device=device)
+    s32 = gpu.TracerStep(case, precision=precision, device=device)
     s64.start()
     s32.start()
     m64_0, m32_0 = s64.mass(), s32.mass()
@@ -93,6 +98,7 @@ def main():
     p.add_argument("--json", default="")
     p.add_argument("--worst", action="store_true",
                    help="report where each tracer's largest difference is")
+    p.add_argument("--precision", default="fp32mixed", choices=sorted(PRECISIONS))
     a = p.parse_args()
     kw = {}
     if a.size:
@@ -100,8 +106,10 @@ def main():
     case = synth.make(a.workload, seed=a.seed, **kw)
     t0 = time.time()
     worst = [] if a.worst else None
-    rows = compare(case, a.steps, a.every, log=lambda s: print(s, flush=True), worst=worst)
+    rows = compare(case, a.steps, a.every, log=lambda s: print(s, flush=True), worst=worst,
+                   precision=PRECISIONS[a.precision])
     out = {"workload": a.workload + ("@" + a.size if a.size else ""), "seed": a.seed,
+           "precision": a.precision,
            "steps": a.steps, "tracers": case.ntr, "wet_cells": case.nwet,
            "seconds": time.time() - t0, "checkpoints": rows}
     if worst is not None:

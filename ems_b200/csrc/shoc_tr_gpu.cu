@@ -72,6 +72,8 @@ struct shoc_tr_gpu {
   std::vector<void *> allocs;
   void *tr[2] = {nullptr, nullptr};   // double (FP64) or float (FP32-mixed)
   size_t esize = sizeof(double);
+  bool comp = false;                  // SHOC_TR_FP32_COMP: 16-bit compensation beside each value
+  int16_t *lo[2] = {nullptr, nullptr};  // [ntr][S] compensation of tr[0] / tr[1]
   double *xfer = nullptr;             // one tracer of FP64, for FP32 upload / download
   Flow32 F3{};
   f32::Face2 *fx2 = nullptr, *fy2 = nullptr;
@@ -200,10 +202,12 @@ __global__ void k_reset(Work W, int *counts) {
 
 // Lateral ghosts take their interior value (set_lateral_BC_tr): written into
 // both tracer buffers so the value read during every sub-step, and the value
-// left in the returned array, is the start-of-step one.
+// left in the returned array, is the start-of-step one.  la / lb (FP32_COMP):
+// the buffers' compensations, copied alike.
 template <class TR>
 __global__ void k_lateral(int nbpt, const int *bpt, const int *bin, const int *slot_tr,
-                          int nslot, int S, TR *tra, TR *trb) {
+                          int nslot, int S, TR *tra, TR *trb, int16_t *la = nullptr,
+                          int16_t *lb = nullptr) {
   long long tot = (long long)nbpt * nslot;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < tot;
        i += (long long)gridDim.x * blockDim.x) {
@@ -212,6 +216,11 @@ __global__ void k_lateral(int nbpt, const int *bpt, const int *bin, const int *s
     TR v = tra[off + bin[b]];
     tra[off + bpt[b]] = v;
     trb[off + bpt[b]] = v;
+    if (la) {
+      const int16_t q = la[off + bin[b]];
+      la[off + bpt[b]] = q;
+      lb[off + bpt[b]] = q;
+    }
   }
 }
 
@@ -455,11 +464,14 @@ __global__ void k_courant(Geo G, Flow F, Work W, double dtu, int only_listed) {
 // one thread per column, tracers in tbdy order, as the reference loops.
 // When the tracers go through in chunks of slots (the drop-in step's
 // pipeline), c3s holds each listed column's cursor state between the chunks
-// of one sub-step: read when c3_load, written back always.
+// of one sub-step: read when c3_load, written back always.  lo_out
+// (FP32_COMP): these columns step their FP32 values as stored, and their
+// compensations, from the sediment ghost to the top cell, are set to 0.
 template <bool LAST, class TR>
 __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
                          const TR *__restrict__ tr_in, TR *__restrict__ tr_out,
-                         uint8_t *__restrict__ c3s, int c3_load) {
+                         uint8_t *__restrict__ c3s, int c3_load,
+                         int16_t *__restrict__ lo_out = nullptr) {
   int cnt = *W.serial_count;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     int col = W.serial_list[i];
@@ -472,6 +484,15 @@ __global__ void k_serial(Geo G, Flow F, Work W, Opt O, TrSet T, SubStep ss,
       if (n >= G.colntr[col]) continue;  // not carried in this column
       column_pass<LAST>(G, F, W, O, T, ss, tr_in + (size_t)n * G.S, tr_out + (size_t)n * G.S,
                         col, n, G.col_kb[col], true, sol, c3, warn, stat);
+      if (lo_out) {
+        int16_t *lo = lo_out + (size_t)n * G.S;
+        int c = G.zm1[G.col_bot[col]];
+        lo[c] = 0;
+        do {
+          c = G.zp1[c];
+          lo[c] = 0;
+        } while (c != G.col_top[col]);
+      }
     }
     if (c3s) c3s[i] = c3 ? 1 : 0;
     if (warn) atomicAdd(W.nwarn, warn);
@@ -606,19 +627,27 @@ __global__ void k_to_f32(const double *a, float *b, size_t n) {
        i += (size_t)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
 }
-// one uploaded tracer into both ping-pong buffers
-__global__ void k_to_f32x2(const double *a, float *b, float *c, size_t n) {
+// one uploaded tracer into both ping-pong buffers (and, SHOC_TR_FP32_COMP,
+// the compensation of both: lb / lc non-null)
+__global__ void k_to_f32x2(const double *a, float *b, float *c, size_t n, int16_t *lb = nullptr,
+                           int16_t *lc = nullptr) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
     const float v = (float)a[i];
     b[i] = v;
     c[i] = v;
+    if (lb) {
+      const int16_t q = lo_enc(a[i], v);
+      lb[i] = q;
+      lc[i] = q;
+    }
   }
 }
-__global__ void k_to_f64(const float *a, double *b, size_t n) {
+// a tracer back to FP64 (with its compensation where l is non-null)
+__global__ void k_to_f64(const float *a, double *b, size_t n, const int16_t *l = nullptr) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
-    b[i] = (double)a[i];
+    b[i] = l ? (double)a[i] + lo_dec(l[i], a[i]) : (double)a[i];
 }
 // K = dzu h2au1 u1kh / h1au1 (e1) or dzu2 h1au2 u2kh / h2au2 (e2): the
 // tracer-independent factor of hor_diffuse (tracers.c:3660-3666)
@@ -636,9 +665,10 @@ __global__ void k_khfac(Geo G, Flow F, float *khx, float *khy) {
 // colreg (or null): the region of each column; only region `reg` is summed.
 template <class TR>
 __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry, double *out,
-                       const int *colreg = nullptr, int reg = 0) {
+                       const int *colreg = nullptr, int reg = 0, const int16_t *lo = nullptr) {
   const int n = blockIdx.y;
   const TR *t = tr + (size_t)n * G.S;
+  const int16_t *l = lo ? lo + (size_t)n * G.S : nullptr;  // compensation (FP32_COMP)
   double s = 0.0, comp = 0.0;
   for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
        col += gridDim.x * blockDim.x) {
@@ -653,7 +683,10 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry,
     for (int it = 0; it <= G.nz; ++it) {
       double bz = (c == bot) ? G.botz[top] : G.gridz[c];
       double h = tz - bz;
-      if (h > 0.0) neumaier(s, comp, (double)t[c] * h * area);
+      if (h > 0.0) {
+        const double v = l ? (double)t[c] + lo_dec(l[c], (float)t[c]) : (double)t[c];
+        neumaier(s, comp, v * h * area);
+      }
       if (c == bot) break;
       tz = bz;
       c = G.zm1[c];
@@ -679,7 +712,8 @@ __global__ void k_mass(Geo G, Flow F, Work W, const TR *tr, const double *carry,
 template <class TA, class TB>
 __global__ void k_compare(Geo G, Tile Tl, const int *colntr_b, const TA *ta, const TB *tb,
                           const int *region, int nreg, unsigned long long *maxabs,
-                          unsigned long long *maxref, double *ssd, double *ssr) {
+                          unsigned long long *maxref, double *ssd, double *ssr,
+                          const int16_t *la, const int16_t *lb) {
   const int n = blockIdx.y;
   for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < G.ncol;
        col += gridDim.x * blockDim.x) {
@@ -690,7 +724,10 @@ __global__ void k_compare(Geo G, Tile Tl, const int *colntr_b, const TA *ta, con
     for (int k = G.col_kb[col]; k < G.nz; ++k) {
       const int c = Tl.cellk[(size_t)k * Tl.ncolp + col];
       if (!c) continue;
-      const double a = (double)ta[(size_t)n * G.S + c], b = (double)tb[(size_t)n * G.S + c];
+      const size_t i = (size_t)n * G.S + c;
+      double a = (double)ta[i], b = (double)tb[i];
+      if (la) a += lo_dec(la[i], (float)ta[i]);  // FP32_COMP: value + compensation
+      if (lb) b += lo_dec(lb[i], (float)tb[i]);
       const double d = a - b;
       ma = fmax(ma, fabs(d));
       mr = fmax(mr, fabs(b));
@@ -848,7 +885,7 @@ __global__ void k_halo_unpack(TR *tra, TR *trb, int S, int ntr, const int *cells
 
 // shared memory of the column kernel of the handle's precision
 size_t vd_smem(const shoc_tr_gpu *h, int nd, int nw) {
-  return h->esize == sizeof(float) ? vd32_smem(nd, nw, h->vd_pf) : vd64_smem(nd, nw);
+  return h->esize == sizeof(float) ? vd32_smem(nd, nw, h->vd_pf, h->comp) : vd64_smem(nd, nw);
 }
 
 // Static tables of the column-tile kernel: the cell of every column at every
@@ -1050,12 +1087,12 @@ int apply_tuning(shoc_tr_gpu *h, const shoc_tr_tuning &t) {
   if (t.tracers_per_block < 1 || t.tracers_per_block > (f32 ? kVd32MaxWarps : 8))
     return SHOC_TR_EUNSUPPORTED;
   if (t.prefetch && !f32) return SHOC_TR_EUNSUPPORTED;
-  const size_t vb = f32 ? vd32_smem(h->nz, t.tracers_per_block, t.prefetch != 0)
+  const size_t vb = f32 ? vd32_smem(h->nz, t.tracers_per_block, t.prefetch != 0, h->comp)
                         : vd64_smem(h->nz, t.tracers_per_block);
   if (vb > 227 * 1024) return SHOC_TR_EUNSUPPORTED;
   if (t.fused) {
     const int ti = tile_index(t.tile_x);
-    if (!f32 || !h->fnwb_max || ti < 0 || !h->ftile[ti].tcol) return SHOC_TR_EUNSUPPORTED;
+    if (!f32 || h->comp || !h->fnwb_max || ti < 0 || !h->ftile[ti].tcol) return SHOC_TR_EUNSUPPORTED;
     if (t.phase_b_warps < 1 || t.phase_b_warps > h->fnwb_max) return SHOC_TR_EUNSUPPORTED;
   } else if (f32 && !h->rnd) {
     const int rc = dalloc(h, &h->rnd, (size_t)h->ntr * h->S);
@@ -1239,7 +1276,9 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   *out = nullptr;
   int rc = check_geom(g, o, ntr);
   if (rc) return rc;
-  if (precision != SHOC_TR_FP64 && precision != SHOC_TR_FP32_MIXED) return SHOC_TR_EUNSUPPORTED;
+  if (precision != SHOC_TR_FP64 && precision != SHOC_TR_FP32_MIXED &&
+      precision != SHOC_TR_FP32_COMP)
+    return SHOC_TR_EUNSUPPORTED;
   if (precision == SHOC_TR_FP32_MIXED && ntr > kMaxTracers) return SHOC_TR_EUNSUPPORTED;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0 || device < 0 || device >= ndev)
@@ -1419,14 +1458,16 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<int>(h, &W.serial_list, nullptr, ncol));
   TRY(dupload<int>(h, &W.serial_count, nullptr, 1));
   TRY(dupload<int>(h, &h->d_counts, nullptr, 2));
-  const bool f32p = precision == SHOC_TR_FP32_MIXED;
+  const bool f32p = precision != SHOC_TR_FP64;
   h->esize = f32p ? sizeof(float) : sizeof(double);
+  h->comp = precision == SHOC_TR_FP32_COMP;
   h->staged = true;
   for (int b = 0; b < 2; b++) {
     if (f32p) {
       float *fp = nullptr;
       TRY(dupload<float>(h, &fp, nullptr, (size_t)ntr * S));
       h->tr[b] = fp;
+      if (h->comp) TRY(dupload<int16_t>(h, &h->lo[b], nullptr, (size_t)ntr * S));
     } else {
       double *dp2 = nullptr;
       TRY(dupload<double>(h, &dp2, nullptr, (size_t)ntr * S));
@@ -1492,7 +1533,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     // the fused sub-step kernel k_step32: every advected tracer's
     // accumulators and the column arrays of up to as many phase-B warps as
     // keep two blocks per SM; tiles of every width the autotuner may choose
-    if (o->ntbdy <= kFusedMaxTracers) {
+    // (not with FP32_COMP: k_step32 keeps no compensation)
+    if (o->ntbdy <= kFusedMaxTracers && !h->comp) {
       for (int c = kFusedWarps; c >= 1 && !h->fnwb_max; c--) {
         int gq;
         if (fused_config(h, c, &gq) <= 113 * 1024) h->fnwb_max = c;
@@ -1508,7 +1550,7 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
     // SHOC_TR_GPU_KERNELS=fused starts with k_step32 (8 x 4 tiles)
     const char *env = getenv("SHOC_TR_GPU_KERNELS");
     shoc_tr_tuning t0 = current_tuning(h);
-    if (env && strcmp(env, "fused") == 0 && h->fnwb_max) {
+    if (env && strcmp(env, "fused") == 0 && h->fnwb_max && !h->comp) {
       t0.fused = 1;
       t0.tile_x = 8;
       t0.phase_b_warps = h->fnwb_max;
@@ -1598,7 +1640,9 @@ void launch_lateral(shoc_tr_gpu *h, int cur, const TrSet &T) {
   int blocks = (int)std::min<long long>((tot + 255) / 256, 148 * 16);
   if (h->esize == sizeof(float))
     k_lateral<float><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, T.slot_tr, T.nslot, h->S,
-                                             (float *)h->tr[cur], (float *)h->tr[cur ^ 1]);
+                                             (float *)h->tr[cur], (float *)h->tr[cur ^ 1],
+                                             h->comp ? h->lo[cur] : nullptr,
+                                             h->comp ? h->lo[cur ^ 1] : nullptr);
   else
     k_lateral<double><<<blocks, 256, 0, st>>>(h->nbpt, h->bpt, h->bin, T.slot_tr, T.nslot,
                                               h->S, (double *)h->tr[cur],
@@ -1777,7 +1821,8 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
         const Tile tl = vd_classes(h, tw);
         tile32_substep(last, h->O.trasc == SHOC_TR_QUICKEST, h->O.ultimate != 0, st, h->G, h->F,
                        h->F3, h->W, h->O, T, ss, tl, h->fx2, h->fy2, tin, tout, h->rnd,
-                       h->fu.carry, h->fzs64, tw, h->vd_pf ? 1 : 0,
+                       h->fu.carry, h->fzs64, h->comp ? h->lo[cur] : nullptr,
+                       h->comp ? h->lo[cur ^ 1] : nullptr, tw, h->vd_pf ? 1 : 0,
                        h->any_hdiff ? 1 : 0, h->adv_flags, prof ? ev : nullptr);
         if (prof) {  // pairs share events; sync destroys each event once
           h->ev.push_back({0, ev[0], ev[2]});
@@ -1787,12 +1832,13 @@ int launch_part_b(shoc_tr_gpu *h, const Sched &s, int cur0, const TrSet &T,
         h->launches += (T.ntb > 0 && tl.nwet > 0 ? 1 : 0);
         for (int k = 0; k < tl.nclass; k++) h->launches += tl.ctile[k + 1] > tl.ctile[k] ? 1 : 0;
       }
+      int16_t *lo_out = h->comp ? h->lo[cur ^ 1] : nullptr;
       if (last)
         k_serial<true, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
-                                                            tin, tout, c3row, c3_load);
+                                                            tin, tout, c3row, c3_load, lo_out);
       else
         k_serial<false, float><<<kSerialBlocks, 64, 0, st>>>(h->G, h->F, h->W, h->O, T, ss,
-                                                             tin, tout, c3row, c3_load);
+                                                             tin, tout, c3row, c3_load, lo_out);
       h->launches++;
       cur ^= 1;
       continue;
@@ -1975,7 +2021,8 @@ int up_tracer(shoc_tr_gpu *h, int cur, int n, const double *src) {
   } else {
     float *a = (float *)h->tr[cur] + n * S, *b = (float *)h->tr[cur ^ 1] + n * S;
     CK(cudaMemcpyAsync(h->xfer, src, S * sizeof(double), cudaMemcpyHostToDevice, s));
-    k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S);
+    k_to_f32x2<<<592, 256, 0, s>>>(h->xfer, a, b, S, h->comp ? h->lo[cur] + n * S : nullptr,
+                                   h->comp ? h->lo[cur ^ 1] + n * S : nullptr);
     h->launches++;
   }
   return 0;
@@ -1988,7 +2035,8 @@ int down_tracer(shoc_tr_gpu *h, int buf, int n, double *dst) {
     CK(cudaMemcpyAsync(dst, (double *)h->tr[buf] + n * S, S * sizeof(double),
                        cudaMemcpyDeviceToHost, s));
   } else {
-    k_to_f64<<<592, 256, 0, s>>>((float *)h->tr[buf] + n * S, h->xout, S);
+    k_to_f64<<<592, 256, 0, s>>>((float *)h->tr[buf] + n * S, h->xout, S,
+                                 h->comp ? h->lo[buf] + n * S : nullptr);
     h->launches++;
     CK(cudaMemcpyAsync(dst, h->xout, S * sizeof(double), cudaMemcpyDeviceToHost, s));
   }
@@ -2078,7 +2126,9 @@ int shoc_tr_gpu_upload_tracers(shoc_tr_gpu *h, double *const *tr_wc) {
       float *a = (float *)h->tr[h->cur] + n * S, *b = (float *)h->tr[h->cur ^ 1] + n * S;
       CK(cudaMemcpyAsync(h->xfer, tr_wc[n], S * sizeof(double), cudaMemcpyHostToDevice,
                          h->stream));
-      k_to_f32x2<<<592, 256, 0, h->stream>>>(h->xfer, a, b, S);
+      k_to_f32x2<<<592, 256, 0, h->stream>>>(h->xfer, a, b, S,
+                                             h->comp ? h->lo[h->cur] + n * S : nullptr,
+                                             h->comp ? h->lo[h->cur ^ 1] + n * S : nullptr);
       h->launches++;
     }
   }
@@ -2094,7 +2144,8 @@ int shoc_tr_gpu_download_tracers(shoc_tr_gpu *h, double **tr_wc) {
       CK(cudaMemcpyAsync(tr_wc[n], (double *)h->tr[h->cur] + n * S, S * sizeof(double),
                          cudaMemcpyDeviceToHost, h->stream));
     } else {
-      k_to_f64<<<592, 256, 0, h->stream>>>((float *)h->tr[h->cur] + n * S, h->xfer, S);
+      k_to_f64<<<592, 256, 0, h->stream>>>((float *)h->tr[h->cur] + n * S, h->xfer, S,
+                                           h->comp ? h->lo[h->cur] + n * S : nullptr);
       h->launches++;
       CK(cudaMemcpyAsync(tr_wc[n], h->xfer, S * sizeof(double), cudaMemcpyDeviceToHost,
                          h->stream));
@@ -2241,6 +2292,7 @@ int shoc_tr_gpu_get_flow(shoc_tr_gpu *h, double *u1flux3d, double *u2flux3d, dou
 
 // ---- checkpoint / resume: a versioned raw image of the resident state ----
 // [header 8 x int64][tracers: ntr x S values of the handle's precision]
+// [compensations: ntr x S int16, FP32_COMP only]
 // [carry: ntr x ncol doubles, FP32-mixed path only][sur_t, nsur_t: ncol ints each]
 namespace {
 constexpr long long kStateMagic = 0x53484f4354524731ll;  // "SHOCTRG1"
@@ -2256,6 +2308,7 @@ void state_layout(const shoc_tr_gpu *h, long long hd[8]) {
 }
 size_t state_bytes(const shoc_tr_gpu *h) {
   return 8 * sizeof(long long) + (size_t)h->ntr * h->S * h->esize +
+         (h->comp ? (size_t)h->ntr * h->S * sizeof(int16_t) : 0) +
          (h->fu.carry ? (size_t)h->ntr * h->ncol * sizeof(double) : 0) +
          2 * (size_t)h->ncol * sizeof(int);
 }
@@ -2278,6 +2331,11 @@ int shoc_tr_gpu_save_state(shoc_tr_gpu *h, void *buf, size_t bytes) {
   const size_t tb = (size_t)h->ntr * h->S * h->esize;
   CK(cudaMemcpyAsync(p, h->tr[h->cur], tb, cudaMemcpyDeviceToHost, h->stream));
   p += tb;
+  if (h->comp) {
+    const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
+    CK(cudaMemcpyAsync(p, h->lo[h->cur], lb, cudaMemcpyDeviceToHost, h->stream));
+    p += lb;
+  }
   if (h->fu.carry) {
     const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
     CK(cudaMemcpyAsync(p, h->fu.carry, cb, cudaMemcpyDeviceToHost, h->stream));
@@ -2306,6 +2364,13 @@ int shoc_tr_gpu_load_state(shoc_tr_gpu *h, const void *buf, size_t bytes) {
   CK(cudaMemcpyAsync(h->tr[h->cur], p, tb, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->tr[h->cur ^ 1], h->tr[h->cur], tb, cudaMemcpyDeviceToDevice, h->stream));
   p += tb;
+  if (h->comp) {
+    const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
+    CK(cudaMemcpyAsync(h->lo[h->cur], p, lb, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->lo[h->cur ^ 1], h->lo[h->cur], lb, cudaMemcpyDeviceToDevice,
+                       h->stream));
+    p += lb;
+  }
   if (h->fu.carry) {
     const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
     CK(cudaMemcpyAsync(h->fu.carry, p, cb, cudaMemcpyHostToDevice, h->stream));
@@ -2403,7 +2468,8 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass) {
   if (h->ntr > 0) {
     if (h->esize == sizeof(float))
       k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
-          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part);
+          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part, nullptr, 0,
+          h->lo[h->cur]);
     else
       k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
           h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part);
@@ -2501,7 +2567,8 @@ int shoc_tr_gpu_mass_noalloc(shoc_tr_gpu *h, double *mass) {
   double *part = scr, *sums = scr + (size_t)kNoAllocMaxTracers * kNoAllocBlocks;
   if (h->esize == sizeof(float))
     k_mass<float><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
-        h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part);
+        h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part, nullptr, 0,
+        h->lo[h->cur]);
   else
     k_mass<double><<<dim3(kNoAllocBlocks, h->ntr), 256, 0, h->stream>>>(
         h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part);
@@ -2558,19 +2625,19 @@ int shoc_tr_gpu_compare(shoc_tr_gpu *a, shoc_tr_gpu *b, const int *region, int n
   if (fa && fb)
     k_compare<float, float><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const float *)ta,
                                                  (const float *)tb, dreg, nregion, dmax, dref,
-                                                 dsd, dsr);
+                                                 dsd, dsr, a->lo[a->cur], b->lo[b->cur]);
   else if (fa)
     k_compare<float, double><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const float *)ta,
                                                   (const double *)tb, dreg, nregion, dmax,
-                                                  dref, dsd, dsr);
+                                                  dref, dsd, dsr, a->lo[a->cur], b->lo[b->cur]);
   else if (fb)
     k_compare<double, float><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr, (const double *)ta,
                                                   (const float *)tb, dreg, nregion, dmax, dref,
-                                                  dsd, dsr);
+                                                  dsd, dsr, a->lo[a->cur], b->lo[b->cur]);
   else
     k_compare<double, double><<<grid, 256, 0, st>>>(a->G, a->tl, b->G.colntr,
                                                    (const double *)ta, (const double *)tb, dreg,
-                                                   nregion, dmax, dref, dsd, dsr);
+                                                   nregion, dmax, dref, dsd, dsr, a->lo[a->cur], b->lo[b->cur]);
   a->launches++;
   CK(cudaGetLastError());
   std::vector<double> out(nout * 4);
@@ -2678,6 +2745,7 @@ int shoc_tr_gpu_halo_plan(shoc_tr_gpu *h, int nsend, const int *send_cells, int 
 
 int shoc_tr_gpu_halo_pack(shoc_tr_gpu *h, void *buf) {
   if (!h || (h->nhalo_send && !buf)) return SHOC_TR_EARG;
+  if (h->comp) return SHOC_TR_EUNSUPPORTED;  // the halo carries no compensation
   DeviceScope dev_(h->device);
   const int n = h->nhalo_send;
   if (n && h->ntr) {
@@ -2698,6 +2766,7 @@ int shoc_tr_gpu_halo_pack(shoc_tr_gpu *h, void *buf) {
 
 int shoc_tr_gpu_halo_unpack(shoc_tr_gpu *h, const void *buf) {
   if (!h || (h->nhalo_recv && !buf)) return SHOC_TR_EARG;
+  if (h->comp) return SHOC_TR_EUNSUPPORTED;
   DeviceScope dev_(h->device);
   const int n = h->nhalo_recv;
   if (n && h->ntr) {
@@ -2736,7 +2805,8 @@ int shoc_tr_gpu_mass_region(shoc_tr_gpu *h, const int *region, int reg, double *
   if (h->ntr > 0) {
     if (h->esize == sizeof(float))
       k_mass<float><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
-          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part, dreg, reg);
+          h->G, h->F, h->W, (const float *)h->tr[h->cur], h->fu.carry, part, dreg, reg,
+          h->lo[h->cur]);
     else
       k_mass<double><<<dim3(nb, h->ntr), 256, 0, h->stream>>>(
           h->G, h->F, h->W, (const double *)h->tr[h->cur], nullptr, part, dreg, reg);
@@ -2914,6 +2984,7 @@ void tune_cache_put(const std::string &path, const std::string &key, const shoc_
 // surface vectors) the trial steps start from.
 struct Snapshot {
   void *tr = nullptr;
+  int16_t *lo = nullptr;  // FP32_COMP: both buffers' compensations
   double *carry = nullptr;
   int *sur = nullptr, *nsur = nullptr;
   int cur = 0;
@@ -2930,6 +3001,13 @@ int snap_take(shoc_tr_gpu *h, Snapshot &s) {
   s.cur = h->cur;
   for (int b = 0; b < 2; b++)
     CK(cudaMemcpyAsync((char *)s.tr + b * tb, h->tr[b], tb, cudaMemcpyDeviceToDevice, h->stream));
+  if (h->comp) {
+    const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
+    CK(cudaMallocAsync((void **)&s.lo, lb ? 2 * lb : 1, h->stream));
+    for (int b = 0; b < 2; b++)
+      CK(cudaMemcpyAsync((char *)s.lo + b * lb, h->lo[b], lb, cudaMemcpyDeviceToDevice,
+                         h->stream));
+  }
   if (s.carry) CK(cudaMemcpyAsync(s.carry, h->fu.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(s.sur, h->W.sur_t, ib, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(s.nsur, h->W.nsur_t, ib, cudaMemcpyDeviceToDevice, h->stream));
@@ -2944,6 +3022,12 @@ int snap_restore(shoc_tr_gpu *h, const Snapshot &s) {
   for (int b = 0; b < 2; b++)
     CK(cudaMemcpyAsync(h->tr[b], (const char *)s.tr + b * tb, tb, cudaMemcpyDeviceToDevice,
                        h->stream));
+  if (s.lo) {
+    const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
+    for (int b = 0; b < 2; b++)
+      CK(cudaMemcpyAsync(h->lo[b], (const char *)s.lo + b * lb, lb, cudaMemcpyDeviceToDevice,
+                         h->stream));
+  }
   if (s.carry) CK(cudaMemcpyAsync(h->fu.carry, s.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(h->W.sur_t, s.sur, ib, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(h->W.nsur_t, s.nsur, ib, cudaMemcpyDeviceToDevice, h->stream));
@@ -2952,6 +3036,7 @@ int snap_restore(shoc_tr_gpu *h, const Snapshot &s) {
 
 void snap_free(shoc_tr_gpu *h, Snapshot &s) {
   if (s.tr) cudaFreeAsync(s.tr, h->stream);
+  if (s.lo) cudaFreeAsync(s.lo, h->stream);
   if (s.carry) cudaFreeAsync(s.carry, h->stream);
   if (s.sur) cudaFreeAsync(s.sur, h->stream);
   cudaStreamSynchronize(h->stream);

@@ -44,6 +44,35 @@ constexpr int COL_THIN = 8;     // tr_bounds thin-surface test is on
 constexpr int COL_NOSOLVE = 16; // degenerate implicit-solve range: status raised, no solve
 constexpr int COL_STAGED = 32;  // handled by the FP32-mixed column-tile kernels
 
+// ---------------------------------------------------------------------------
+// 16-bit compensation of an FP32-stored value (the SHOC_TR_FP32_COMP
+// precision).  A value v stored as v32 = (float)v (round to nearest, so
+// |v - v32| <= ulp(v32) / 2) keeps q = rint((v - v32) / ulp(v32) * 2^15),
+// |q| <= 2^14, beside it; v32 + q ulp(v32) 2^-15 gives v back to about 2^-39
+// of its size.  Without it a value whose change per step is below half an
+// FP32 ulp is rounded back to the same FP32 number every step.  q is held
+// to |q| <= 2^14 - 1, so the decoded value lies strictly inside v32's
+// rounding interval: converting it to FP32 and encoding again gives v32 and
+// q back (the drop-in step's trip through FP64 host arrays changes nothing).
+
+// 2^k for -1022 <= k <= 1023, exactly
+__device__ __forceinline__ double pow2(int k) {
+  return __longlong_as_double((long long)(k + 1023) << 52);
+}
+// the exponent of ulp(v32) minus 15
+__device__ __forceinline__ int lo_exp(float v32) {
+  const int e = (int)((__float_as_uint(v32) >> 23) & 0xffu);
+  return (e == 0 ? 1 : e) - 150 - 15;
+}
+__device__ __forceinline__ int16_t lo_enc(double v, float v32) {
+  const double q = rint((v - (double)v32) * pow2(-lo_exp(v32)));
+  if (!(q >= -32767.0 && q <= 32767.0)) return 0;  // NaN / inf
+  return (int16_t)fmin(fmax(q, -16383.0), 16383.0);
+}
+__device__ __forceinline__ double lo_dec(int16_t q, float v32) {
+  return (double)q * pow2(lo_exp(v32));
+}
+
 // 2D face metrics of one direction, precomputed per surface-layer cell:
 // d = d3/d4 weight, db/df = 2/(h_m+h_0), 2/(h_0+h_p), h_m/h_0/h_p = metric
 // at the backward neighbour / the cell / the forward neighbour.

@@ -23,8 +23,8 @@ void tile32_substep(bool last, bool quick, bool ult, cudaStream_t st, const Geo 
                     const Flow &F, const Flow32 &F3, const Work &W, const Opt &O,
                     const TrSet &T, const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2,
                     const f32::Face2 *fy2, const float *tin, float *tout, float *rnd,
-                    double *carry, double *fzs, int vd_nw, int vd_pf, int any_hd,
-                    int adv_flags, cudaEvent_t *ev);
+                    double *carry, double *fzs, const int16_t *lo_in, int16_t *lo_out,
+                    int vd_nw, int vd_pf, int any_hd, int adv_flags, cudaEvent_t *ev);
 
 // allow every k_step32 instance `bytes` of dynamic shared memory
 cudaError_t fused32_set_smem_attr(int bytes);

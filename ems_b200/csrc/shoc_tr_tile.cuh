@@ -186,7 +186,8 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
                                                      const float *__restrict__ tri,
                                                      float *__restrict__ tro,
                                                      float *__restrict__ rso,
-                                                     double *__restrict__ fzs, int any_hd) {
+                                                     double *__restrict__ fzs, int any_hd,
+                                                     const int16_t *__restrict__ loi) {
   using namespace f32;
   constexpr unsigned FULL = 0xffffffffu;
   __shared__ int sTr[kMaxTracers], sTf[kMaxTracers];
@@ -334,6 +335,9 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         const int s = s0 + u;
         if (s >= ntb) break;
         const float *v = P + u * NQ * kAdv32Block;
+        // FP32_COMP: the cell's own value with its compensation (the stencil
+        // neighbours are read as stored)
+        const int16_t q0 = (loi && on) ? loi[(size_t)sTr[s] * G.S + c] : (int16_t)0;
         const float t0 = v[0];
         const float tym1 = v[1 * kAdv32Block], tym2 = v[2 * kAdv32Block];
         const float typ1 = v[3 * kAdv32Block], typ2 = v[4 * kAdv32Block];
@@ -354,7 +358,8 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         double a = dtr;
         if (zt) {
           const double Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
-          a = (double)t0 - (dtr * ia + (Fzt - Fzb)) * idz;
+          const double t0d = loi ? (double)t0 + lo_dec(q0, t0) : (double)t0;
+          a = t0d - (dtr * ia + (Fzt - Fzb)) * idz;
         } else if (zf) {
           fzs[(size_t)n * G.ncol + col] = Fzb;
         }
@@ -422,8 +427,11 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       // FP64 flux divergence (tracers.c:888-892)
       const double dtr = ((Fxe - Fxw) + (Fyn - Fys)) * dtu;
       double a = dtr;
-      if (zt)
-        a = (double)t0 - (dtr * ia + (Fzt - Fzb)) * idz;
+      if (zt) {
+        const double t0d =
+            loi ? (double)t0 + lo_dec(loi[(size_t)nn[u] * G.S + c], t0) : (double)t0;
+        a = t0d - (dtr * ia + (Fzt - Fzb)) * idz;
+      }
       else if (k == ks)
         fzs[(size_t)nn[u] * G.ncol + col] = Fzb;
       const float val = (float)a;
@@ -466,7 +474,13 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
                                               const float *tr, float *to, double area, double ia,
                                               double idt, ColSums cs,
                                               double *carry, bool steady, long long &nwarn,
-                                              bool &bad) {
+                                              bool &bad, float *R0 = nullptr,
+                                              const int16_t *li = nullptr,
+                                              int16_t *lout = nullptr) {
+  // FP32_COMP (R0, li, lout non-null): R0 keeps each row's value - stored
+  // (the advection's rounding residual, or the old value's compensation) for
+  // the solve's residual and the final value, li is the tracer's
+  // compensation on the way in, lout on the way out
   const ColInfo &ci = tc.ci;
   const int kb = tc.kb, nz = G.nz, c2 = tc.c2;
   const int nk = tc.ks - kb;  // cells below the surface cell
@@ -474,7 +488,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   const bool solve = vdf && !single;
   const double mn = T.mintr[n], mx = T.maxtr[n];
   const double dzs_old = (double)W.dz32[ci.s];
-  const double ts_old = (double)tr[ci.s];  // surface value before the sub-step
+  // surface value before the sub-step
+  const double ts_old = (double)tr[ci.s] + (li ? lo_dec(li[ci.s], tr[ci.s]) : 0.0);
   const double dzs = D0[nk * 32];
   // FP64 mass bookkeeping per unit area: what the step computed (mxs) and
   // what is stored (mss)
@@ -494,8 +509,10 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   }
   if (!tbdy) {
     vs = (double)A0[nk * sa];
+    if (li) vs += lo_dec(li[C0[nk * 32]], A0[nk * sa]);
     for (int j = nk + 1; j < nz - kb; ++j) {
       to[C0[j * 32]] = A0[j * sa];
+      if (lout) lout[C0[j * 32]] = li[C0[j * 32]];
       bad |= isnan(A0[j * sa]);
     }
   }
@@ -508,11 +525,18 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     float a = A0[j * sa];
     const double dz = D0[j * 32];
     H += dz;
-    if (!tbdy || RES) m += (tbdy ? (double)a + (double)S0[j * sa] : (double)a) * dz;
+    // the row's value - stored: the advection's rounding residual, or the
+    // old value's compensation
+    double r = 0.0;
+    if (tbdy && RES) r = (double)S0[j * sa];
+    else if (!tbdy && li) r = lo_dec(li[C0[j * 32]], a);
+    if (!tbdy || RES) m += ((double)a + r) * dz;
     if (clip && a < mn_up) {
-      mxs += ((double)mnf - (double)a) * dz;
+      mxs += ((double)mnf - ((double)a + r)) * dz;
       a = mnf;
+      r = 0.0;
     }
+    if (R0) R0[j * sa] = (float)r;
     if (tbdy) {
       nw += (a < mn_up || a > mx_dn);
       A0[j * sa] = a;
@@ -525,7 +549,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   }
   mxs += (tbdy && !RES) ? cs.m : m;
   if (tbdy) {
-    const double a_below = nk > 0 ? (double)A0[(nk - 1) * sa] : 0.0;
+    const double a_below =
+        nk > 0 ? (double)A0[(nk - 1) * sa] + (R0 ? (double)R0[(nk - 1) * sa] : 0.0) : 0.0;
     // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
     if (adv) {
       const double wb = (ci.s == tc.cbot) ? G.botz[c2] : G.gridz[ci.s];
@@ -547,27 +572,37 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     if (vs < mn || vs > mx) ++nw;
     bad |= isnan(vs);
     const float vs32 = (float)vs;
-    for (int j = nk + 1; j < nz - kb; ++j) to[C0[j * 32]] = vs32;
+    const int16_t qs = lout ? lo_enc(vs, vs32) : (int16_t)0;
+    for (int j = nk + 1; j < nz - kb; ++j) {
+      to[C0[j * 32]] = vs32;
+      if (lout) lout[C0[j * 32]] = qs;
+    }
   }
   mxs += vs * dzs;
   const double carry_in = (carry && steady) ? carry[(size_t)n * G.ncol + col] : 0.0;
   // the carry goes back as a uniform shift of the column's values
   const double dl = H > 0.0 ? carry_in * ia / H : 0.0;
   if (H > 0.0) mxs += carry_in * ia;
+  // stores one final value: FP32 (and, FP32_COMP, its compensation); adds
+  // what is stored to the stored mass
+  auto store = [&](int c, double v, double dz) {
+    const float fin = (float)v;
+    to[c] = fin;
+    bad |= isnan(fin);
+    double st = (double)fin;
+    if (lout) {
+      const int16_t q = lo_enc(v, fin);
+      lout[c] = q;
+      st += lo_dec(q, fin);
+    }
+    mss += st * dz;
+  };
   if (!solve) {
     // the values as they are, plus the carry's shift (tr_bounds has run)
-    for (int j = 0; j < nk; ++j) {
-      const float fin = (float)((double)A0[j * sa] + dl);
-      to[C0[j * 32]] = fin;
-      bad |= isnan(fin);
-      mss += (double)fin * D0[j * 32];
-    }
+    for (int j = 0; j < nk; ++j)
+      store(C0[j * 32], (double)A0[j * sa] + (R0 ? (double)R0[j * sa] : 0.0) + dl, D0[j * 32]);
     const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
-    const float fin = (vdf && single) ? (float)(vs + dl + F.dt * (0.0 - 0.0) / h)
-                                      : (float)(vs + dl);
-    to[ci.s] = fin;
-    bad |= isnan(fin);
-    mss += (double)fin * dzs;
+    store(ci.s, (vdf && single) ? vs + dl + F.dt * (0.0 - 0.0) / h : vs + dl, dzs);
   } else {
     // the surface row of the forward sweep
     {
@@ -594,7 +629,10 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       const float x = S0[j * sa] - l1.w * x1;
       S0[j * sa] = x;
       const double xd = (double)x, l1y = (double)l1.y;
-      const double aj1 = ((j + 1 == nk) ? vs : (double)A0[(j + 1) * sa]) + dl;
+      const double aj1 =
+          ((j + 1 == nk) ? vs
+                         : (double)A0[(j + 1) * sa] + (R0 ? (double)R0[(j + 1) * sa] : 0.0)) +
+          dl;
       double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
       if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
       A0[(j + 1) * sa] = (float)r;
@@ -606,7 +644,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       dzdt1 = D0[j * 32] * idt;
     }
     {
-      const double a0 = ((nk == 0) ? vs : (double)A0[0]) + dl;
+      const double a0 =
+          ((nk == 0) ? vs : (double)A0[0] + (R0 ? (double)R0[0] : 0.0)) + dl;
       double r = dzdt1 * (a0 - xd1);
       if (nk > 0) r = r - l2y * (xd2 - xd1);
       A0[0] = (float)r;
@@ -619,18 +658,10 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       A0[j * sa] = u;
     }
     float d = A0[nk * sa];
-    {
-      const float fin = (float)((double)S0[nk * sa] + (double)d);
-      to[C0[nk * 32]] = fin;
-      bad |= isnan(fin);
-      mss += (double)fin * dzs;
-    }
+    store(C0[nk * 32], (double)S0[nk * sa] + (double)d, dzs);
     for (int j = nk - 1; j >= 0; --j) {
       d = A0[j * sa] - L0[(j + 1) * 32].w * d;
-      const float fin = (float)((double)S0[j * sa] + (double)d);
-      to[C0[j * 32]] = fin;
-      bad |= isnan(fin);
-      mss += (double)fin * D0[j * 32];
+      store(C0[j * 32], (double)S0[j * sa] + (double)d, D0[j * 32]);
     }
   }
   if (carry && steady) carry[(size_t)n * G.ncol + col] = (mxs - mss) * area;
@@ -648,12 +679,15 @@ constexpr int kVd32MaxWarps = 16;
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
 // LU float4[nd][32], thicknesses double[nd][32], colC int[nd][32], A, S
 // float[nd][nw][32] (twice with pf: the next tracer's column is staged
-// while the current one is solved)
-inline size_t vd32_smem(int nd, int nw, bool pf = false) {
-  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)(pf ? 4 : 2) * nd * nw * 32 * 4;
+// while the current one is solved), with comp (FP32_COMP) R float[nd][nw][32]
+inline size_t vd32_smem(int nd, int nw, bool pf = false, bool comp = false) {
+  return (size_t)nd * 32 * (16 + 8 + 4) +
+         (size_t)((pf ? 4 : 2) + (comp ? 1 : 0)) * nd * nw * 32 * 4;
 }
 
-template <bool LAST, bool PF>
+// COMP: FP32_COMP, each value's 16-bit compensation read from loi and
+// written to loo ([ntr][S] like the values)
+template <bool LAST, bool PF, bool COMP>
 __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work W, Opt O,
                                                              TrSet T, SubStep ss, Tile Tl,
                                                              const float4 *__restrict__ lu32,
@@ -662,6 +696,8 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
                                                              const float *__restrict__ rsi,
                                                              double *__restrict__ carry,
                                                              const double *__restrict__ fzs,
+                                                             const int16_t *__restrict__ loi,
+                                                             int16_t *__restrict__ loo,
                                                              int nw, int tile0, int kbase) {
   extern __shared__ __align__(16) unsigned char smem[];
   // the arrays hold layers kbase .. nz-1 (every column of this launch's
@@ -670,7 +706,7 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   float4 *LU = reinterpret_cast<float4 *>(smem);          // [nd][32]
   double *DZ = reinterpret_cast<double *>(LU + nd * 32);  // [nd][32]
   int *colC = reinterpret_cast<int *>(DZ + nd * 32);      // [nd][32]
-  // per buffer (two with PF): A, S float [nd][nw][32]
+  // per buffer (two with PF): A, S float [nd][nw][32]; then R (COMP)
   float *const bufs = reinterpret_cast<float *>(colC + nd * 32);
 
   const int lane = threadIdx.x, wy = threadIdx.y;
@@ -702,6 +738,7 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   const size_t off = (size_t)wy * 32 + lane + (size_t)(kb - kbase) * sa;
   auto A0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + off; };
   auto S0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + (size_t)nd * sa + off; };
+  float *const R0 = COMP ? bufs + (size_t)(PF ? 4 : 2) * nd * sa + off : nullptr;
   const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const double *const D0 = DZ + (kb - kbase) * 32 + lane;
@@ -755,11 +792,14 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
     const float *tr = tri + (size_t)n * G.S;
     float *to = tro + (size_t)n * G.S;
     to[sed] = tbdy ? tr[cbot] : tr[sed];  // sediment ghost (tracers.c:827-830)
+    const int16_t *li = COMP ? loi + (size_t)n * G.S : nullptr;
+    int16_t *lo = COMP ? loo + (size_t)n * G.S : nullptr;
+    if (COMP) lo[sed] = tbdy ? li[cbot] : li[sed];
     const ColSums cs{0.0, 0.0, adv ? fzs[(size_t)n * G.ncol + col] : 0.0};
     if (!PF) cp_async_wait<0>();
     column_finish<LAST, true>(G, F, W, O, T, ss, tc, col, n, tbdy, adv, vdf, A0of(b), S0of(b),
                               sa, L0, C0, D0, tr, to, area, ia, 1.0 / F.dt, cs, carry, steady,
-                              nwarn, bad);
+                              nwarn, bad, R0, li, lo);
     slot = nxt;
     if (PF) b ^= 1;
   }

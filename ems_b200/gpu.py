@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libshoc_tr_gpu.so")
 
 FP64 = 0
 FP32_MIXED = 1
+FP32_COMP = 2
 
 # every entry point include/shoc_tr_gpu.h declares
 EXPORTS = (

@@ -48,6 +48,16 @@ extern "C" {
 #define SHOC_TR_FP64 0        /* plain: FP64 everywhere, matches tracers.c */
 #define SHOC_TR_FP32_MIXED 1  /* FP32 tracers/fluxes/Thomas, FP64 mass sums
                                  and one FP64-residual refinement per solve */
+#define SHOC_TR_FP32_COMP 2   /* FP32_MIXED with a 16-bit compensation stored
+                                 beside every FP32 value (6 bytes a value): a
+                                 value changing by less than half an FP32 ulp
+                                 per step keeps its changes.  Two-kernel
+                                 sub-step only (no fused k_step32); a
+                                 decomposed basin's halo exchange answers
+                                 SHOC_TR_EUNSUPPORTED; columns the general
+                                 path steps (surface crossing a layer face)
+                                 keep their FP32 values and restart their
+                                 compensation at 0 */
 
 typedef struct shoc_tr_gpu shoc_tr_gpu;
 

@@ -42,3 +42,14 @@ def test_create_rejects_bad_arguments_without_device_work(L):
     h = C.c_void_p()
     assert L.shoc_tr_gpu_create(None, None, 1, 0, 0, C.byref(h)) == 7  # SHOC_TR_EARG
     assert not h.value
+
+
+def test_precision_constants_match_header():
+    """The binding's precision codes are the header's SHOC_TR_FP* values."""
+    import re
+    from ems_b200 import gpu
+    with open(os.path.join(ROOT, "include", "shoc_tr_gpu.h")) as f:
+        txt = f.read()
+    want = {m.group(1): int(m.group(2))
+            for m in re.finditer(r"#define SHOC_TR_(FP\w+)\s+(\d+)", txt)}
+    assert want == {"FP64": gpu.FP64, "FP32_MIXED": gpu.FP32_MIXED, "FP32_COMP": gpu.FP32_COMP}
