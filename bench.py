@@ -284,19 +284,66 @@ def kernel_bytes(case, kernel, fp64, comp=False):
     return case.cell_tracers() * 2 * st + case.nwet * fields * s
 
 
+# device bytes per cell of a plain FP64 window besides its two tracer
+# buffers: flow fields, work arrays, LU factors and tile tables (an upper
+# estimate)
+FP64_CELL_BYTES = 480
+
+
+def host_room(case):
+    """Whether the host can hold two FP64 copies of every tracer besides
+    what it holds now (the sequential comparison of host_compare)."""
+    import psutil
+    need = 2 * case.ntr * case.win.sgsiz * 8
+    return psutil.virtual_memory().available > 1.5 * need
+
+
+def host_compare(case, x32, x64, basins):
+    """compare() on the host for two [ntr][sgsiz] tracer arrays: per region
+    (basin, or the whole window) and tracer, over the region's wet cells."""
+    c = case.win.wet_cells()
+    if basins:
+        reg = case.basin2d[case.win.m2d[c]]
+        groups = [c[reg == b] for b in range(len(basins))]
+    else:
+        groups = [c]
+    shape = (len(groups), case.ntr)
+    d = {k: np.zeros(shape) for k in ("max_abs", "max_ref", "sumsq_diff", "sumsq_ref")}
+    for g, cells in enumerate(groups):
+        for n in range(case.ntr):
+            a, r = x32[n, cells], x64[n, cells]
+            e = a - r
+            d["max_abs"][g, n] = np.abs(e).max() if e.size else 0.0
+            d["max_ref"][g, n] = np.abs(r).max() if r.size else 0.0
+            d["sumsq_diff"][g, n] = float(np.dot(e, e))
+            d["sumsq_ref"][g, n] = float(np.dot(r, r))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        d["max_rel"] = np.where(d["max_ref"] > 0, d["max_abs"] / d["max_ref"], np.nan)
+        d["rms_rel"] = np.where(d["sumsq_ref"] > 0, np.sqrt(d["sumsq_diff"] / d["sumsq_ref"]),
+                                np.nan)
+    return d
+
+
 def time_arm(case, prec, local, args, pg, dev, clocks=None):
     """Warm up, then time args.steps graph-replayed steps on the library's
     stream (CUDA events, barrier + synchronize on both sides, max over
     ranks); then one profiled pass for the per-kernel split."""
     import torch
-    from ems_b200 import gpu
+    from ems_b200 import _abi, gpu
     step = gpu.TracerStep(case, precision=prec, device=local)
     step.start()
     tuning, cached = None, None
     if not args.no_autotune:
         # the autotuner's trial steps start from a device copy of the state
         # and put it back (untimed); its choice is cached per GPU and window
-        tuning, cached = step.autotune_ex(2)
+        try:
+            tuning, cached = step.autotune_ex(2)
+        except _abi.StatusError as e:
+            if e.code != 8:  # SHOC_TR_ENOMEM
+                raise
+            # no device memory left for the copy: the default configuration
+            tuning, cached = dict(step.get_tuning(), autotune="skipped: no room for the "
+                                  "state copy"), False
     own0 = step.mass()
     m0 = mass_over_ranks(pg, own0, dev)
     stream = torch.cuda.ExternalStream(step.stream(), device=dev)
@@ -374,20 +421,37 @@ def main():
                    ClockSampler(local))
     step = arm["step"]
     fp64 = None
-    if mixed and not args.no_fp64:
+    basins = getattr(case, "basins", None)
+    both_fit = case.win.sgsiz * (2 * case.ntr * 8 + FP64_CELL_BYTES) < torch.cuda.mem_get_info(dev)[0]
+    if mixed and not args.no_fp64 and not both_fit and not host_room(case):
+        fp64 = {"skipped": "the FP64 window fits neither beside the mixed one on the device "
+                           "nor, sequentially, in host memory"}
+    elif mixed and not args.no_fp64:
+        d = None
+        if not both_fit:
+            # the FP64 window does not fit beside the mixed one: the mixed
+            # run's tracers go to the host, its window is freed, and the two
+            # are compared on the host after the FP64 run
+            x32 = step.download()
+            step.close()
+            step = arm["step"] = None
         ref = time_arm(case, gpu.FP64, local, args, pg, dev)
+        if not both_fit:
+            d = host_compare(case, x32, ref["step"].download(), basins)
+            del x32
         # both precisions have stepped the same inputs the same number of
-        # steps: per tracer (and basin) max |x32 - x64| / max |x64|, on the device
-        basins = getattr(case, "basins", None)
+        # steps: per tracer (and basin) max |x32 - x64| / max |x64|
         if basins:
-            d = step.compare(ref["step"], region=case.basin2d, nregion=len(basins))
+            if d is None:
+                d = step.compare(ref["step"], region=case.basin2d, nregion=len(basins))
             per = [[float(v) for v in d["max_rel"][b, :T]] for b, (_, _, _, T) in
                    enumerate(basins)]
             err = max(max(r) for r in per)
             rms = max(float(v) for b, (_, _, _, T) in enumerate(basins)
                       for v in d["rms_rel"][b, :T])
         else:
-            d = step.compare(ref["step"])
+            if d is None:
+                d = step.compare(ref["step"])
             per = [float(v) for v in d["max_rel"][0]]
             err = max(per)
             rms = float(np.nanmax(d["rms_rel"][0]))
@@ -399,7 +463,8 @@ def main():
                 "speedup_fp32mixed": ref["ms_step"] / arm["ms_step"],
                 "max_rel_err_fp32mixed": err, "max_rms_rel_err_fp32mixed": rms,
                 ("max_rel_err_per_basin" if basins else "max_rel_err_per_tracer"): per,
-                "steps_compared": arm["nsteps"]}
+                "steps_compared": arm["nsteps"],
+                "compared_on": "device" if both_fit else "host (windows run one after the other)"}
         ref["step"].close()
 
     value = job_units / (arm["ms_step"] / 1000.0)
@@ -429,7 +494,7 @@ def main():
     # end to end through the drop-in C-ABI call on pinned host buffers
     S = case.win.sgsiz
     e2e_s = float("nan")
-    if args.e2e_steps > 0 and host_gb <= 16.0:
+    if args.e2e_steps > 0 and host_gb <= 16.0 and step is not None:
         tr_host = case.tr.copy()
         sur, nsur = case.sur_t.copy(), case.nsur_t.copy()
         # every array the call copies is page-locked once, as a host model
@@ -497,7 +562,8 @@ def main():
     }
     if rank == 0:
         print(json.dumps(out))
-    step.close()
+    if step is not None:
+        step.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

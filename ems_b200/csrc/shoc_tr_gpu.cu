@@ -2982,9 +2982,12 @@ void tune_cache_put(const std::string &path, const std::string &key, const shoc_
 
 // Device copy of the resident state (both tracer buffers, mass carry,
 // surface vectors) the trial steps start from.
+// The resident state the autotuner's trial steps start from: the current
+// tracer buffer (and compensation), put back into both ping-pong buffers as
+// shoc_tr_gpu_load_state does.
 struct Snapshot {
   void *tr = nullptr;
-  int16_t *lo = nullptr;  // FP32_COMP: both buffers' compensations
+  int16_t *lo = nullptr;  // FP32_COMP: the current buffer's compensations
   double *carry = nullptr;
   int *sur = nullptr, *nsur = nullptr;
   int cur = 0;
@@ -2994,19 +2997,16 @@ int snap_take(shoc_tr_gpu *h, Snapshot &s) {
   const size_t tb = (size_t)h->ntr * h->S * h->esize;
   const size_t cb = (size_t)h->ntr * h->ncol * sizeof(double);
   const size_t ib = (size_t)h->ncol * sizeof(int);
-  CK(cudaMallocAsync(&s.tr, tb ? 2 * tb : 1, h->stream));
+  CK(cudaMallocAsync(&s.tr, tb ? tb : 1, h->stream));
   if (h->fu.carry) CK(cudaMallocAsync((void **)&s.carry, cb ? cb : 1, h->stream));
   CK(cudaMallocAsync((void **)&s.sur, 2 * ib, h->stream));
   s.nsur = s.sur + h->ncol;
   s.cur = h->cur;
-  for (int b = 0; b < 2; b++)
-    CK(cudaMemcpyAsync((char *)s.tr + b * tb, h->tr[b], tb, cudaMemcpyDeviceToDevice, h->stream));
+  CK(cudaMemcpyAsync(s.tr, h->tr[h->cur], tb, cudaMemcpyDeviceToDevice, h->stream));
   if (h->comp) {
     const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
-    CK(cudaMallocAsync((void **)&s.lo, lb ? 2 * lb : 1, h->stream));
-    for (int b = 0; b < 2; b++)
-      CK(cudaMemcpyAsync((char *)s.lo + b * lb, h->lo[b], lb, cudaMemcpyDeviceToDevice,
-                         h->stream));
+    CK(cudaMallocAsync((void **)&s.lo, lb ? lb : 1, h->stream));
+    CK(cudaMemcpyAsync(s.lo, h->lo[h->cur], lb, cudaMemcpyDeviceToDevice, h->stream));
   }
   if (s.carry) CK(cudaMemcpyAsync(s.carry, h->fu.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(s.sur, h->W.sur_t, ib, cudaMemcpyDeviceToDevice, h->stream));
@@ -3020,13 +3020,11 @@ int snap_restore(shoc_tr_gpu *h, const Snapshot &s) {
   const size_t ib = (size_t)h->ncol * sizeof(int);
   h->cur = s.cur;
   for (int b = 0; b < 2; b++)
-    CK(cudaMemcpyAsync(h->tr[b], (const char *)s.tr + b * tb, tb, cudaMemcpyDeviceToDevice,
-                       h->stream));
+    CK(cudaMemcpyAsync(h->tr[b], s.tr, tb, cudaMemcpyDeviceToDevice, h->stream));
   if (s.lo) {
     const size_t lb = (size_t)h->ntr * h->S * sizeof(int16_t);
     for (int b = 0; b < 2; b++)
-      CK(cudaMemcpyAsync(h->lo[b], (const char *)s.lo + b * lb, lb, cudaMemcpyDeviceToDevice,
-                         h->stream));
+      CK(cudaMemcpyAsync(h->lo[b], s.lo, lb, cudaMemcpyDeviceToDevice, h->stream));
   }
   if (s.carry) CK(cudaMemcpyAsync(h->fu.carry, s.carry, cb, cudaMemcpyDeviceToDevice, h->stream));
   CK(cudaMemcpyAsync(h->W.sur_t, s.sur, ib, cudaMemcpyDeviceToDevice, h->stream));
@@ -3092,9 +3090,10 @@ int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tu
   }
   Snapshot snap;
   int rc = snap_take(h, snap);
-  if (rc) {
+  if (rc) {  // no room for the copy: nothing has run, the handle is unchanged
+    cudaGetLastError();
     snap_free(h, snap);
-    return rc;
+    return SHOC_TR_ENOMEM;
   }
   const bool prof0 = h->profile;
   shoc_tr_tuning win = base;

@@ -287,6 +287,9 @@ int shoc_tr_gpu_set_tuning(shoc_tr_gpu *h, const shoc_tr_tuning *t);
  * $HOME/.cache/shoc_tr_gpu/tuning.txt, "off" for none): a cached choice is
  * applied without trial steps and *from_cache set to 1.  best / from_cache
  * may be NULL.  Call after the flow is set and any earlier step synced.
+ * The device copy holds one tracer buffer (ntr x S values, plus their
+ * compensations with SHOC_TR_FP32_COMP); without room for it the call
+ * returns SHOC_TR_ENOMEM and changes nothing.
  * shoc_tr_gpu_autotune is autotune_ex without the cache, returning the
  * tracers per block. */
 int shoc_tr_gpu_autotune_ex(shoc_tr_gpu *h, int steps, int use_cache, shoc_tr_tuning *best,
