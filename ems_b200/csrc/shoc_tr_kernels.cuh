@@ -69,6 +69,18 @@ __device__ __forceinline__ int16_t lo_enc(double v, float v32) {
   if (!(q >= -32767.0 && q <= 32767.0)) return 0;  // NaN / inf
   return (int16_t)fmin(fmax(q, -16383.0), 16383.0);
 }
+// lo_enc, and what the returned compensation decodes to (lo_dec) in dec
+__device__ __forceinline__ int16_t lo_round(double v, float v32, double &dec) {
+  const int k = lo_exp(v32);
+  const double q = rint((v - (double)v32) * pow2(-k));
+  if (!(q >= -32767.0 && q <= 32767.0)) {  // NaN / inf
+    dec = 0.0;
+    return 0;
+  }
+  const double qc = fmin(fmax(q, -16383.0), 16383.0);
+  dec = qc * pow2(k);
+  return (int16_t)qc;
+}
 __device__ __forceinline__ double lo_dec(int16_t q, float v32) {
   return (double)q * pow2(lo_exp(v32));
 }
