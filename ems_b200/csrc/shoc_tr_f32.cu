@@ -17,8 +17,13 @@ void adv(int grid, cudaStream_t st, const Geo &G, const Flow32 &F3, const Work &
          const SubStep &ss, const Tile &Tl, const f32::Face2 *fx2, const f32::Face2 *fy2,
          const float *tin, float *tout, float *rnd, double *fzs, int hd,
          const int16_t *loi) {
-  k_adv32<Q, U, M><<<grid, kAdv32Block, M != 0 ? kAdvSmem : 0, st>>>(G, F3, W, T, ss, Tl, fx2, fy2,
-                                                                  tin, tout, rnd, fzs, hd, loi);
+  const size_t sm = M != 0 ? kAdvSmem : 0;
+  if (loi)
+    k_adv32<Q, U, M, true><<<grid, kAdv32Block, sm, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin,
+                                                          tout, rnd, fzs, hd, loi);
+  else
+    k_adv32<Q, U, M, false><<<grid, kAdv32Block, sm, st>>>(G, F3, W, T, ss, Tl, fx2, fy2, tin,
+                                                           tout, rnd, fzs, hd, nullptr);
 }
 template <bool Q, bool U>
 void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F3,
@@ -37,15 +42,19 @@ void adv_mode(int mode, int grid, cudaStream_t st, const Geo &G, const Flow32 &F
 cudaError_t tile32_set_smem_attr() {
   cudaError_t e = cudaSuccess;
   const int a = (int)kAdvSmem;
-  const cudaError_t r[16] = {
+  const cudaError_t r[24] = {
       attr(k_vd32<true, false, false>),  attr(k_vd32<false, false, false>),
       attr(k_vd32<true, true, false>),   attr(k_vd32<false, true, false>),
       attr(k_vd32<true, false, true>),   attr(k_vd32<false, false, true>),
       attr(k_vd32<true, true, true>),    attr(k_vd32<false, true, true>),
-      attr(k_adv32<true, true, 1>, a), attr(k_adv32<true, true, 2>, a),
-      attr(k_adv32<true, false, 1>, a), attr(k_adv32<true, false, 2>, a),
-      attr(k_adv32<false, true, 1>, a), attr(k_adv32<false, true, 2>, a),
-      attr(k_adv32<false, false, 1>, a), attr(k_adv32<false, false, 2>, a)};
+      attr(k_adv32<true, true, 1, false>, a), attr(k_adv32<true, true, 2, false>, a),
+      attr(k_adv32<true, false, 1, false>, a), attr(k_adv32<true, false, 2, false>, a),
+      attr(k_adv32<false, true, 1, false>, a), attr(k_adv32<false, true, 2, false>, a),
+      attr(k_adv32<false, false, 1, false>, a), attr(k_adv32<false, false, 2, false>, a),
+      attr(k_adv32<true, true, 1, true>, a), attr(k_adv32<true, true, 2, true>, a),
+      attr(k_adv32<true, false, 1, true>, a), attr(k_adv32<true, false, 2, true>, a),
+      attr(k_adv32<false, true, 1, true>, a), attr(k_adv32<false, true, 2, true>, a),
+      attr(k_adv32<false, false, 1, true>, a), attr(k_adv32<false, false, 2, true>, a)};
   for (auto x : r)
     if (x != cudaSuccess) e = x;
   return e;

@@ -1567,6 +1567,8 @@ int shoc_tr_gpu_create(const shoc_tr_geom *g, const shoc_tr_opts *o, int ntr, in
   TRY(dupload<double>(h, (double **)&F.Kz, nullptr, S));
   if (f32p) {  // the FP32-mixed kernels take the FP64 volume fluxes
     h->F3.u1flux3d = F.u1flux3d;
+    h->F3.u1_64 = F.u1;
+    h->F3.u2_64 = F.u2;
     h->F3.u2flux3d = F.u2flux3d;
     h->F3.w64 = F.w;
   }

@@ -47,43 +47,33 @@ constexpr int COL_STAGED = 32;  // handled by the FP32-mixed column-tile kernels
 // ---------------------------------------------------------------------------
 // 16-bit compensation of an FP32-stored value (the SHOC_TR_FP32_COMP
 // precision).  A value v stored as v32 = (float)v (round to nearest, so
-// |v - v32| <= ulp(v32) / 2) keeps q = rint((v - v32) / ulp(v32) * 2^15),
-// |q| <= 2^14, beside it; v32 + q ulp(v32) 2^-15 gives v back to about 2^-39
-// of its size.  Without it a value whose change per step is below half an
-// FP32 ulp is rounded back to the same FP32 number every step.  q is held
-// to |q| <= 2^14 - 1, so the decoded value lies strictly inside v32's
-// rounding interval: converting it to FP32 and encoding again gives v32 and
-// q back (the drop-in step's trip through FP64 host arrays changes nothing).
-
-// 2^k for -1022 <= k <= 1023, exactly
-__device__ __forceinline__ double pow2(int k) {
-  return __longlong_as_double((long long)(k + 1023) << 52);
+// |v - v32| <= ulp(v32) / 2) keeps beside it the residual r = v - v32 as a
+// bfloat16 (the upper half of r's FP32 bits: 8 significant bits, rounded
+// toward zero, as is r's own conversion to FP32); v32 + r gives v back to
+// about 2^-32 of its size, and reading
+// it back is one shift.  Without it a value whose change per step is below
+// half an FP32 ulp is rounded back to the same FP32 number every step.
+// Rounding r toward zero keeps the decoded value inside v32's rounding
+// interval (at most half an ulp away, a tie only where v itself was one and
+// v32 is the even neighbour): converting it to FP32 gives v32 back and
+// encoding again gives the same bits, so the drop-in step's trip through
+// FP64 host arrays changes nothing.
+__device__ __forceinline__ float lo_val(int16_t q) {
+  return __uint_as_float((uint32_t)(uint16_t)q << 16);
 }
-// the exponent of ulp(v32) minus 15
-__device__ __forceinline__ int lo_exp(float v32) {
-  const int e = (int)((__float_as_uint(v32) >> 23) & 0xffu);
-  return (e == 0 ? 1 : e) - 150 - 15;
+__device__ __forceinline__ int16_t lo_bits(float r) {
+  return isfinite(r) ? (int16_t)(__float_as_uint(r) >> 16) : (int16_t)0;
 }
 __device__ __forceinline__ int16_t lo_enc(double v, float v32) {
-  const double q = rint((v - (double)v32) * pow2(-lo_exp(v32)));
-  if (!(q >= -32767.0 && q <= 32767.0)) return 0;  // NaN / inf
-  return (int16_t)fmin(fmax(q, -16383.0), 16383.0);
+  return lo_bits(__double2float_rz(v - (double)v32));
 }
-// lo_enc, and what the returned compensation decodes to (lo_dec) in dec
+// lo_enc, and what the returned compensation decodes to in dec
 __device__ __forceinline__ int16_t lo_round(double v, float v32, double &dec) {
-  const int k = lo_exp(v32);
-  const double q = rint((v - (double)v32) * pow2(-k));
-  if (!(q >= -32767.0 && q <= 32767.0)) {  // NaN / inf
-    dec = 0.0;
-    return 0;
-  }
-  const double qc = fmin(fmax(q, -16383.0), 16383.0);
-  dec = qc * pow2(k);
-  return (int16_t)qc;
+  const int16_t q = lo_enc(v, v32);
+  dec = (double)lo_val(q);
+  return q;
 }
-__device__ __forceinline__ double lo_dec(int16_t q, float v32) {
-  return (double)q * pow2(lo_exp(v32));
-}
+__device__ __forceinline__ double lo_dec(int16_t q, float) { return (double)lo_val(q); }
 
 // 2D face metrics of one direction, precomputed per surface-layer cell:
 // d = d3/d4 weight, db/df = 2/(h_m+h_0), 2/(h_0+h_p), h_m/h_0/h_p = metric
@@ -138,6 +128,7 @@ struct Work {
 
 // FP32 copies of the flow fields (FP32-mixed path), made by set_flow.
 struct Flow32 {
+  const double *u1_64, *u2_64;  // the FP64 velocities (FP32_COMP face set-up)
   const float *u1, *u2, *w;  // FP32 copies for the Courant numbers
   const double *u1flux3d, *u2flux3d, *w64;  // the FP64 arrays of Flow: volume fluxes
   const float *khx, *khy;  // dzu1 h2au1 u1kh / h1au1 and the e2 analogue

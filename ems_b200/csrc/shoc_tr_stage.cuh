@@ -47,6 +47,7 @@ namespace f32 {
 struct Face {
   float wg, wa, ircr, K;
   double U;
+  double V;  // FP32_COMP: U / |cr| in FP64 (set_face64; 0 otherwise)
   int bits;
 };
 constexpr int FB_POS = 1, FB_NEG = 2, FB_ULT = 4;
@@ -60,7 +61,7 @@ struct Face2 {
 __device__ __forceinline__ void face_zero(Face &f) {
   f.wg = f.wa = 0.f;
   f.ircr = f.K = 0.f;
-  f.U = 0.0;
+  f.U = f.V = 0.0;
   f.bits = 0;
 }
 
@@ -92,6 +93,39 @@ __device__ __forceinline__ void set_face(Face &f, bool quick, float cr, float d,
   }
   f.ircr = cr != 0.f ? __frcp_rn(fabsf(cr)) : 0.f;
   f.U = U;
+  f.V = 0.0;
+  f.K = K;
+}
+
+// FP32_COMP: set_face from the FP64 Courant number and metric factors, each
+// weight formed in FP64 and rounded once, and V = U / |cr| in FP64: the
+// volume flux per unit of tc - tu of a face ULTIMATE caps at its Courant
+// bound (tu + (tc - tu) / |cr|).  That cap does not shrink with the Courant
+// number, so it is applied in FP64 to compensated values (face_c).
+__device__ __forceinline__ void set_face64(Face &f, bool quick, double cr, double d, double Ap,
+                                           double Bp, double Am, double Bm, double U, bool ult,
+                                           float K) {
+  f.bits = (cr > 0.0 ? FB_POS : 0) | (cr < 0.0 ? FB_NEG : 0) | ((ult && cr != 0.0) ? FB_ULT : 0);
+  if (quick) {
+    const double a = d - 0.5 * cr, b = (1.0 - cr * cr) / 6.0;
+    if (cr > 0.0) {
+      f.wg = (float)(a - b * Ap);
+      f.wa = (float)(-b * Bp);
+    } else if (cr < 0.0) {
+      f.wg = (float)(a + b * Bm);
+      f.wa = (float)(-b * Am);
+    } else {
+      f.wg = (float)d;
+      f.wa = 0.f;
+    }
+  } else {
+    f.wa = (float)(cr > 0.0 ? 0.5 * (1.0 - cr) : 0.5 * (1.0 + cr));
+    f.wg = 0.f;
+  }
+  const double ir = cr != 0.0 ? 1.0 / fabs(cr) : 0.0;
+  f.ircr = (float)ir;
+  f.U = U;
+  f.V = U * ir;
   f.K = K;
 }
 
@@ -145,6 +179,73 @@ __device__ __forceinline__ double face(const Face &f, bool adv, bool hd, float t
     flux = __dmul_rn((double)F, f.U);
   }
   if (hd) flux = __dsub_rn(flux, (double)__fmul_rn(f.K, __fsub_rn(t0, tm1)));
+  return flux;
+}
+
+// FP32_COMP face flux: face() on compensated values, each value the stored
+// FP32 one (tm2..tp1) plus its compensation (lm2..lp1).  Differences are
+// the stored difference plus the compensations' difference (FP32, accurate
+// to their own size), so the limiter decides as on the FP64 values.  The face
+// value is a base value (a stored value) plus a correction (its compensation
+// and the FP32 increment), and the flux U (base + correction) in FP64; a face
+// capped at ULTIMATE's Courant bound carries U (tu + lu) + V (tc - tu), the
+// second term with the FP64 V.
+template <bool QUICK, bool ULT>
+__device__ __forceinline__ double face_c(const Face &f, bool adv, bool hd, float tm2, float tm1,
+                                         float t0, float tp1, float lm2, float lm1, float l0,
+                                         float lp1) {
+  const bool pos = (f.bits & FB_POS) != 0;
+  const float tu = pos ? tm2 : tp1, tc = pos ? tm1 : t0;
+  const float lu = pos ? lm2 : lp1, lc = pos ? lm1 : l0;
+  const float g01 = __fadd_rn(__fsub_rn(t0, tm1), __fsub_rn(l0, lm1));  // t0 - tm1
+  float base, lbase, inc;
+  if (QUICK) {
+    const float e = __fadd_rn(__fsub_rn(tu, tc), __fsub_rn(lu, lc));  // tu - tc
+    inc = __fmaf_rn(f.wa, e, __fmul_rn(f.wg, g01));
+    base = tm1;
+    lbase = lm1;
+  } else {
+    const bool neg = (f.bits & FB_NEG) != 0;
+    const float p = pos ? __fadd_rn(__fsub_rn(tm1, tm2), __fsub_rn(lm1, lm2)) : g01;
+    const float q = pos ? g01 : __fadd_rn(__fsub_rn(tp1, t0), __fsub_rn(lp1, l0));
+    const float den = pos ? __fadd_rn(__fsub_rn(t0, tm2), __fsub_rn(l0, lm2))
+                          : __fadd_rn(__fsub_rn(tp1, tm1), __fsub_rn(lp1, lm1));
+    const float pq = __fmul_rn(p, q);
+    const float df = pq > 0.f ? __fmul_rn(2.f, __fdiv_rn(pq, den)) : 0.f;
+    inc = pos ? __fmul_rn(f.wa, df) : (neg ? -__fmul_rn(f.wa, df) : 0.f);
+    base = pos ? tm1 : (neg ? t0 : 0.f);
+    lbase = pos ? lm1 : (neg ? l0 : 0.f);
+  }
+  int br = 0;  // 0 the face value, 1 the Courant cap, 2 tc, 3 td
+  if (ULT && (f.bits & FB_ULT)) {
+    const float td = pos ? t0 : tm1, ld = pos ? l0 : lm1;
+    const float dc = __fadd_rn(__fsub_rn(tc, tu), __fsub_rn(lc, lu));
+    const float dd = __fadd_rn(__fsub_rn(td, tu), __fsub_rn(ld, lu));
+    const float dF = __fadd_rn(__fadd_rn(__fsub_rn(base, tu), __fsub_rn(lbase, lu)), inc);
+    const float sg = dd < 0.f ? -1.f : 1.f;
+    const float d = fabsf(dd), c = __fmul_rn(dc, sg), a = __fmul_rn(dF, sg);
+    const float q = __fmul_rn(c, f.ircr);
+    if (a > q) br = 1;
+    if (a < c) br = 2;
+    if (a > d) br = 3;
+    if (!(c >= 0.f && c <= d)) br = 2;
+    if (br >= 2) {
+      base = br == 2 ? tc : td;
+      lbase = br == 2 ? lc : ld;
+      inc = 0.f;
+    }
+  }
+  double flux = 0.0;
+  if (adv) {
+    // one expression for every branch: U (b + lb) + Vq dq
+    const bool cap = br == 1;
+    const float b = cap ? tu : base;
+    const float lb = cap ? lu : __fadd_rn(lbase, inc);
+    const float dq = cap ? __fadd_rn(__fsub_rn(tc, tu), __fsub_rn(lc, lu)) : 0.f;
+    flux = __fma_rn(cap ? f.V : 0.0, (double)dq,
+                    __dmul_rn(f.U, __dadd_rn((double)b, (double)lb)));
+  }
+  if (hd) flux = __dsub_rn(flux, (double)__fmul_rn(f.K, g01));
   return flux;
 }
 

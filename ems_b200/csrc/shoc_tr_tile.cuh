@@ -178,8 +178,10 @@ constexpr int kMaxTracers = 256;   // tracers a handle of the FP32-mixed path ma
 
 // MODE: 0 tracers with their own advect / diffuse flags, 1 every advected
 // tracer advected without horizontal diffusion, 2 advected with it.
-template <bool QUICK, bool ULT, int MODE>
-__global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
+// COMP (FP32_COMP): faces set up in FP64 (set_face64) and every stencil
+// value read with its compensation from loi (face_c); 4 blocks per SM.
+template <bool QUICK, bool ULT, int MODE, bool COMP>
+__global__ void __launch_bounds__(kAdv32Block, COMP ? 4 : kAdv32MinBlocks) k_adv32(Geo G, Flow32 F3, Work W, TrSet T,
                                                      SubStep ss, Tile Tl,
                                                      const f32::Face2 *__restrict__ fx2,
                                                      const f32::Face2 *__restrict__ fy2,
@@ -248,7 +250,49 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
   face_zero(fzb);
   face_zero(fzt);
   double idz = 0.0, ia = 0.0;
-  if (on) {
+  if (on && COMP) {
+    // FP64 Courant numbers (tracers.c:730-736) and metric factors
+    auto hset = [&](Face &f, bool wet, bool eb, double u, double h, const Face2D &m, double U,
+                    float K) {
+      if (!wet) {
+        face_zero(f);
+      } else if (!QUICK && !eb) {  // Van Leer advects interior faces only
+        face_zero(f);
+        f.K = K;
+      } else {
+        set_face64(f, QUICK, u * dtu / h, m.d, m.db * m.hm, m.db * m.h0, m.df * m.h0,
+                   m.df * m.hp, U, ULT && eb, K);
+      }
+    };
+    // the face at the bottom of cell cc (below it zm, above it zp), from the
+    // work arrays as quickest_zface takes them
+    auto zset = [&](Face &f, int cc, int zm, int zp) {
+      const double w90 = W.w9[cc];
+      set_face64(f, QUICK, F3.w64[cc] * dtu / (w90 * 1.0), W.w5[cc], W.dbz[cc] * W.w9[zm],
+                 W.dbz[cc] * w90, W.dfz[cc] * w90, W.dfz[cc] * W.w9[zp],
+                 __dmul_rn(F3.w64[cc], dtu), ULT, 0.f);
+    };
+    hset(fw, fl & CF_WET, fl & CF_E1, F3.u1_64[c], G.h1au1[c2], G.fx[c2], F3.u1flux3d[c],
+         hdf ? F3.khx[c] : 0.f);
+    hset(fs, fl & CF_WET, fl & CF_E2, F3.u2_64[c], G.h2au2[c2], G.fy[c2], F3.u2flux3d[c],
+         hdf ? F3.khy[c] : 0.f);
+    if (fl & FL_YP_WET) {
+      const int yp = n1.w;
+      hset(fn, true, fl & FL_YP_E2, F3.u2_64[yp], G.h2au2[me.y], G.fy[me.y], F3.u2flux3d[yp],
+           hdf ? F3.khy[yp] : 0.f);
+    }
+    if (!sxp1 && (fl & FL_XP_WET)) {
+      const int xp = n1.y;
+      hset(fe, true, fl & FL_XP_E1, F3.u1_64[xp], G.h1au1[me.x], G.fx[me.x], F3.u1flux3d[xp],
+           hdf ? F3.khx[xp] : 0.f);
+    }
+    if (k <= ks) {
+      zset(fzb, c, nzv.x, nzv.z);
+      if (k < ks) zset(fzt, nzv.z, c, nzv.w);  // the bottom face of the cell above
+    }
+    idz = 1.0 / W.dz[c];
+    ia = 1.0 / G.cellarea[c2];
+  } else if (on) {
     const Face2 mx = fx2[c2], my = fy2[c2];
     hface(fw, fl & CF_WET, fl & CF_E1, QUICK, ULT, __fmul_rn(__fmul_rn(F3.u1[c], fdtu), mx.ih),
           F3.u1flux3d[c], hdf ? F3.khx[c] : 0.f, mx);
@@ -320,12 +364,16 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       cp_async_commit();
     };
     issue(0, 0);
-    // FP32_COMP: the cell's own compensation, loaded one tracer ahead
-    static_assert(U == 1, "the compensation is prefetched for one tracer at a time");
-    const bool lon = loi && on;
-    int16_t qcur = (lon && ntb > 0) ? loi[(size_t)sTr[0] * G.S + c] : (int16_t)0, qnext = 0;
-    for (int s0 = 0, g = 0; s0 < ntb; s0 += U, ++g, qcur = qnext) {
-      qnext = (lon && s0 + 1 < ntb) ? loi[(size_t)sTr[s0 + 1] * G.S + c] : (int16_t)0;
+    static_assert(U == 1, "the compensations are loaded for one tracer at a time");
+    for (int s0 = 0, g = 0; s0 < ntb; s0 += U, ++g) {
+      // COMP: the stencil's compensations, in flight while the stencil
+      // values' copies complete
+      int16_t lq[NQ];
+      if constexpr (COMP) {
+        const int16_t *Lp = loi + (size_t)sTr[s0] * G.S;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) lq[q] = Lp[idx[q]];
+      }
       if (s0 + U < ntb) {
         issue(s0 + U, (g + 1) & 1);
         cp_async_wait<1>();
@@ -340,9 +388,6 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         const int s = s0 + u;
         if (s >= ntb) break;
         const float *v = P + u * NQ * kAdv32Block;
-        // FP32_COMP: the cell's own value with its compensation (the stencil
-        // neighbours are read as stored)
-        const int16_t q0 = qcur;
         const float t0 = v[0];
         const float tym1 = v[1 * kAdv32Block], tym2 = v[2 * kAdv32Block];
         const float typ1 = v[3 * kAdv32Block], typ2 = v[4 * kAdv32Block];
@@ -350,20 +395,45 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         const float tp1 = v[7 * kAdv32Block], tp2 = v[8 * kAdv32Block];
         const float txm1 = v[9 * kAdv32Block], txm2 = v[10 * kAdv32Block];
         const float txp1 = v[11 * kAdv32Block], txp2 = v[12 * kAdv32Block];
-        const double Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
-        const double Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
-        const double Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
-        const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
-        const double Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
-        const double Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.0;
+        double Fxw, Fys, Fyn, Fxe, Fzb;
+        float l0 = 0.f, lm1 = 0.f, lm2 = 0.f, lp1 = 0.f, lp2 = 0.f;
+        if constexpr (COMP) {
+          l0 = lo_val(lq[0]);
+          const float lym1 = lo_val(lq[1]), lym2 = lo_val(lq[2]);
+          const float lyp1 = lo_val(lq[3]), lyp2 = lo_val(lq[4]);
+          lm1 = lo_val(lq[5]);
+          lm2 = lo_val(lq[6]);
+          lp1 = lo_val(lq[7]);
+          lp2 = lo_val(lq[8]);
+          const float lxm1 = lo_val(lq[9]), lxm2 = lo_val(lq[10]);
+          const float lxp1 = lo_val(lq[11]), lxp2 = lo_val(lq[12]);
+          Fxw = face_c<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1, lxm2, lxm1, l0, lxp1);
+          Fys = face_c<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1, lym2, lym1, l0, lyp1);
+          Fyn = face_c<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2, lym1, l0, lyp1, lyp2);
+          const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
+          Fxe = sxp1 ? Fnext
+                     : face_c<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2, lxm1, l0, lxp1,
+                                          lxp2);
+          Fzb = zf ? face_c<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1, lm2, lm1, l0, lp1)
+                   : 0.0;
+        } else {
+          Fxw = face<QUICK, ULT>(fw, true, HD, txm2, txm1, t0, txp1);
+          Fys = face<QUICK, ULT>(fs, true, HD, tym2, tym1, t0, typ1);
+          Fyn = face<QUICK, ULT>(fn, true, HD, tym1, t0, typ1, typ2);
+          const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
+          Fxe = sxp1 ? Fnext : face<QUICK, ULT>(fe, true, HD, txm1, t0, txp1, txp2);
+          Fzb = zf ? face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1) : 0.0;
+        }
         const int n = sTr[s];
         if (!on || n >= ntc) continue;
         // FP64 flux divergence (tracers.c:888-892)
         const double dtr = ((Fxe - Fxw) + (Fyn - Fys)) * dtu;
         double a = dtr;
         if (zt) {
-          const double Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
-          const double t0d = loi ? (double)t0 + lo_dec(q0, t0) : (double)t0;
+          const double Fzt =
+              COMP ? face_c<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2, lm1, l0, lp1, lp2)
+                   : face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, tp2);
+          const double t0d = COMP ? (double)t0 + (double)l0 : (double)t0;
           a = t0d - (dtr * ia + (Fzt - Fzb)) * idz;
         } else if (zf) {
           fzs[(size_t)n * G.ncol + col] = Fzb;
@@ -376,6 +446,7 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
   } else {
   for (int s0 = 0; s0 < ntb; s0 += U) {
     float v[U][13];  // t0, y-2..y+2, z-2..z+2, x-2..x+2 (off-tile x only)
+    float lv[U][13];  // COMP: their compensations (x-neighbours read for every cell)
     int nn[U], tf[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -398,6 +469,22 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       v[u][10] = (hor && !sxm2) ? tr[n2.x] : 0.f;
       v[u][11] = (hor && !sxp1) ? tr[n1.y] : 0.f;
       v[u][12] = (hor && !sxp1 && !sxp2) ? tr[n2.y] : 0.f;
+      if constexpr (COMP) {
+        const int16_t *L = loi + (size_t)nn[u] * G.S;
+        lv[u][0] = on && s < ntb ? lo_val(L[c]) : 0.f;
+        lv[u][1] = hor ? lo_val(L[n1.z]) : 0.f;
+        lv[u][2] = hor ? lo_val(L[n2.z]) : 0.f;
+        lv[u][3] = hor ? lo_val(L[n1.w]) : 0.f;
+        lv[u][4] = hor ? lo_val(L[n2.w]) : 0.f;
+        lv[u][5] = vz ? lo_val(L[vm1]) : 0.f;
+        lv[u][6] = vz ? lo_val(L[vm2]) : 0.f;
+        lv[u][7] = vz ? lo_val(L[vp1]) : 0.f;
+        lv[u][8] = (vz && zt) ? lo_val(L[vp2]) : 0.f;
+        lv[u][9] = hor ? lo_val(L[n1.x]) : 0.f;
+        lv[u][10] = hor ? lo_val(L[n2.x]) : 0.f;
+        lv[u][11] = hor ? lo_val(L[n1.y]) : 0.f;
+        lv[u][12] = hor ? lo_val(L[n2.y]) : 0.f;
+      }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -413,17 +500,37 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
         const float txm2 = sxm2 ? u2v : v[u][10];
         const float txp1 = sxp1 ? d1v : v[u][11];
         const float tym1 = v[u][1], tym2 = v[u][2], typ1 = v[u][3], typ2 = v[u][4];
-        Fxw = face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1);
-        Fys = face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1);
-        Fyn = face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2);
-        if (!sxp1) {
-          const float txp2 = sxp2 ? d2v : v[u][12];
-          Fxe = face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2);
-        }
-        if (adv && zf) {
-          const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7];
-          Fzb = face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1);
-          if (zt) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, v[u][8]);
+        if constexpr (COMP) {
+          const float *l = lv[u];
+          Fxw = face_c<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1, l[10], l[9], l[0], l[11]);
+          Fys = face_c<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1, l[2], l[1], l[0], l[3]);
+          Fyn = face_c<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2, l[1], l[0], l[3], l[4]);
+          if (!sxp1) {
+            const float txp2 = sxp2 ? d2v : v[u][12];
+            Fxe = face_c<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2, l[9], l[0], l[11],
+                                     l[12]);
+          }
+          if (adv && zf) {
+            const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7];
+            Fzb = face_c<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1, l[6], l[5], l[0],
+                                     l[7]);
+            if (zt)
+              Fzt = face_c<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, v[u][8], l[5], l[0],
+                                       l[7], l[8]);
+          }
+        } else {
+          Fxw = face<QUICK, ULT>(fw, adv, hd, txm2, txm1, t0, txp1);
+          Fys = face<QUICK, ULT>(fs, adv, hd, tym2, tym1, t0, typ1);
+          Fyn = face<QUICK, ULT>(fn, adv, hd, tym1, t0, typ1, typ2);
+          if (!sxp1) {
+            const float txp2 = sxp2 ? d2v : v[u][12];
+            Fxe = face<QUICK, ULT>(fe, adv, hd, txm1, t0, txp1, txp2);
+          }
+          if (adv && zf) {
+            const float tm1 = v[u][5], tm2 = v[u][6], tp1 = v[u][7];
+            Fzb = face<QUICK, ULT>(fzb, true, false, tm2, tm1, t0, tp1);
+            if (zt) Fzt = face<QUICK, ULT>(fzt, true, false, tm1, t0, tp1, v[u][8]);
+          }
         }
       }
       const double Fnext = __shfl_down_sync(FULL, Fxw, 1);
@@ -433,8 +540,7 @@ __global__ void __launch_bounds__(kAdv32Block, kAdv32MinBlocks) k_adv32(Geo G, F
       const double dtr = ((Fxe - Fxw) + (Fyn - Fys)) * dtu;
       double a = dtr;
       if (zt) {
-        const double t0d =
-            loi ? (double)t0 + lo_dec(loi[(size_t)nn[u] * G.S + c], t0) : (double)t0;
+        const double t0d = COMP ? (double)t0 + (double)lv[u][0] : (double)t0;
         a = t0d - (dtr * ia + (Fzt - Fzb)) * idz;
       }
       else if (k == ks)
