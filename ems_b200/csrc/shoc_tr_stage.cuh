@@ -198,10 +198,10 @@ __device__ __forceinline__ double face_c(const Face &f, bool adv, bool hd, float
   const float tu = pos ? tm2 : tp1, tc = pos ? tm1 : t0;
   const float lu = pos ? lm2 : lp1, lc = pos ? lm1 : l0;
   const float g01 = __fadd_rn(__fsub_rn(t0, tm1), __fsub_rn(l0, lm1));  // t0 - tm1
+  const float dc = __fadd_rn(__fsub_rn(tc, tu), __fsub_rn(lc, lu));   // tc - tu
   float base, lbase, inc;
   if (QUICK) {
-    const float e = __fadd_rn(__fsub_rn(tu, tc), __fsub_rn(lu, lc));  // tu - tc
-    inc = __fmaf_rn(f.wa, e, __fmul_rn(f.wg, g01));
+    inc = __fmaf_rn(f.wa, -dc, __fmul_rn(f.wg, g01));
     base = tm1;
     lbase = lm1;
   } else {
@@ -216,35 +216,30 @@ __device__ __forceinline__ double face_c(const Face &f, bool adv, bool hd, float
     base = pos ? tm1 : (neg ? t0 : 0.f);
     lbase = pos ? lm1 : (neg ? l0 : 0.f);
   }
-  int br = 0;  // 0 the face value, 1 the Courant cap, 2 tc, 3 td
-  if (ULT && (f.bits & FB_ULT)) {
+  // the face value as base + lb, and the capped face's difference dq
+  float b = base, lb = __fadd_rn(lbase, inc), dq = 0.f;
+  if (ULT) {
     const float td = pos ? t0 : tm1, ld = pos ? l0 : lm1;
-    const float dc = __fadd_rn(__fsub_rn(tc, tu), __fsub_rn(lc, lu));
-    const float dd = __fadd_rn(__fsub_rn(td, tu), __fsub_rn(ld, lu));
-    const float dF = __fadd_rn(__fadd_rn(__fsub_rn(base, tu), __fsub_rn(lbase, lu)), inc);
+    const float dd = __fadd_rn(__fsub_rn(td, tu), __fsub_rn(ld, lu));  // td - tu
+    // F - tu: the base is tc, or td for QUICKEST with the flow negative
+    const float dF = __fadd_rn((QUICK && !pos) ? dd : dc, inc);
     const float sg = dd < 0.f ? -1.f : 1.f;
     const float d = fabsf(dd), c = __fmul_rn(dc, sg), a = __fmul_rn(dF, sg);
     const float q = __fmul_rn(c, f.ircr);
-    if (a > q) br = 1;
-    if (a < c) br = 2;
-    if (a > d) br = 3;
-    if (!(c >= 0.f && c <= d)) br = 2;
-    if (br >= 2) {
-      base = br == 2 ? tc : td;
-      lbase = br == 2 ? lc : ld;
-      inc = 0.f;
-    }
+    // the limiter's cases in the order that decides them: outside the
+    // monotone range tc; above td td; below tc tc; above the cap the cap
+    const bool lim = (f.bits & FB_ULT) != 0;
+    const bool out = !(c >= 0.f && c <= d), above = a > d;
+    const bool selc = lim && (out || (!above && a < c));
+    const bool seld = lim && !out && above;
+    const bool selq = lim && !out && !above && !(a < c) && a > q;
+    b = selc ? tc : (seld ? td : (selq ? tu : b));
+    lb = selc ? lc : (seld ? ld : (selq ? lu : lb));
+    dq = selq ? dc : 0.f;
   }
-  double flux = 0.0;
-  if (adv) {
-    // one expression for every branch: U (b + lb) + Vq dq
-    const bool cap = br == 1;
-    const float b = cap ? tu : base;
-    const float lb = cap ? lu : __fadd_rn(lbase, inc);
-    const float dq = cap ? __fadd_rn(__fsub_rn(tc, tu), __fsub_rn(lc, lu)) : 0.f;
-    flux = __fma_rn(cap ? f.V : 0.0, (double)dq,
-                    __dmul_rn(f.U, __dadd_rn((double)b, (double)lb)));
-  }
+  // U (b + lb) + V dq, V = U / |cr| (zero dq unless capped)
+  double flux = adv ? __fma_rn(f.V, (double)dq, __dmul_rn(f.U, __dadd_rn((double)b, (double)lb)))
+                    : 0.0;
   if (hd) flux = __dsub_rn(flux, (double)__fmul_rn(f.K, g01));
   return flux;
 }

@@ -585,13 +585,13 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
                                               const float *tr, float *to, double area, double ia,
                                               double idt, ColSums cs,
                                               double *carry, bool steady, long long &nwarn,
-                                              bool &bad, float *R0 = nullptr,
+                                              bool &bad, int16_t *R0 = nullptr,
                                               const int16_t *li = nullptr,
                                               int16_t *lout = nullptr) {
   // FP32_COMP (R0, li, lout non-null): R0 keeps each row's value - stored
-  // (the advection's rounding residual, or the old value's decoded
-  // compensation, both exact in FP32) for the solve's residual and the final
-  // value; li is the tracer's compensation on the way in, lout on the way out
+  // (the advection's rounding residual, or the old value's compensation) in
+  // the compensation's format for the solve's residual and the final value;
+  // li is the tracer's compensation on the way in, lout on the way out
   const ColInfo &ci = tc.ci;
   const int kb = tc.kb, nz = G.nz, c2 = tc.c2;
   const int nk = tc.ks - kb;  // cells below the surface cell
@@ -647,7 +647,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       a = mnf;
       r = 0.0;
     }
-    if (R0) R0[j * sa] = (float)r;
+    if (R0) R0[j * sa] = lo_bits((float)r);
     if (tbdy) {
       nw += (a < mn_up || a > mx_dn);
       A0[j * sa] = a;
@@ -661,7 +661,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   mxs += (tbdy && !RES) ? cs.m : m;
   if (tbdy) {
     const double a_below =
-        nk > 0 ? (double)A0[(nk - 1) * sa] + (R0 ? (double)R0[(nk - 1) * sa] : 0.0) : 0.0;
+        nk > 0 ? (double)A0[(nk - 1) * sa] + (R0 ? (double)lo_val(R0[(nk - 1) * sa]) : 0.0)
+               : 0.0;
     // surf_conc with s == co (tracers.c:3097-3206): column mass in FP64
     if (adv) {
       const double wb = (ci.s == tc.cbot) ? G.botz[c2] : G.gridz[ci.s];
@@ -711,7 +712,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
   if (!solve) {
     // the values as they are, plus the carry's shift (tr_bounds has run)
     for (int j = 0; j < nk; ++j)
-      store(C0[j * 32], (double)A0[j * sa] + (R0 ? (double)R0[j * sa] : 0.0) + dl, D0[j * 32]);
+      store(C0[j * 32], (double)A0[j * sa] + (R0 ? (double)lo_val(R0[j * sa]) : 0.0) + dl,
+            D0[j * 32]);
     const double h = dzs_old > O.hmin ? dzs_old : O.hmin;
     store(ci.s, (vdf && single) ? vs + dl + F.dt * (0.0 - 0.0) / h : vs + dl, dzs);
   } else {
@@ -742,7 +744,8 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
       const double xd = (double)x, l1y = (double)l1.y;
       const double aj1 =
           ((j + 1 == nk) ? vs
-                         : (double)A0[(j + 1) * sa] + (R0 ? (double)R0[(j + 1) * sa] : 0.0)) +
+                         : (double)A0[(j + 1) * sa] +
+                               (R0 ? (double)lo_val(R0[(j + 1) * sa]) : 0.0)) +
           dl;
       double r = dzdt1 * (aj1 - xd1) - l1y * (xd - xd1);
       if (j + 1 < nk) r = r - l2y * (xd2 - xd1);
@@ -756,7 +759,7 @@ __device__ __forceinline__ void column_finish(const Geo &G, const Flow &F, const
     }
     {
       const double a0 =
-          ((nk == 0) ? vs : (double)A0[0] + (R0 ? (double)R0[0] : 0.0)) + dl;
+          ((nk == 0) ? vs : (double)A0[0] + (R0 ? (double)lo_val(R0[0]) : 0.0)) + dl;
       double r = dzdt1 * (a0 - xd1);
       if (nk > 0) r = r - l2y * (xd2 - xd1);
       A0[0] = (float)r;
@@ -790,10 +793,11 @@ constexpr int kVd32MaxWarps = 16;
 // shared memory of k_vd32 (bytes) for columns of at most nd layers:
 // LU float4[nd][32], thicknesses double[nd][32], colC int[nd][32], A, S
 // float[nd][nw][32] (twice with pf: the next tracer's column is staged
-// while the current one is solved), with comp (FP32_COMP) R float[nd][nw][32]
+// while the current one is solved), with comp (FP32_COMP) R, compensations
+// int16[nd][nw][32]
 inline size_t vd32_smem(int nd, int nw, bool pf = false, bool comp = false) {
-  return (size_t)nd * 32 * (16 + 8 + 4) +
-         (size_t)((pf ? 4 : 2) + (comp ? 1 : 0)) * nd * nw * 32 * 4;
+  return (size_t)nd * 32 * (16 + 8 + 4) + (size_t)(pf ? 4 : 2) * nd * nw * 32 * 4 +
+         (comp ? (size_t)nd * nw * 32 * 2 : 0);
 }
 
 // COMP: FP32_COMP, each value's 16-bit compensation read from loi and
@@ -849,7 +853,8 @@ __global__ void __launch_bounds__(kVd32MaxWarps * 32) k_vd32(Geo G, Flow F, Work
   const size_t off = (size_t)wy * 32 + lane + (size_t)(kb - kbase) * sa;
   auto A0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + off; };
   auto S0of = [&](int b) { return bufs + (size_t)b * 2 * nd * sa + (size_t)nd * sa + off; };
-  float *const R0 = COMP ? bufs + (size_t)(PF ? 4 : 2) * nd * sa + off : nullptr;
+  int16_t *const R0 =
+      COMP ? reinterpret_cast<int16_t *>(bufs + (size_t)(PF ? 4 : 2) * nd * sa) + off : nullptr;
   const float4 *const L0 = LU + (kb - kbase) * 32 + lane;
   const int *const C0 = colC + (kb - kbase) * 32 + lane;
   const double *const D0 = DZ + (kb - kbase) * 32 + lane;
