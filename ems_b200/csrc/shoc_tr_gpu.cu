@@ -251,6 +251,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
                                                 int fp32, const int *own, int probe) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
   double dtmin = __longlong_as_double(0x7ff0000000000000ll);
+  int nwetcol = 0, ncells = 0;  // this column's share of counts[0], counts[1]
   if (col < G.ncol) {
     const int top = G.col_top[col], bot = G.col_bot[col], kb = G.col_kb[col];
     const int nk = G.nz - kb;  // wet layers of the column
@@ -347,8 +348,8 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     int cbs = 0;
     if (wet) {
       flags |= COL_WET;
-      atomicAdd(&counts[0], 1);
-      atomicAdd(&counts[1], nc);
+      nwetcol = 1;
+      ncells = nc;
       // tr_bounds thin-surface test (:3250-3252)
       if (js > 1 && dz_js0 < O.hmin) {
         flags |= COL_THIN;
@@ -439,11 +440,16 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
       W.serial_list[i] = col;
     }
   }
-  // block-reduce the sub-step minimum
+  // warp-reduce the counts and the sub-step minimum: one atomic per warp
+  const int wc = __reduce_add_sync(0xffffffffu, nwetcol);
+  const int wn = __reduce_add_sync(0xffffffffu, ncells);
   double v = dtmin;
   for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  if ((threadIdx.x & 31) == 0 && v < __longlong_as_double(0x7ff0000000000000ll))
-    atomic_min_pos(W.dtm_bits, v);
+  if ((threadIdx.x & 31) == 0) {
+    if (wc) atomicAdd(&counts[0], wc);
+    if (wn) atomicAdd(&counts[1], wn);
+    if (v < __longlong_as_double(0x7ff0000000000000ll)) atomic_min_pos(W.dtm_bits, v);
+  }
 }
 
 // Courant numbers of one sub-step over every wet cell (tracers.c:730-736).
