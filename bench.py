@@ -483,6 +483,8 @@ def main():
     achieved = kb / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
     traffic = None
     try:
+        if args.size:  # the recorded traffic is of the workload's own size
+            raise KeyError(args.size)
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             t = json.load(f).get("%s/%s/%s" % (kname, args.workload, args.precision))
         if t:

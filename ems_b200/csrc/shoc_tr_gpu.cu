@@ -246,6 +246,9 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
 // own (or null): 1 for the columns whose cells count in the sub-step minimum
 // (a strip of a decomposed basin counts its own columns, not its halo).
 // probe: compute the minimum only and leave the surface vectors as they are.
+// Reads of arrays no kernel of the step writes go through the read-only
+// path (__ldg), so the compiler may issue them ahead of this thread's stores
+// to the work arrays.
 __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Tile Tl,
                                                 int any_vdiff, int *counts, int list_all,
                                                 int fp32, const int *own, int probe) {
@@ -258,16 +261,16 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     const int sed = G.zm1[bot];
     // cell of layer j and the layer of a cell of this column
     auto cell = [&](int j) {
-      return j == 0 ? sed : Tl.cellk[(size_t)(kb + j - 1) * Tl.ncolp + col];
+      return j == 0 ? sed : __ldg(&Tl.cellk[(size_t)(kb + j - 1) * Tl.ncolp + col]);
     };
-    auto jof = [&](int c) { return c == sed ? 0 : G.kof[c] - kb + 1; };
+    auto jof = [&](int c) { return c == sed ? 0 : __ldg(&G.kof[c]) - kb + 1; };
 
     // new and old surface cells (tracers.c:5739-5755): down from the top
     // while the cell's bottom is at or above eta, at most to the sediment
     int sur = W.nsur_t[col];
     int jn = nk;
     const double etat = F.eta[top];
-    while (jn > 0 && G.gridz[cell(jn)] >= etat) --jn;
+    while (jn > 0 && __ldg(&G.gridz[cell(jn)]) >= etat) --jn;
     int nsur = cell(jn);
     if (!probe) {
       W.sur_t[col] = sur;
@@ -291,8 +294,8 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
     auto dzof = [&](int j) -> double {
       const int jj = j < js0 ? j : js0;
       if (jj == 0) return dzsed;
-      const double tp = (jj == js0) ? oet : G.gridz[cell(jj + 1)];
-      return tp - ((jj > 1) ? G.gridz[cell(jj)] : bott);
+      const double tp = (jj == js0) ? oet : __ldg(&G.gridz[cell(jj + 1)]);
+      return tp - ((jj > 1) ? __ldg(&G.gridz[cell(jj)]) : bott);
     };
     // top-down pass: dz, dz32, w5, w9, dbz, dfz (:530-567), the sub-step
     // search over the cells to process (:591-661) and what the flags need
@@ -320,17 +323,17 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
       if (wet && j <= js) {
         nc++;
         if (substep && counts_min) {
-          const int xp = G.xp1[cc], yp = G.yp1[cc], zp = cell(j < nk ? j + 1 : nk);
-          double d4 = 0.5 * (F.u1[cc] + F.u1[xp]);
+          const int xp = __ldg(&G.xp1[cc]), yp = __ldg(&G.yp1[cc]), zp = cell(j < nk ? j + 1 : nk);
+          double d4 = 0.5 * (__ldg(&F.u1[cc]) + __ldg(&F.u1[xp]));
           if (fabs(d4) < kMinVal) d4 = kMinVal;
           double d1 = kSF * fabs(G.h1acell[c2] / d4);
           if (d1 < dtmin) dtmin = d1;
-          d4 = 0.5 * (F.u2[cc] + F.u2[yp]);
+          d4 = 0.5 * (__ldg(&F.u2[cc]) + __ldg(&F.u2[yp]));
           if (fabs(d4) < kMinVal) d4 = kMinVal;
           double d2 = kSF * fabs(G.h2acell[c2] / d4);
           if (d2 < dtmin) dtmin = d2;
           if (j != js) {
-            d4 = 0.5 * (F.w[cc] + F.w[zp]);
+            d4 = 0.5 * (__ldg(&F.w[cc]) + __ldg(&F.w[zp]));
             if (fabs(d4) < kMinVal) d4 = kMinVal;
             double d3 = kSF * fabs(dzc * 1.0 / d4);
             if (d3 > 0.0 && d3 < dtmin) dtmin = d3;
@@ -375,7 +378,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
         double dzj = W.dz[cb], dzj1 = W.dz[zpb];
         double dzf_p = 0.5 * (dzj + dzj1);
         double dzdt = dzj / dt;
-        double cp1 = -F.Kz[zpb] / dzf_p;
+        double cp1 = -__ldg(&F.Kz[zpb]) / dzf_p;
         double C = dzdt - cp1;
         double div = C;
         W.vd_cm1[cb] = 0.0;
@@ -391,8 +394,8 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
           double dzf_c = dzf_p;
           dzf_p = 0.5 * (dzj1 + dzn);
           dzdt = dzj1 / dt;
-          double cm1 = -F.Kz[cc2] / dzf_c;
-          cp1 = -F.Kz[zp] / dzf_p;
+          double cm1 = -__ldg(&F.Kz[cc2]) / dzf_c;
+          cp1 = -__ldg(&F.Kz[zp]) / dzf_p;
           C = dzdt - cm1 - cp1;
           double ud = bp1 / div;
           div = C - cm1 * ud;
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Ti
         {
           double dzf_c = dzf_p;
           dzdt = dz_jn / dt;
-          double cm1 = -F.Kz[cs] / dzf_c;
+          double cm1 = -__ldg(&F.Kz[cs]) / dzf_c;
           C = dzdt - cm1;
           double ud = bp1 / div;
           div = C - cm1 * ud;
