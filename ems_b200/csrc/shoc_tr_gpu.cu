@@ -248,8 +248,11 @@ __device__ __forceinline__ void atomic_min_pos(unsigned long long *p, double v) 
 // probe: compute the minimum only and leave the surface vectors as they are.
 // Reads of arrays no kernel of the step writes go through the read-only
 // path (__ldg), so the compiler may issue them ahead of this thread's stores
-// to the work arrays.
-__global__ void __launch_bounds__(128) k_set_dz(Geo G, Flow F, Work W, Opt O, Tile Tl,
+// to the work arrays.  The walk down a column waits on dependent loads, so
+// the kernel is held to 64 registers for 8 blocks (32 warps) per SM: 2.26
+// against 2.67 ms outside the transport kernels at stiff2048 (80 registers,
+// 6 blocks); tighter bounds spill.
+__global__ void __launch_bounds__(128, 8) k_set_dz(Geo G, Flow F, Work W, Opt O, Tile Tl,
                                                 int any_vdiff, int *counts, int list_all,
                                                 int fp32, const int *own, int probe) {
   int col = blockIdx.x * blockDim.x + threadIdx.x;
