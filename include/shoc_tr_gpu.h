@@ -158,9 +158,8 @@ int shoc_tr_gpu_mass(shoc_tr_gpu *h, double *mass);
  * for 64 tracers) that every device loading the library holds until the
  * process exits; with more tracers it returns SHOC_TR_ESCRATCH.  The first
  * call on a device looks the array's device address up once
- * (cudaGetSymbolAddress) and keeps it, so make that first call before any
- * stream capture, and do not keep using the library across a reset of the
- * device (cudaDeviceReset).  All calls share the one array: calls whose GPU
+ * (cudaGetSymbolAddress) and keeps it, so do not keep using the library
+ * across a reset of the device (cudaDeviceReset).  All calls share the one array: calls whose GPU
  * work overlaps in time (two handles on different streams, say) race and
  * must be serialised by the caller.  mass[ntr] is host memory; the call
  * copies the sums into it and waits for its stream before returning. */
