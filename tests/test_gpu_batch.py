@@ -74,3 +74,20 @@ def test_batch_mass_per_carried_columns(batch):
     t.close()
     # tracer 31 is carried by the largest basin only, tracer 0 by all
     assert m[0] > m[31] > 0
+
+
+def test_batch_fp32_comp_within_tolerance(batch):
+    """FP32_COMP on the batch: every carried pair within 1e-7 of the oracle
+    after 3 steps, and the pairs a column does not carry come back as
+    uploaded to the compensation's precision (2^-32)."""
+    case, ref = batch
+    got = run(case, 3, gpu.FP32_COMP)
+    m, w = carried(case)
+    g, r = got[:, w], ref[:, w]
+    for n in range(case.ntr):
+        sel = m[n]
+        if not sel.any():
+            continue
+        e = np.abs(g[n, sel] - r[n, sel]).max() / np.abs(r[n, sel]).max()
+        assert e <= 1e-7, (n, e)
+    assert np.allclose(g[~m], case.tr[:, w][~m], rtol=1e-9, atol=0)

@@ -120,7 +120,7 @@ def test_steps_with_device_preamble_equal_given_fields(name):
 
 @pytest.mark.gpu
 @pytest.mark.usefixtures("need_gpu")
-@pytest.mark.parametrize("precision", [gpu.FP64, gpu.FP32_MIXED])
+@pytest.mark.parametrize("precision", [gpu.FP64, gpu.FP32_MIXED, gpu.FP32_COMP])
 def test_dropin_steps_with_preamble_equal_resident(precision):
     """The drop-in call on host arrays runs the preamble too: 3 drop-in steps
     with it on give the resident run's tracers and surfaces bit for bit, and
