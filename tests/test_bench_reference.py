@@ -67,3 +67,12 @@ def test_reference_arm_loads_no_package_library():
     assert r.returncode == 0, r.stderr[-2000:]
     libs = {l.split()[-1] for l in r.stdout.splitlines() if l.endswith(".so") and ROOT in l}
     assert libs and all(os.sep + "oracle" + os.sep in p for p in libs), libs
+
+
+def test_reference_arm_bounds_full_window_steps():
+    """On the full window the arm times at most REF_MAX_STEPS of the steps
+    asked for, and says so in its line."""
+    d = run_bench("--workload", "stiff2048", "--size", "64x48", "--steps", "7", "--warmup", "2")
+    check_line(d, "stiff2048@64x48")
+    assert d["steps"] == 3 and d["steps_requested"] == 7 and d["warmup"] == 1
+    assert "3 timed steps in one call (of 7 requested)" in d["cpu_baseline"]["sample"]
